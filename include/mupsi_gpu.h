@@ -1,0 +1,258 @@
+/*
+ * mupsi_gpu.h -- C ABI of the B200 GPIS path-tracing library (libmupsi_gpu.so).
+ *
+ * The reference renderer enters its hot path through per-point virtual calls
+ * (SparseGPNoiseGenerator::RawNoise, MeanFunction::eval/gradient,
+ * Medium::sampleDistance, BVH::intersect/closest) driven by an OpenMP pixel loop
+ * (Renderer::startRenderProgressive). A GPU can only be entered at batch
+ * granularity, so this ABI sits at two levels:
+ *   - the Renderer level: a scene handle plus a progressive render call, which
+ *     a GpuRenderer in the reference host calls instead of its pixel loop;
+ *   - batched probes of each per-point interface, used by parity tests and by
+ *     hosts that want the kernels without the renderer.
+ *
+ * Conventions (mirroring the reference's bool + std::cerr error style,
+ * controller/controller.cpp:44-47):
+ *   - every entry returns int: 0 (MUPSI_OK) or a negative mupsi_status;
+ *     mupsi_gpu_last_error() gives a message for the calling thread;
+ *   - the caller owns every input/output buffer; `mem` says whether the
+ *     buffers of that call are host or device pointers (all of one kind);
+ *   - `stream` is a cudaStream_t (NULL = the library's internal stream);
+ *     calls are synchronous with respect to the host unless named *_async;
+ *   - plain C types only: no CUDA, torch or C++ types cross this boundary.
+ */
+#ifndef MUPSI_GPU_H
+#define MUPSI_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MUPSI_GPU_ABI_VERSION 1
+
+typedef enum { MUPSI_MEM_HOST = 0, MUPSI_MEM_DEVICE = 1 } mupsi_mem;
+
+typedef enum {
+  MUPSI_OK = 0,
+  MUPSI_ERR_INVALID = -1,      /* bad argument or descriptor */
+  MUPSI_ERR_CUDA = -2,         /* a CUDA runtime call failed */
+  MUPSI_ERR_OOM = -3,          /* device allocation failed */
+  MUPSI_ERR_CANCELLED = -4,    /* *cancel became non-zero between passes */
+  MUPSI_ERR_UNSUPPORTED = -5,  /* feature not available on this build/device */
+  MUPSI_ERR_DEVICE_LIMIT = -6, /* a device-side iteration cap fired */
+  MUPSI_ERR_IO = -7            /* file could not be read/parsed */
+} mupsi_status;
+
+/* GP correlation modes (gp/gpnoise.h:9-15) */
+typedef enum { MUPSI_GP_SINGLE_REALIZATION = 0, MUPSI_GP_RENEWAL_PLUS = 1 } mupsi_gp_mode;
+/* BSDFs (bsdf/bsdf.h:38-105) */
+typedef enum { MUPSI_BSDF_LAMBERTIAN = 0, MUPSI_BSDF_NULL = 1, MUPSI_BSDF_SPECULAR = 2 } mupsi_bsdf;
+/* mean functions (gp/meanfunction.h:10-57) */
+typedef enum { MUPSI_MEAN_SPHERE = 0, MUPSI_MEAN_MESH = 1 } mupsi_mean_type;
+/* primitives (geometry/primitive.h:17-67) */
+typedef enum { MUPSI_PRIM_SPHERE = 0, MUPSI_PRIM_MESH = 1 } mupsi_prim_type;
+
+/* SparseSEKernel(sigma, kernelRadius, lengthScale) + impulse density
+ * (gp/kernel.h:39-78, gp/gpnoise.h:23-49). JSON keys: kernel.sigma,
+ * kernel.length_scale (-> kernel_radius, the grid cell size), kernel.aniso
+ * (-> the lengthScale vector; h() uses L2 = |aniso|^2), kernel.points_per_cell. */
+typedef struct {
+  float sigma;
+  float kernel_radius;
+  float aniso[3];
+  int32_t points_per_cell;
+} mupsi_kernel;
+
+/* GPConditioningState (medium/medium.h:12-17), 32 bytes. */
+typedef struct {
+  float C[3];
+  float u_tilde;
+  float g_tilde[3];
+  uint32_t active;
+} mupsi_cond;
+
+/* Ray (geometry/ray.h:10-28): origin, unit direction, nearT, farT; 32 bytes. */
+typedef struct {
+  float o[3];
+  float d[3];
+  float near_t;
+  float far_t;
+} mupsi_ray;
+
+/* MediumSample subset returned by a march (medium/medium.h:21-29), 32 bytes. */
+typedef struct {
+  uint32_t exited; /* 1: no surface found along the ray */
+  float t;
+  float p[3];
+  float normal[3];
+} mupsi_medium_sample;
+
+/* Triangle mesh (primitives/mesh.h:15-78). Object-space arrays plus the
+ * Translation(position)*Scaling(scale) transform the JSON schema allows. */
+typedef struct {
+  int64_t num_vertices;
+  const float* vertices; /* [num_vertices*3] */
+  int64_t num_faces;
+  const int32_t* faces; /* [num_faces*3], 0-based */
+  const float* vertex_normals; /* nullable [num_vertices*3] */
+  float position[3];
+  float scale;
+} mupsi_mesh_desc;
+
+/* Mean function + kernel of one GPMedium (medium/gpmedium.h:19-51). */
+typedef struct {
+  int32_t mean_type;     /* mupsi_mean_type */
+  float mean_center[3];  /* sphere mean */
+  float mean_radius;
+  int32_t mean_mesh;     /* index into scene meshes (mesh mean) */
+  mupsi_kernel kernel;
+} mupsi_medium_desc;
+
+/* One scene primitive (sphere or mesh) in scene order. */
+typedef struct {
+  int32_t type;          /* mupsi_prim_type */
+  float center[3];       /* sphere: Translation(center)*Scaling(radius) */
+  float radius;
+  int32_t mesh;          /* mesh: index into scene meshes */
+  int32_t bsdf;          /* mupsi_bsdf */
+  float albedo[3];       /* Lambertian albedo (reference default 0.8) */
+  int32_t has_emission;
+  float emission[3];
+  int32_t int_medium;    /* index into media, -1 = none */
+  int32_t ext_medium;
+} mupsi_primitive_desc;
+
+/* Everything Controller::load builds (controller/controller.cpp:40-264) plus
+ * the RenderContext snapshot (rendering/render_context.h:16-27). */
+typedef struct {
+  int32_t width, height, spp;
+  int32_t max_bounce;
+  int32_t max_medium_bounce; /* parsed but unused by the reference trace loop */
+  int32_t gp_mode;           /* mupsi_gp_mode */
+  float cam_pos[3], cam_dir[3], cam_up[3];
+  float cam_fov;             /* as in scene.json; tan(fov/2) is taken with fov in radians (camera.cpp:10-11) */
+  float eps;                 /* PathTracerSettings::eps (1e-4) */
+  float nearteps;            /* PathTracerSettings::nearteps (1.5e-3) */
+  int32_t has_sky;           /* skydrome present */
+  float sky[3];              /* constant skydrome radiance (Skydrome() = 1.0) */
+  int32_t num_media;
+  const mupsi_medium_desc* media;
+  int32_t num_meshes;
+  const mupsi_mesh_desc* meshes;
+  int32_t num_primitives;
+  const mupsi_primitive_desc* primitives;
+} mupsi_scene_desc;
+
+typedef struct mupsi_scene mupsi_scene;
+typedef struct mupsi_mesh mupsi_mesh;
+
+/* ---------------------------------------------------------------- errors -- */
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* mupsi_gpu_last_error(void);
+/* ABI version compiled into the library (MUPSI_GPU_ABI_VERSION). */
+int32_t mupsi_gpu_abi_version(void);
+/* Number of kernel launches this library has issued on this process. */
+int64_t mupsi_gpu_launch_count(void);
+
+/* ------------------------------------------------------- GP noise batch -- */
+
+/* psi and grad psi at n points: SparseGPNoiseGenerator::RawNoise(p, seed)
+ * (gp/gpnoise.h:44, gp/gpnoise.cpp:51-87). out[n*4] = (psi, dpsi/dx, dpsi/dy, dpsi/dz).
+ * cond (nullable, n entries): adds the Renewal+ terms of GPMedium::evalWithGradient
+ * (medium/gpmedium.cpp:26-41) for entries with active != 0, without the mean. */
+int mupsi_gpu_psi(const mupsi_kernel* kernel, int64_t n, const float* p, const uint32_t* seed,
+                  const mupsi_cond* cond, float* out, mupsi_mem mem, void* stream);
+/* psi value only (no gradient), same sum as mupsi_gpu_psi's first output. */
+int mupsi_gpu_psi_value(const mupsi_kernel* kernel, int64_t n, const float* p, const uint32_t* seed,
+                        const mupsi_cond* cond, float* out, mupsi_mem mem, void* stream);
+
+/* ----------------------------------------------------- meshes and BVHs -- */
+
+/* Host BVH build (bvh/bvh.cpp:115-193): same split rule, leaf size, partition
+ * order and post-order node emission as BVH::build, so node arrays and triangle
+ * ids match. nodes_out[2*num_faces*8] words per node: min xyz, max xyz (float
+ * bits), left, right|0x80000000 for leaves. Returns the node count in
+ * *num_nodes and the root (last node) in *root. */
+int mupsi_bvh_build_host(int64_t num_vertices, const float* vertices, int64_t num_faces, const int32_t* faces,
+                         uint32_t* nodes_out, uint32_t* tri_indices_out, int64_t* num_nodes, uint32_t* root);
+
+/* Device copy of a mesh and its BVH (Mesh::prepareForRender, mesh.cpp:299-319). */
+int mupsi_gpu_mesh_create(const mupsi_mesh_desc* desc, mupsi_mesh** out);
+void mupsi_gpu_mesh_destroy(mupsi_mesh* mesh);
+
+/* BVH::intersect (bvh.cpp:197-250) in object space for n rays. out_tri[n]
+ * (0xFFFFFFFF on miss), out_tuv[n*3] = (t, u, v). */
+int mupsi_gpu_bvh_intersect(const mupsi_mesh* mesh, int64_t n, const mupsi_ray* rays, uint32_t* out_tri,
+                            float* out_tuv, mupsi_mem mem, void* stream);
+/* BVH::occluded (bvh.cpp:254-300), including its traversal start at node 0. */
+int mupsi_gpu_bvh_occluded(const mupsi_mesh* mesh, int64_t n, const mupsi_ray* rays, uint8_t* out,
+                           mupsi_mem mem, void* stream);
+/* BVH::closest (bvh.cpp:302-353): out_tri[n], out_dq[n*4] = (dist, q xyz). */
+int mupsi_gpu_bvh_closest(const mupsi_mesh* mesh, int64_t n, const float* p, uint32_t* out_tri, float* out_dq,
+                          mupsi_mem mem, void* stream);
+/* Mesh::inside (mesh.cpp:341-362) and Mesh::distToPoint (mesh.cpp:325-339)
+ * in world space: out_inside[n], out_tri[n], out_dq[n*4] = (dist, q xyz). */
+int mupsi_gpu_mesh_queries(const mupsi_mesh* mesh, int64_t n, const float* p, uint8_t* out_inside,
+                           uint32_t* out_tri, float* out_dq, mupsi_mem mem, void* stream);
+
+/* ------------------------------------------------------------ scenes -- */
+
+/* Flatten a scene description to device buffers (builds mesh BVHs on the host).
+ * The library copies everything; the descriptor may be freed afterwards. */
+int mupsi_gpu_scene_create(const mupsi_scene_desc* desc, mupsi_scene** out);
+void mupsi_gpu_scene_destroy(mupsi_scene* scene);
+
+/* MeanFunction::eval + gradient of medium `medium` (gp/meanfunction.cpp:13-39):
+ * out[n*4] = (mu, grad xyz). */
+int mupsi_gpu_mean(const mupsi_scene* scene, int32_t medium, int64_t n, const float* p, float* out,
+                   mupsi_mem mem, void* stream);
+/* GPMedium::evalWithGradient(p, seed, state) (gpmedium.cpp:19-41): out[n*4]. */
+int mupsi_gpu_medium_eval(const mupsi_scene* scene, int32_t medium, int64_t n, const float* p,
+                          const uint32_t* seed, const mupsi_cond* cond, float* out, mupsi_mem mem, void* stream);
+/* GPMedium::sampleDistance (gpmedium.cpp:46-103) for n rays; seed[i] is the value
+ * the march draws from its ConstantSampler (medium_sampler.nextI()). */
+int mupsi_gpu_sample_distance(const mupsi_scene* scene, int32_t medium, int64_t n, const mupsi_ray* rays,
+                              const uint32_t* seed, const mupsi_cond* cond, mupsi_medium_sample* out,
+                              mupsi_mem mem, void* stream);
+/* GPMedium::sampleCondition (gpmedium.cpp:133-161) for n medium samples; seed[i]
+ * is the next bounce's ConstantSampler draw. */
+int mupsi_gpu_sample_condition(const mupsi_scene* scene, int32_t medium, int64_t n,
+                               const mupsi_medium_sample* samples, const uint32_t* seed, mupsi_cond* out,
+                               mupsi_mem mem, void* stream);
+
+/* PathTracer::trace (rendering/trace.cpp:118-213) for n explicit (x, y, k)
+ * samples, hash seed 42 as Renderer uses (renderer.cpp:37). out_rgb[n*3]. */
+int mupsi_gpu_trace_samples(mupsi_scene* scene, int64_t n, const int32_t* x, const int32_t* y, const int32_t* k,
+                            float* out_rgb, mupsi_mem mem, void* stream);
+
+/* Progressive render (Renderer::startRenderProgressive, renderer.cpp:22-49):
+ * passes k in [spp_begin, spp_end) are traced and accumulated into the scene's
+ * running per-pixel sum (Framebuffer::accumulate, framebuffer.cpp:28-35), in
+ * pass order. After the call rgb_out[h*w*3] holds sum / passes-so-far (row y =
+ * camera y, as Controller::copyDisplayRawTo). spp_begin == 0 resets the sum.
+ * cancel (nullable) is polled between waves of passes; on_spp (nullable) is
+ * called with the number of completed passes after each wave.
+ * moments_out (nullable, h*w*6 doubles) receives per pixel the FP64 sum and
+ * sum of squares (r,g,b,r2,g2,b2) of this call's samples. */
+typedef struct {
+  int32_t spp_begin;
+  int32_t spp_end;
+  const volatile int32_t* cancel;
+  void (*on_spp)(int32_t passes_done, void* user);
+  void* user;
+  float* rgb_out;
+  mupsi_mem out_mem;
+  double* moments_out;
+  void* stream;
+} mupsi_render_args;
+int mupsi_gpu_render(mupsi_scene* scene, const mupsi_render_args* args);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MUPSI_GPU_H */

@@ -1,0 +1,395 @@
+"""Scene descriptions: scene.json loading and the synthetic benchmark scenes.
+
+`Scene` holds what the reference's Controller::load builds
+(controller/controller.cpp:40-264) as flat numpy arrays and turns it into the
+C ABI's mupsi_scene_desc (include/mupsi_gpu.h). The arrays stay referenced by
+the Scene, so a descriptor is valid while its Scene lives.
+"""
+import ctypes as C
+import json
+import math
+import os
+
+import numpy as np
+
+from . import _abi
+
+DEFAULT_ALBEDO = 0.8  # Bsdf::default_albedo_ (bsdf/bsdf.cpp:11)
+
+
+class Mesh:
+    """Triangle mesh (primitives/mesh.h): object-space vertices/faces + T*S transform."""
+
+    def __init__(self, vertices, faces, vertex_normals=None, position=(0.0, 0.0, 0.0), scale=1.0):
+        self.vertices = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
+        self.faces = np.ascontiguousarray(faces, dtype=np.int32).reshape(-1, 3)
+        self.vertex_normals = (None if vertex_normals is None else
+                               np.ascontiguousarray(vertex_normals, dtype=np.float32).reshape(-1, 3))
+        self.position = tuple(float(v) for v in position)
+        self.scale = float(scale)
+
+    def desc(self):
+        return _abi.MeshDesc(
+            len(self.vertices), self.vertices.ctypes.data, len(self.faces), self.faces.ctypes.data,
+            None if self.vertex_normals is None else self.vertex_normals.ctypes.data,
+            _abi.f3(*self.position), self.scale)
+
+
+def load_obj(path):
+    """OBJ reader following Mesh::fetchFrom (primitives/mesh.cpp:20-136): v, vn,
+    vt, triangular f in v, v/vt, v//vn, v/vt/vn forms, 1-based or negative indices;
+    faces with other vertex counts are skipped."""
+    verts, normals, faces = [], [], []
+    with open(path) as fh:
+        for line in fh:
+            line = line.rstrip("\r\n")
+            if not line or line[0] == "#":
+                continue
+            parts = line.split()
+            if not parts:
+                continue
+            t = parts[0]
+            if t == "v":
+                verts.append([float(v) for v in parts[1:4]])
+            elif t == "vn":
+                normals.append([float(v) for v in parts[1:4]])
+            elif t == "f":
+                idx = []
+                for spec in parts[1:]:
+                    vi = int(spec.split("/")[0])
+                    idx.append(vi - 1 if vi > 0 else (len(verts) + vi if vi < 0 else 0))
+                if len(idx) == 3:
+                    faces.append(idx)
+    if not verts or not faces:
+        raise ValueError(f"{path}: no valid geometry")
+    return np.array(verts, np.float32), np.array(faces, np.int32), (np.array(normals, np.float32) if normals else None)
+
+
+def save_obj(path, vertices, faces):
+    """Write a mesh as OBJ (vertices at full float32 precision, 1-based faces)."""
+    v = np.asarray(vertices, np.float32)
+    f = np.asarray(faces, np.int64) + 1
+    with open(path, "w") as fh:
+        fh.write("".join("v %.9g %.9g %.9g\n" % tuple(r) for r in v.tolist()))
+        fh.write("".join("f %d %d %d\n" % tuple(r) for r in f.tolist()))
+
+
+class Scene:
+    """Python-side mirror of the scene the reference builds from scene.json."""
+
+    def __init__(self):
+        self.width = 256
+        self.height = 256
+        self.spp = 1
+        self.max_bounce = 3          # PathTracerSettings default (trace.h:17)
+        self.max_medium_bounce = 3
+        self.gp_mode = _abi.GP_SINGLE_REALIZATION
+        self.cam_pos = (0.0, 0.0, 0.0)
+        self.cam_dir = (0.0, 0.0, -1.0)
+        self.cam_up = (0.0, 1.0, 0.0)
+        self.cam_fov = 45.0
+        self.eps = float(np.float32(1e-4))
+        self.nearteps = float(np.float32(1e-4) * np.float32(15))
+        self.sky = None              # None = no skydrome; else constant RGB radiance
+        self.media = []              # dicts: mean_type, center, radius, mesh, sigma, length, aniso, ppc
+        self.meshes = []             # Mesh
+        self.primitives = []         # dicts
+        self._keep = []
+
+    # -- construction helpers -------------------------------------------------
+    def add_medium(self, mean_type="sphere", center=(0, 0, 0), radius=70.0, mesh=-1, sigma=1.0, length_scale=1.0,
+                   aniso=(1.0, 1.0, 1.0), points_per_cell=3):
+        self.media.append(dict(mean_type=_abi.MEAN_SPHERE if mean_type == "sphere" else _abi.MEAN_MESH,
+                               center=tuple(center), radius=float(radius), mesh=int(mesh), sigma=float(sigma),
+                               length=float(length_scale), aniso=tuple(aniso), ppc=int(points_per_cell)))
+        return len(self.media) - 1
+
+    def add_mesh(self, mesh):
+        self.meshes.append(mesh)
+        return len(self.meshes) - 1
+
+    def add_sphere(self, center, radius, bsdf=_abi.BSDF_LAMBERTIAN, albedo=DEFAULT_ALBEDO, emission=None,
+                   int_medium=-1, ext_medium=-1):
+        self.primitives.append(dict(type=_abi.PRIM_SPHERE, center=tuple(center), radius=float(radius), mesh=-1,
+                                    bsdf=bsdf, albedo=_rgb(albedo), emission=emission, int_medium=int_medium,
+                                    ext_medium=ext_medium))
+
+    def add_mesh_primitive(self, mesh_index, bsdf=_abi.BSDF_LAMBERTIAN, albedo=DEFAULT_ALBEDO, emission=None,
+                           int_medium=-1, ext_medium=-1):
+        self.primitives.append(dict(type=_abi.PRIM_MESH, center=(0, 0, 0), radius=1.0, mesh=mesh_index, bsdf=bsdf,
+                                    albedo=_rgb(albedo), emission=emission, int_medium=int_medium,
+                                    ext_medium=ext_medium))
+
+    # -- scene.json (controller.cpp:40-264) ------------------------------------
+    @classmethod
+    def from_json(cls, path_or_dict, sky=None, base_dir=None):
+        """Build a Scene the way Controller::load does. `sky` adds a constant
+        skydrome (Skydrome() is 1.0) since the reference only takes an image path."""
+        if isinstance(path_or_dict, dict):
+            j = path_or_dict
+            base_dir = base_dir or os.getcwd()
+        else:
+            with open(path_or_dict) as fh:
+                j = json.load(fh)
+            base_dir = base_dir or os.path.dirname(os.path.abspath(path_or_dict))
+        s = cls()
+        if "max_bounce" in j:
+            s.max_bounce = int(j["max_bounce"])
+        if "max_medium_bounce" in j:
+            s.max_medium_bounce = int(j["max_medium_bounce"])
+        if "spp" in j:
+            s.spp = int(j["spp"])
+        s.width = int(j.get("width", 256))
+        s.height = int(j.get("height", 256))
+        cam = j["camera"]
+        s.cam_pos = tuple(float(v) for v in cam["pos"])
+        s.cam_dir = tuple(float(v) for v in cam["dir"])
+        s.cam_up = tuple(float(v) for v in cam.get("up", [0, 1, 0]))
+        s.cam_fov = float(cam.get("fov", 45.0))
+        s.gp_mode = _abi.GP_RENEWAL_PLUS if j.get("gp_mode", "single_realization") == "renewal_plus" \
+            else _abi.GP_SINGLE_REALIZATION
+        gpm_index = -1
+        if "gp_medium" in j:
+            g = j["gp_medium"]
+            mt = g.get("mean_type", "sphere")
+            kern = j.get("kernel", {})
+            kw = dict(sigma=kern.get("sigma", 1.0), length_scale=kern.get("length_scale", 1.0),
+                      aniso=tuple(kern.get("aniso", [1, 1, 1])), points_per_cell=kern.get("points_per_cell", 3))
+            if mt == "sphere":
+                gpm_index = s.add_medium("sphere", center=g["mean_center"], radius=g.get("mean_radius", 70.0), **kw)
+            elif mt == "mesh":
+                v, f, n = load_obj(_resolve(base_dir, g["file"]))
+                t = g.get("transform", {})
+                mi = s.add_mesh(Mesh(v, f, n, position=t.get("position", (0, 0, 0)), scale=t.get("scale", 1.0)))
+                gpm_index = s.add_medium("mesh", mesh=mi, **kw)
+            else:
+                raise ValueError(f"unknown mean_type: {mt}")
+        for key in ("sdf_medium", "external_gp_medium"):
+            if key in j:
+                raise NotImplementedError(f"{key} is not part of the GPIS GPU path")
+        if "skydrome" in j:
+            raise NotImplementedError("image skydromes are not supported yet; pass sky=<constant radiance>")
+        if sky is not None:
+            s.sky = _rgb(sky)
+        if "primitives" not in j or not isinstance(j["primitives"], list):
+            raise ValueError("no primitives array in config")
+        bsdfs = {"lambertian": _abi.BSDF_LAMBERTIAN, "null": _abi.BSDF_NULL, "specular": _abi.BSDF_SPECULAR}
+        for pj in j["primitives"]:
+            typ = pj.get("type", "sphere")
+            bsdf = bsdfs.get(pj.get("bsdf", "lambertian"), _abi.BSDF_LAMBERTIAN)
+            if typ == "sphere":
+                em = _rgb(pj["emission"]) if "emission" in pj else None
+                s.add_sphere(pj["center"], pj.get("radius", 100.0), bsdf=bsdf, emission=em,
+                             int_medium=gpm_index if "int_medium" in pj else -1)
+            elif typ == "mesh":
+                if "texture" in pj:
+                    raise NotImplementedError("bitmap textures are not supported yet")
+                v, f, n = load_obj(_resolve(base_dir, pj["file"]))
+                t = pj.get("transform", {})
+                mi = s.add_mesh(Mesh(v, f, n, position=t.get("position", (0, 0, 0)), scale=t.get("scale", 1.0)))
+                s.add_mesh_primitive(mi, bsdf=bsdf)
+            # unknown primitive types are skipped, as the reference does
+        return s
+
+    # -- C ABI descriptor -------------------------------------------------------
+    def desc(self):
+        media = (_abi.MediumDesc * max(len(self.media), 1))()
+        for i, m in enumerate(self.media):
+            media[i] = _abi.MediumDesc(m["mean_type"], _abi.f3(*m["center"]), m["radius"], m["mesh"],
+                                       _abi.Kernel(m["sigma"], m["length"], _abi.f3(*m["aniso"]), m["ppc"]))
+        meshes = (_abi.MeshDesc * max(len(self.meshes), 1))()
+        for i, m in enumerate(self.meshes):
+            meshes[i] = m.desc()
+        prims = (_abi.PrimitiveDesc * max(len(self.primitives), 1))()
+        for i, p in enumerate(self.primitives):
+            em = p["emission"]
+            prims[i] = _abi.PrimitiveDesc(p["type"], _abi.f3(*p["center"]), p["radius"], p["mesh"], p["bsdf"],
+                                          _abi.f3(*p["albedo"]), 0 if em is None else 1,
+                                          _abi.f3(*(em if em is not None else (0, 0, 0))), p["int_medium"],
+                                          p["ext_medium"])
+        d = _abi.SceneDesc()
+        d.width, d.height, d.spp = self.width, self.height, self.spp
+        d.max_bounce, d.max_medium_bounce, d.gp_mode = self.max_bounce, self.max_medium_bounce, self.gp_mode
+        d.cam_pos, d.cam_dir, d.cam_up = _abi.f3(*self.cam_pos), _abi.f3(*self.cam_dir), _abi.f3(*self.cam_up)
+        d.cam_fov, d.eps, d.nearteps = self.cam_fov, self.eps, self.nearteps
+        d.has_sky = 0 if self.sky is None else 1
+        d.sky = _abi.f3(*(self.sky if self.sky is not None else (0, 0, 0)))
+        d.num_media, d.media = len(self.media), C.cast(media, C.POINTER(_abi.MediumDesc))
+        d.num_meshes, d.meshes = len(self.meshes), C.cast(meshes, C.POINTER(_abi.MeshDesc))
+        d.num_primitives, d.primitives = len(self.primitives), C.cast(prims, C.POINTER(_abi.PrimitiveDesc))
+        self._keep = [media, meshes, prims]
+        return d
+
+    def to_json(self, obj_paths=None):
+        """scene.json dict the reference's Controller::load accepts for this scene
+        (meshes must have been written to `obj_paths`). Returns (dict, extra_meshes):
+        primitives the schema cannot express (non-default albedo) are returned as
+        (obj_path, albedo) pairs for a harness to add."""
+        j = {"width": self.width, "height": self.height, "spp": self.spp, "max_bounce": self.max_bounce,
+             "max_medium_bounce": self.max_medium_bounce,
+             "gp_mode": "renewal_plus" if self.gp_mode == _abi.GP_RENEWAL_PLUS else "single_realization",
+             "camera": {"pos": list(self.cam_pos), "dir": list(self.cam_dir), "up": list(self.cam_up),
+                        "fov": self.cam_fov}, "primitives": []}
+        extra = []
+        if self.media:
+            if len(self.media) > 1:
+                raise ValueError("scene.json holds one gp_medium")
+            m = self.media[0]
+            j["kernel"] = {"sigma": m["sigma"], "length_scale": m["length"], "aniso": list(m["aniso"]),
+                           "points_per_cell": m["ppc"]}
+            if m["mean_type"] == _abi.MEAN_SPHERE:
+                j["gp_medium"] = {"mean_type": "sphere", "mean_center": list(m["center"]), "mean_radius": m["radius"]}
+            else:
+                mm = self.meshes[m["mesh"]]
+                j["gp_medium"] = {"mean_type": "mesh", "file": obj_paths[m["mesh"]],
+                                  "transform": {"position": list(mm.position), "scale": mm.scale}}
+        names = {_abi.BSDF_LAMBERTIAN: "lambertian", _abi.BSDF_NULL: "null", _abi.BSDF_SPECULAR: "specular"}
+        for p in self.primitives:
+            if p["type"] == _abi.PRIM_SPHERE:
+                pj = {"type": "sphere", "center": list(p["center"]), "radius": p["radius"], "bsdf": names[p["bsdf"]]}
+                if p["emission"] is not None:
+                    pj["emission"] = list(p["emission"])
+                if p["int_medium"] >= 0:
+                    pj["int_medium"] = True
+                j["primitives"].append(pj)
+            else:
+                mm = self.meshes[p["mesh"]]
+                if p["albedo"] != _rgb(DEFAULT_ALBEDO) or mm.position != (0, 0, 0) or mm.scale != 1.0:
+                    extra.append((obj_paths[p["mesh"]], p["albedo"][0]))
+                else:
+                    j["primitives"].append({"type": "mesh", "file": obj_paths[p["mesh"]], "bsdf": names[p["bsdf"]]})
+        return j, extra
+
+
+def _rgb(v):
+    if isinstance(v, (int, float)):
+        return (float(v),) * 3
+    return tuple(float(x) for x in v)
+
+
+def _resolve(base, f):
+    return f if os.path.isabs(f) else os.path.join(base, f)
+
+
+# ---------------------------------------------------------------------------
+# Synthetic scenes
+# ---------------------------------------------------------------------------
+
+def icosphere(level):
+    """Unit icosphere: 20*4^level faces, 10*4^level+2 vertices, deterministic order."""
+    t = (1.0 + 5 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+         (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10),
+         (8, 6, 7), (9, 8, 1)]
+    verts = np.array(v, np.float64)
+    verts /= np.linalg.norm(verts, axis=1, keepdims=True)
+    faces = np.array(f, np.int64)
+    for _ in range(level):
+        nv = len(verts)
+        e = np.concatenate([faces[:, [0, 1]], faces[:, [1, 2]], faces[:, [2, 0]]], axis=0)
+        e.sort(axis=1)
+        key = e[:, 0] * (nv + 1) + e[:, 1]
+        uniq, inv = np.unique(key, return_inverse=True)
+        a, b = uniq // (nv + 1), uniq % (nv + 1)
+        mid = verts[a] + verts[b]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        verts = np.concatenate([verts, mid], axis=0)
+        m = inv.reshape(3, -1) + nv
+        m01, m12, m20 = m[0], m[1], m[2]
+        v0, v1, v2 = faces[:, 0], faces[:, 1], faces[:, 2]
+        faces = np.stack([np.stack([v0, m01, m20], 1), np.stack([v1, m12, m01], 1), np.stack([v2, m20, m12], 1),
+                          np.stack([m01, m12, m20], 1)], axis=1).reshape(-1, 3)
+    return verts, faces
+
+
+def _real_sh(l, m, theta, phi):
+    """Orthonormal real spherical harmonic Y_lm (theta polar, phi azimuth)."""
+    x = np.cos(theta)
+    am = abs(m)
+    # associated Legendre P_l^|m|(x) by the standard upward recurrence
+    pmm = np.ones_like(x)
+    somx2 = np.sqrt(np.maximum(0.0, 1.0 - x * x))
+    fact = 1.0
+    for _ in range(am):
+        pmm = -pmm * fact * somx2
+        fact += 2.0
+    if l == am:
+        plm = pmm
+    else:
+        pmmp1 = x * (2 * am + 1) * pmm
+        if l == am + 1:
+            plm = pmmp1
+        else:
+            for ll in range(am + 2, l + 1):
+                pll = ((2 * ll - 1) * x * pmmp1 - (ll + am - 1) * pmm) / (ll - am)
+                pmm, pmmp1 = pmmp1, pll
+            plm = pmmp1
+    norm = math.sqrt((2 * l + 1) / (4 * math.pi) * math.factorial(l - am) / math.factorial(l + am))
+    if m > 0:
+        return math.sqrt(2.0) * norm * plm * np.cos(m * phi)
+    if m < 0:
+        return math.sqrt(2.0) * norm * plm * np.sin(am * phi)
+    return norm * plm
+
+
+def displaced_icosphere(level, radius=60.0, center=(0.0, 0.0, -300.0), n_harmonics=8, max_degree=6, max_amp=5.0,
+                        seed=0):
+    """Icosphere of `radius` displaced radially by a seeded sum of real spherical
+    harmonics (degree <= max_degree, amplitudes U(0, max_amp)), baked to world space."""
+    rng = np.random.default_rng(seed)
+    verts, faces = icosphere(level)
+    theta = np.arccos(np.clip(verts[:, 2], -1.0, 1.0))
+    phi = np.arctan2(verts[:, 1], verts[:, 0])
+    r = np.full(len(verts), float(radius))
+    for _ in range(n_harmonics):
+        l = int(rng.integers(1, max_degree + 1))
+        m = int(rng.integers(-l, l + 1))
+        a = float(rng.uniform(0.0, max_amp))
+        r += a * _real_sh(l, m, theta, phi)
+    world = verts * r[:, None] + np.asarray(center, np.float64)[None, :]
+    return world.astype(np.float32), faces.astype(np.int32)
+
+
+def floor_quad(y=-80.0, x0=-1000.0, x1=1000.0, z0=-1600.0, z1=400.0):
+    """Two-triangle quad at height y with face normals +y."""
+    v = np.array([[x0, y, z0], [x1, y, z0], [x1, y, z1], [x0, y, z1]], np.float32)
+    f = np.array([[0, 2, 1], [0, 3, 2]], np.int32)
+    return v, f
+
+
+def config0_scene(width=256, height=256, spp=20):
+    """Plain method, small: sphere mean (0,0,-500) r=70 inside a null sphere r=130,
+    renewal_plus, SE kernel sigma 1, length 1, aniso (1,1,1), 3 points/cell,
+    camera at the origin along -z, fov 45, constant sky 1.0, max_bounce 10."""
+    s = Scene()
+    s.width, s.height, s.spp = width, height, spp
+    s.max_bounce = 10
+    s.max_medium_bounce = 10
+    s.gp_mode = _abi.GP_RENEWAL_PLUS
+    s.sky = (1.0, 1.0, 1.0)
+    m = s.add_medium("sphere", center=(0, 0, -500), radius=70.0, sigma=1.0, length_scale=1.0, aniso=(1, 1, 1),
+                     points_per_cell=3)
+    s.add_sphere((0, 0, -500), 130.0, bsdf=_abi.BSDF_NULL, int_medium=m)
+    return s
+
+
+def config_mesh_scene(level=6, width=512, height=512, spp=64, seed=0):
+    """Mesh mean: displaced icosphere (r 60 at (0,0,-300)) as the GP mean inside a
+    null sphere r=100, Lambertian floor quad (albedo 0.7) at y=-80, renewal_plus,
+    SE kernel sigma 1, length 2, 3 points/cell."""
+    s = Scene()
+    s.width, s.height, s.spp = width, height, spp
+    s.max_bounce = 10
+    s.max_medium_bounce = 10
+    s.gp_mode = _abi.GP_RENEWAL_PLUS
+    s.sky = (1.0, 1.0, 1.0)
+    v, f = displaced_icosphere(level, seed=seed)
+    mesh = s.add_mesh(Mesh(v, f))
+    m = s.add_medium("mesh", mesh=mesh, sigma=1.0, length_scale=2.0, aniso=(1, 1, 1), points_per_cell=3)
+    s.add_sphere((0, 0, -300), 100.0, bsdf=_abi.BSDF_NULL, int_medium=m)
+    fv, ff = floor_quad()
+    fm = s.add_mesh(Mesh(fv, ff))
+    s.add_mesh_primitive(fm, bsdf=_abi.BSDF_LAMBERTIAN, albedo=0.7)
+    return s

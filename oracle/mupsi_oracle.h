@@ -1,0 +1,82 @@
+/*
+ * mupsi_oracle.h -- CPU restatement of the reference renderer's GPIS hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This library is the checker the parity tests,
+ * smoke() and bench.py's CPU-baseline leg use; the product never links it.
+ * Each function restates, in plain C, the reference function cited beside it.
+ * Parity of this restatement is pinned against the reference's own sources
+ * (compiled into oracle/_ref) and against the committed fixtures under
+ * tests/golden/.
+ *
+ * Buffers follow include/mupsi_gpu.h (the same structs), always host memory.
+ */
+#ifndef MUPSI_ORACLE_H
+#define MUPSI_ORACLE_H
+
+#include <stdint.h>
+
+#include "../include/mupsi_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* math/random.h:13-25 */
+uint32_t mo_make_seed4(uint32_t a, uint32_t b, uint32_t c, uint32_t d);
+uint32_t mo_make_seed5(uint32_t a, uint32_t b, uint32_t c, uint32_t d, uint32_t e);
+/* math/random.h:73-102: n draws of Random(seed) as u32 and as next1D() */
+void mo_random_stream(uint64_t seed, int n, uint32_t* out_u32, float* out_f);
+/* math/sampler.h:43-61 */
+void mo_constant_sampler(uint32_t seed, float* x, float* y, uint32_t* i);
+
+/* gp/gpnoise.cpp:51-87 + gpnoise.h:31,44; cond as in gpmedium.cpp:26-41 (no mean) */
+void mo_psi(const mupsi_kernel* k, int64_t n, const float* p, const uint32_t* seed, const mupsi_cond* cond,
+            float* out);
+/* Same impulses (positions from FP32 as the reference computes them), sums in FP64.
+ * out[n*4] doubles; also out_abs[n] = sum over impulses of |w*h| * sigma/sqrt(Var)
+ * (the conditioning scale of the value sum), nullable. */
+void mo_psi_f64(const mupsi_kernel* k, int64_t n, const float* p, const uint32_t* seed, double* out,
+                double* out_abs);
+/* Impulse listing for one (p, seed): positions s[27*ppc*3], weights w[27*ppc],
+ * cell indices cells[27*3], cell seeds cell_seed[27] (bit-exact quantities). */
+void mo_psi_impulses(const mupsi_kernel* k, const float* p, uint32_t seed, float* s, float* w, int32_t* cells,
+                     uint32_t* cell_seed);
+
+/* bvh/bvh.cpp:115-193 */
+int64_t mo_bvh_build(int64_t nv, const float* verts, int64_t nf, const int32_t* faces, uint32_t* nodes_out,
+                     uint32_t* tri_out, uint32_t* root);
+
+/* Scenes: the same descriptor the GPU library takes. */
+typedef struct mo_scene mo_scene;
+mo_scene* mo_scene_create(const mupsi_scene_desc* desc);
+void mo_scene_free(mo_scene* s);
+/* bvh.cpp:197-250 / :254-300 / :302-353 on scene mesh `mesh` (object space) */
+void mo_bvh_intersect(const mo_scene* s, int mesh, int64_t n, const mupsi_ray* rays, uint32_t* out_tri,
+                      float* out_tuv);
+void mo_bvh_occluded(const mo_scene* s, int mesh, int64_t n, const mupsi_ray* rays, uint8_t* out);
+void mo_bvh_closest(const mo_scene* s, int mesh, int64_t n, const float* p, uint32_t* out_tri, float* out_dq);
+/* mesh.cpp:325-362 (world space) */
+void mo_mesh_queries(const mo_scene* s, int mesh, int64_t n, const float* p, uint8_t* out_inside, uint32_t* out_tri,
+                     float* out_dq);
+/* meanfunction.cpp:13-39 */
+void mo_mean(const mo_scene* s, int medium, int64_t n, const float* p, float* out);
+/* gpmedium.cpp:19-41 */
+void mo_medium_eval(const mo_scene* s, int medium, int64_t n, const float* p, const uint32_t* seed,
+                    const mupsi_cond* cond, float* out);
+/* gpmedium.cpp:46-103 */
+void mo_sample_distance(const mo_scene* s, int medium, int64_t n, const mupsi_ray* rays, const uint32_t* seed,
+                        const mupsi_cond* cond, mupsi_medium_sample* out);
+/* gpmedium.cpp:133-161 */
+void mo_sample_condition(const mo_scene* s, int medium, int64_t n, const mupsi_medium_sample* samples,
+                         const uint32_t* seed, mupsi_cond* out);
+/* trace.cpp:118-213 with seed 42 (renderer.cpp:37); OpenMP over samples */
+void mo_trace(const mo_scene* s, int64_t n, const int32_t* x, const int32_t* y, const int32_t* k, float* out_rgb);
+/* Count the march steps and psi evaluations PathTracer::trace spends on samples
+ * (for roofline bookkeeping): out[0] = steps, out[1] = psi evaluations. */
+void mo_trace_work(const mo_scene* s, int64_t n, const int32_t* x, const int32_t* y, const int32_t* k,
+                   int64_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
