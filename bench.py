@@ -1,0 +1,327 @@
+"""GPIS path samples/s on B200: the configuration-0 render.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One step = one full render of the configuration-0 scene: 256x256 pixels x 20
+passes (1,310,720 path samples; sphere mean (0,0,-500) r=70 in a null sphere
+r=130, renewal_plus, SE kernel sigma 1 / length 1 / aniso (1,1,1), 3 points per
+cell, max_bounce 10, constant sky 1.0). Under torchrun every rank renders its
+own 20 passes (pass offset rank*20: weak scaling) and the framebuffers are
+summed with one all_reduce per step. Path state (~220 MB) exceeds the 126 MB L2
+and a 256 MB buffer is written between steps as well.
+
+`--impl reference` times the reference's own CPU implementation
+(oracle/_ref/libmupsi_ref_timing.so: its sources at -O3 with OpenMP; the C
+restatement of the oracle when that library is absent) on a strided pixel
+subset of the same scene at all 20 passes, with every host thread.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GPIS path samples/s (configuration-0 render)"
+UNIT = "samples/s"
+W, H, SPP = 256, 256, 20
+SAMPLES_PER_STEP = W * H * SPP
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=8.0, help="CPU work per reference/baseline step")
+    return ap.parse_args()
+
+
+def _config(extra=None):
+    c = {"workload": "config0: sphere-mean GPIS render 256x256x20spp, renewal_plus, sigma 1, length 1, "
+                     "aniso (1,1,1), 3 pts/cell, max_bounce 10, constant sky",
+         "width": W, "height": H, "spp": SPP, "max_bounce": 10, "l2": "state > L2 (126 MB) and 256 MB flush "
+                                                                       "between steps"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ------------------------------------------------------------------ CPU side
+def _cpu_info():
+    model = ""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return model, os.cpu_count()
+
+
+def _cpu_engine():
+    from oracle import bind
+    if bind.ref_available("ref_timing"):
+        return "reference", bind.RefOracle("ref_timing")
+    return "port", bind.PortOracle()
+
+
+def _cpu_scene(engine_kind, engine, scene):
+    if engine_kind == "reference":
+        td = tempfile.mkdtemp()
+        j, _ = scene.to_json()
+        jp = os.path.join(td, "config0.json")
+        with open(jp, "w") as fh:
+            json.dump(j, fh)
+        return engine.scene_load(jp, sky=1.0)
+    return engine.scene_create(scene.desc())
+
+
+def _cpu_samples(n, offset=0):
+    """n samples on a strided pixel subset, every pass of each pixel."""
+    npix = max(1, n // SPP)
+    stride = max(1, (W * H) // npix) | 1  # odd: the subset spreads over columns and rows
+    pix = (np.arange(npix) * stride + offset) % (W * H)
+    xs = np.repeat(pix % W, SPP).astype(np.int32)
+    ys = np.repeat(pix // W, SPP).astype(np.int32)
+    ks = np.tile(np.arange(SPP, dtype=np.int32), npix)
+    return xs, ys, ks, stride
+
+
+def cpu_rate(seconds, scene, steps=1, warmup=0):
+    """Time the CPU implementation on bounded strided samples; returns a dict."""
+    kind, eng = _cpu_engine()
+    h = _cpu_scene(kind, eng, scene)
+    xs, ys, ks, _ = _cpu_samples(SPP * 256)
+    t = time.perf_counter()
+    eng.trace(h, xs, ys, ks)
+    rate0 = len(xs) / (time.perf_counter() - t)
+    n = int(max(SPP * 16, rate0 * seconds))
+    times = []
+    for i in range(warmup + steps):
+        xs, ys, ks, stride = _cpu_samples(n, offset=i)
+        t = time.perf_counter()
+        eng.trace(h, xs, ys, ks)
+        if i >= warmup:
+            times.append(time.perf_counter() - t)
+    model, cores = _cpu_info()
+    threads = eng.num_threads() if kind == "reference" else cores
+    return {"value": len(xs) * len(times) / sum(times), "kind": kind, "cores": threads, "n": len(xs),
+            "stride": stride, "seconds": sum(times), "model": model,
+            "sample": f"{len(xs)} path samples per step: every {stride}th pixel (row-major) x all {SPP} passes of "
+                      f"the configuration-0 scene, {threads} OpenMP threads on {model}"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from mupsi_b200 import scene as S
+    r = cpu_rate(args.cpu_seconds, S.config0_scene(W, H, SPP), steps=args.steps, warmup=args.warmup)
+    line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * r["n"] / r["value"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": _config({"parallelism": "openmp", "sample": r["sample"]}),
+            "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
+                             "sample": r["sample"]},
+            "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU side
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.idx = device_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(device_index), "--query-gpu=" + self.FIELDS,
+                                       "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        rows = [[c.strip() for c in r] for r in rows if len(r) >= 9]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": float(rows[0][2]),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return json.load(fh), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+# Source-level operations per impulse evaluation of the march's psi sum (the
+# roofline unit): 4 PCG32 steps at 10 integer ops each (64-bit multiply-add as
+# three 32-bit multiply-adds plus carry, xorshift, rotate), 4 mantissa-trick
+# uniforms (shift/or + subtract), the impulse position (3 multiply + 3 add), the
+# weight compare/select, |p - s|^2 (3 sub, 3 mul, 2 add), the exponent scale
+# (1 mul), exp2 on the SFU (1), the signed accumulate (1): 40 integer + 25 float
+# = 65 issue slots, 1 of them on the SFU.
+OPS_PER_IMPULSE = 65
+
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    from mupsi_b200 import scene as S
+    from mupsi_b200.api import GpuRenderer, GpuScene
+    from mupsi_b200.lib import launch_count
+
+    stream = torch.cuda.current_stream()
+    sc = S.config0_scene(W, H, SPP)
+    gs = GpuScene(sc)
+    rend = GpuRenderer()
+    rend.prepare_render(gs)
+    fb = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    pass0 = rank * SPP
+
+    def step():
+        rend.start_render_progressive(pass0 + SPP, spp_begin=pass0, out=fb)
+        if world > 1:
+            dist.all_reduce(fb)
+
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        step()
+    torch.cuda.synchronize()
+    clocks = Clocks(local) if rank == 0 else None
+    time.sleep(0.3)
+    l0 = launch_count()
+    total_ms = 0.0
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for _ in range(args.steps):
+        flush.fill_(2)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = launch_count() - l0
+    time.sleep(0.2)
+    clk = clocks.stop() if clocks else None
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_per_step = t.item() / args.steps
+    value = SAMPLES_PER_STEP * world / (ms_per_step / 1000.0)
+
+    # roofline of the dominant kernel (the march), timed live with CUDA events
+    gs.profile(True)
+    gs.stats(reset=True)
+    for _ in range(2):
+        flush.fill_(3)
+        rend.start_render_progressive(pass0 + SPP, spp_begin=pass0, out=fb)
+    st = gs.stats(reset=True)
+    gs.profile(False)
+    peaks, peak_kind = _peaks()
+    mhz = float(peaks.get("sm_max_mhz", 1965.0))
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    peak_gimp = sms * 4 * 32 * mhz * 1e6 / OPS_PER_IMPULSE / 1e9  # 4 schedulers x 32 lanes, 1 issue/clock
+    achieved = st["impulse_evals"] / (st["march_ms"] / 1000.0) / 1e9 if st["march_ms"] > 0 else 0.0
+    roof = {"bound": "issue", "kernel": "k_march", "achieved": achieved, "peak": peak_gimp,
+            "unit": "Gimpulse-evals/s", "frac": achieved / peak_gimp, "traffic": None,
+            "peak_basis": f"{sms} SMs x 128 lanes x {mhz:.0f} MHz ({peak_kind} sm_max_mhz) / {OPS_PER_IMPULSE} "
+                          f"ops per impulse", "march_share": st["march_ms"] / max(1e-9, st["march_ms"] + st["shade_ms"]),
+            "launches": st["march_launches"], "ms_per_launch": st["march_ms"] / max(1, st["march_launches"]),
+            "impulse_evals_per_launch": st["impulse_evals"] / max(1, st["march_launches"]),
+            "psi_evals_per_sample": st["psi_evals"] / (2.0 * SAMPLES_PER_STEP),
+            "march_steps_per_sample": st["march_steps"] / (2.0 * SAMPLES_PER_STEP)}
+
+    # end to end through the public API with pinned host buffers: scene upload,
+    # render, framebuffer read back, release, every step
+    host_fb = torch.empty((H, W, 3), dtype=torch.float32, pin_memory=True).numpy()
+    e2e_times = []
+    desc_bytes = 0
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g2 = GpuScene(sc)
+        r2 = GpuRenderer()
+        r2.prepare_render(g2)
+        r2.start_render_progressive(pass0 + SPP, spp_begin=pass0, out=host_fb)
+        g2.close()
+        if i >= args.warmup:
+            e2e_times.append(time.perf_counter() - t0)
+    # bytes the scene create copies host->device: descriptor + march table (4001 floats)
+    desc_bytes = 4 * 4001 + 8192
+    e2e_t = torch.tensor([sum(e2e_times)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_val = SAMPLES_PER_STEP * world * len(e2e_times) / e2e_t.item()
+
+    cpu = None
+    if rank == 0 and world == 1:
+        r = cpu_rate(args.cpu_seconds, sc, steps=1, warmup=0)
+        cpu = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"], "sample": r["sample"]}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": _config({"parallelism": f"spp-sharded x{world}" if world > 1 else "single GPU",
+                                   "global_batch": SAMPLES_PER_STEP * world}),
+                "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": desc_bytes,
+                        "d2h_bytes_per_step": W * H * 3 * 4},
+                "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clk}
+        print(json.dumps(line), flush=True)
+    gs.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = _args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

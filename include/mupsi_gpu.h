@@ -233,7 +233,9 @@ int mupsi_gpu_trace_samples(mupsi_scene* scene, int64_t n, const int32_t* x, con
  * passes k in [spp_begin, spp_end) are traced and accumulated into the scene's
  * running per-pixel sum (Framebuffer::accumulate, framebuffer.cpp:28-35), in
  * pass order. After the call rgb_out[h*w*3] holds sum / passes-so-far (row y =
- * camera y, as Controller::copyDisplayRawTo). spp_begin == 0 resets the sum.
+ * camera y, as Controller::copyDisplayRawTo). A call continues the running sum
+ * when spp_begin equals the previous call's spp_end; otherwise (and always for
+ * spp_begin == 0) it starts a new image.
  * cancel (nullable) is polled between waves of passes; on_spp (nullable) is
  * called with the number of completed passes after each wave.
  * moments_out (nullable, h*w*6 doubles) receives per pixel the FP64 sum and
@@ -250,6 +252,26 @@ typedef struct {
   void* stream;
 } mupsi_render_args;
 int mupsi_gpu_render(mupsi_scene* scene, const mupsi_render_args* args);
+
+/* ------------------------------------------------------ instrumentation -- */
+
+/* Work and device time of the wavefront kernels, for roofline reporting. The
+ * reference prints only a progress percentage (renderer.h:33-37); this is the
+ * GPU path's counterpart. Counting and timing are off until enabled. */
+typedef struct {
+  uint64_t march_steps;   /* march steps visited (mean function evaluated) */
+  uint64_t psi_evals;     /* psi value evaluations inside marches */
+  uint64_t impulse_evals; /* sum over those of 27 * points_per_cell */
+  uint64_t marches;       /* rays marched */
+  double march_ms;        /* device time of the march kernels (CUDA events on the launch stream) */
+  double shade_ms;        /* device time of the shading kernels */
+  int64_t march_launches;
+  int64_t shade_launches;
+} mupsi_render_stats;
+/* enable != 0 starts counting work and timing kernels on later renders. */
+int mupsi_gpu_scene_profile(mupsi_scene* scene, int32_t enable);
+/* Copy the accumulated statistics; reset != 0 clears them afterwards. */
+int mupsi_gpu_scene_stats(mupsi_scene* scene, mupsi_render_stats* out, int32_t reset);
 
 #ifdef __cplusplus
 }

@@ -129,3 +129,16 @@ class RenderArgs(C.Structure):
 
 
 assert C.sizeof(Cond) == 32 and C.sizeof(Ray) == 32 and C.sizeof(MediumSample) == 32
+
+
+class RenderStats(C.Structure):
+    _fields_ = [
+        ("march_steps", C.c_uint64),
+        ("psi_evals", C.c_uint64),
+        ("impulse_evals", C.c_uint64),
+        ("marches", C.c_uint64),
+        ("march_ms", C.c_double),
+        ("shade_ms", C.c_double),
+        ("march_launches", C.c_int64),
+        ("shade_launches", C.c_int64),
+    ]

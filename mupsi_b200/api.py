@@ -1,0 +1,330 @@
+"""Host-side mirror of the reference renderer's interfaces, backed by the GPU library.
+
+Names and argument meaning follow the reference (src/gp, src/medium, src/bvh,
+src/rendering); every call is a batch over numpy arrays (host memory) or CUDA
+torch tensors (device memory) and goes through the C ABI in include/mupsi_gpu.h.
+Errors raise MupsiError with the library's message, the counterpart of the
+reference's bool + std::cerr returns.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from .lib import check, load
+from .scene import Scene
+
+try:  # torch is optional plumbing: device buffers and streams
+    import torch
+except Exception:  # pragma: no cover
+    torch = None
+
+
+def _is_dev(a):
+    return torch is not None and isinstance(a, torch.Tensor) and a.is_cuda
+
+
+def _mem(*arrays):
+    kinds = {_is_dev(a) for a in arrays if a is not None}
+    if len(kinds) > 1:
+        raise ValueError("all buffers of one call must be host (numpy) or all device (CUDA tensors)")
+    return _abi.MEM_DEVICE if kinds == {True} else _abi.MEM_HOST
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if _is_dev(a):
+        if not a.is_contiguous():
+            raise ValueError("device buffers must be contiguous")
+        return a.data_ptr()
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("host buffers must be C-contiguous")
+    return a.ctypes.data
+
+
+def _stream(stream):
+    if stream is not None:
+        return stream
+    if torch is not None and torch.cuda.is_available():
+        return torch.cuda.current_stream().cuda_stream
+    return None
+
+
+def _empty(like_dev, shape, dtype):
+    if like_dev:
+        tdt = {np.float32: torch.float32, np.uint32: torch.int32, np.uint8: torch.uint8}[dtype]
+        return torch.empty(shape, dtype=tdt, device="cuda")
+    return np.empty(shape, dtype=dtype)
+
+
+def _host(a, dtype):
+    if _is_dev(a):
+        return a.contiguous()
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def cond_records(cond):
+    """(n, 8) [C xyz, u, g xyz, active] -> GPConditioningState records (mupsi_cond)."""
+    if cond is None:
+        return None
+    if _is_dev(cond):
+        c = cond.float().contiguous().clone()
+        c.view(torch.int32)[:, 7] = (cond[:, 7] != 0).int()
+        return c
+    cond = np.ascontiguousarray(cond, np.float32)
+    out = cond.copy()
+    out.view(np.uint32)[:, 7] = (cond[:, 7] != 0).astype(np.uint32)
+    return out
+
+
+class SparseSEKernel:
+    """SparseSEKernel(sigma, kernelRadius, lengthScale) (gp/kernel.h:39-78)."""
+
+    def __init__(self, sigma, kernel_radius, length_scale=(1.0, 1.0, 1.0)):
+        self.sigma = float(sigma)
+        self.kernel_radius = float(kernel_radius)
+        self.length_scale = tuple(float(v) for v in length_scale)
+
+    def struct(self, impulse_density):
+        return _abi.Kernel(self.sigma, self.kernel_radius, _abi.f3(*self.length_scale), int(impulse_density))
+
+
+class SparseGPNoiseGenerator:
+    """SparseGPNoiseGenerator(kernel, impulseDensity) (gp/gpnoise.h:23-49), batched on the GPU."""
+
+    def __init__(self, kernel, impulse_density):
+        self.kernel = kernel
+        self.impulse_density = int(impulse_density)
+        self._k = kernel.struct(impulse_density)
+
+    def raw_noise(self, p, seed, cond=None, out=None, stream=None):
+        """RawNoise(p, seed) for n points -> (n, 4) (psi, grad psi); with `cond`
+        ((n, 8) [C, u_tilde, g_tilde, active]) the Renewal+ terms are added."""
+        p = _host(p, np.float32)
+        seed = _host(seed, np.uint32)
+        n = p.shape[0]
+        c = cond_records(cond)
+        mem = _mem(p, seed, c, out)
+        if out is None:
+            out = _empty(mem == _abi.MEM_DEVICE, (n, 4), np.float32)
+        check(load().mupsi_gpu_psi(C.byref(self._k), n, _ptr(p), _ptr(seed), _ptr(c), _ptr(out), mem,
+                                   _stream(stream)))
+        return out
+
+    def raw_noise_value(self, p, seed, cond=None, out=None, stream=None):
+        p = _host(p, np.float32)
+        seed = _host(seed, np.uint32)
+        n = p.shape[0]
+        c = cond_records(cond)
+        mem = _mem(p, seed, c, out)
+        if out is None:
+            out = _empty(mem == _abi.MEM_DEVICE, (n,), np.float32)
+        check(load().mupsi_gpu_psi_value(C.byref(self._k), n, _ptr(p), _ptr(seed), _ptr(c), _ptr(out), mem,
+                                         _stream(stream)))
+        return out
+
+
+def bvh_build_host(vertices, faces):
+    """BVH::build node array (bvh.cpp:115-193) from the library's host builder:
+    (nodes (count, 8) u32 words, triIndices, root)."""
+    v = np.ascontiguousarray(vertices, np.float32)
+    f = np.ascontiguousarray(faces, np.int32)
+    nodes = np.zeros((max(2 * len(f), 1), 8), np.uint32)
+    idx = np.zeros(max(len(f), 1), np.uint32)
+    cnt, root = C.c_int64(), C.c_uint32()
+    check(load().mupsi_bvh_build_host(len(v), v.ctypes.data, len(f), f.ctypes.data, nodes.ctypes.data,
+                                      idx.ctypes.data, C.byref(cnt), C.byref(root)))
+    return nodes[: cnt.value], idx[: len(f)], root.value
+
+
+class DeviceMesh:
+    """A Mesh with its BVH on the device (primitives/mesh.h, bvh/bvh.h)."""
+
+    def __init__(self, vertices, faces, vertex_normals=None, position=(0, 0, 0), scale=1.0):
+        from .scene import Mesh
+        self._mesh = Mesh(vertices, faces, vertex_normals, position, scale)
+        self._desc = self._mesh.desc()
+        h = C.c_void_p()
+        check(load().mupsi_gpu_mesh_create(C.byref(self._desc), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            load().mupsi_gpu_mesh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def intersect(self, rays, stream=None):
+        """BVH::intersect: rays (n, 8) [o, d, nearT, farT] -> (tri u32 (0xFFFFFFFF miss), (t, u, v))."""
+        rays = _host(rays, np.float32)
+        n = rays.shape[0]
+        mem = _mem(rays)
+        dev = mem == _abi.MEM_DEVICE
+        tri, tuv = _empty(dev, (n,), np.uint32), _empty(dev, (n, 3), np.float32)
+        check(load().mupsi_gpu_bvh_intersect(self.h, n, _ptr(rays), _ptr(tri), _ptr(tuv), mem, _stream(stream)))
+        return tri, tuv
+
+    def occluded(self, rays, stream=None):
+        rays = _host(rays, np.float32)
+        n = rays.shape[0]
+        mem = _mem(rays)
+        out = _empty(mem == _abi.MEM_DEVICE, (n,), np.uint8)
+        check(load().mupsi_gpu_bvh_occluded(self.h, n, _ptr(rays), _ptr(out), mem, _stream(stream)))
+        return out
+
+    def closest(self, p, stream=None):
+        """BVH::closest: p (n, 3) -> (tri, (dist, q xyz))"""
+        p = _host(p, np.float32)
+        n = p.shape[0]
+        mem = _mem(p)
+        dev = mem == _abi.MEM_DEVICE
+        tri, dq = _empty(dev, (n,), np.uint32), _empty(dev, (n, 4), np.float32)
+        check(load().mupsi_gpu_bvh_closest(self.h, n, _ptr(p), _ptr(tri), _ptr(dq), mem, _stream(stream)))
+        return tri, dq
+
+    def queries(self, p, stream=None):
+        """Mesh::inside and Mesh::distToPoint: -> (inside u8, tri, (dist, q xyz))"""
+        p = _host(p, np.float32)
+        n = p.shape[0]
+        mem = _mem(p)
+        dev = mem == _abi.MEM_DEVICE
+        ins, tri, dq = _empty(dev, (n,), np.uint8), _empty(dev, (n,), np.uint32), _empty(dev, (n, 4), np.float32)
+        check(load().mupsi_gpu_mesh_queries(self.h, n, _ptr(p), _ptr(ins), _ptr(tri), _ptr(dq), mem,
+                                            _stream(stream)))
+        return ins, tri, dq
+
+
+class GpuScene:
+    """A scene on the device: the RenderContext plus GPMedium/MeanFunction batch probes."""
+
+    def __init__(self, scene: Scene):
+        self.scene = scene
+        self._desc = scene.desc()
+        h = C.c_void_p()
+        check(load().mupsi_gpu_scene_create(C.byref(self._desc), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            load().mupsi_gpu_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def mean(self, medium, p, stream=None):
+        """MeanFunction eval + gradient -> (n, 4)"""
+        p = _host(p, np.float32)
+        mem = _mem(p)
+        out = _empty(mem == _abi.MEM_DEVICE, (p.shape[0], 4), np.float32)
+        check(load().mupsi_gpu_mean(self.h, medium, p.shape[0], _ptr(p), _ptr(out), mem, _stream(stream)))
+        return out
+
+    def eval_with_gradient(self, medium, p, seed, cond=None, stream=None):
+        """GPMedium::evalWithGradient(p, seed, state) -> (n, 4)"""
+        p = _host(p, np.float32)
+        seed = _host(seed, np.uint32)
+        c = cond_records(cond)
+        mem = _mem(p, seed, c)
+        out = _empty(mem == _abi.MEM_DEVICE, (p.shape[0], 4), np.float32)
+        check(load().mupsi_gpu_medium_eval(self.h, medium, p.shape[0], _ptr(p), _ptr(seed), _ptr(c), _ptr(out), mem,
+                                           _stream(stream)))
+        return out
+
+    def sample_distance(self, medium, rays, seed, cond=None, stream=None):
+        """GPMedium::sampleDistance -> (n, 8) [exited, t, p xyz, normal xyz] (exited as float)."""
+        rays = _host(rays, np.float32)
+        seed = _host(seed, np.uint32)
+        c = cond_records(cond)
+        mem = _mem(rays, seed, c)
+        out = _empty(mem == _abi.MEM_DEVICE, (rays.shape[0], 8), np.float32)
+        check(load().mupsi_gpu_sample_distance(self.h, medium, rays.shape[0], _ptr(rays), _ptr(seed), _ptr(c),
+                                               _ptr(out), mem, _stream(stream)))
+        if mem == _abi.MEM_DEVICE:
+            res = out.clone()
+            res[:, 0] = out.view(torch.int32)[:, 0].float()
+            return res
+        res = out.copy()
+        res[:, 0] = out.view(np.uint32)[:, 0].astype(np.float32)
+        return res
+
+    def sample_condition(self, medium, samples, seed, stream=None):
+        """GPMedium::sampleCondition: samples (n, 7) [exited, p xyz, normal xyz] -> (n, 8) [C, u, g, active]."""
+        samples = np.asarray(samples, np.float32)
+        seed = np.ascontiguousarray(seed, np.uint32)
+        n = samples.shape[0]
+        ms = np.zeros((n, 8), np.float32)
+        ms.view(np.uint32)[:, 0] = samples[:, 0].astype(np.uint32)
+        ms[:, 2:5] = samples[:, 1:4]
+        ms[:, 5:8] = samples[:, 4:7]
+        out = np.zeros((n, 8), np.float32)
+        check(load().mupsi_gpu_sample_condition(self.h, medium, n, ms.ctypes.data, seed.ctypes.data, out.ctypes.data,
+                                                _abi.MEM_HOST, _stream(stream)))
+        res = out.copy()
+        res[:, 7] = out.view(np.uint32)[:, 7].astype(np.float32)
+        return res
+
+    def profile(self, enable=True):
+        """Count march work and time the wavefront kernels with CUDA events."""
+        check(load().mupsi_gpu_scene_profile(self.h, 1 if enable else 0))
+
+    def stats(self, reset=False):
+        st = _abi.RenderStats()
+        check(load().mupsi_gpu_scene_stats(self.h, C.byref(st), 1 if reset else 0))
+        return {f: getattr(st, f) for f, _ in _abi.RenderStats._fields_}
+
+    def trace(self, x, y, k, stream=None):
+        """PathTracer::trace(pixel (x, y), ctx, 42, k) for n samples -> (n, 3) radiance."""
+        x, y, k = (_host(a, np.int32) for a in (x, y, k))
+        mem = _mem(x, y, k)
+        n = x.shape[0]
+        if mem == _abi.MEM_DEVICE:
+            out = torch.empty((n, 3), dtype=torch.float32, device="cuda")
+        else:
+            out = np.empty((n, 3), np.float32)
+        check(load().mupsi_gpu_trace_samples(self.h, n, _ptr(x), _ptr(y), _ptr(k), _ptr(out), mem, _stream(stream)))
+        return out
+
+
+class GpuRenderer:
+    """Renderer (rendering/renderer.h:11-41) on the GPU: prepare_render + start_render_progressive."""
+
+    def __init__(self):
+        self.scene = None
+        self.cancel_flag = C.c_int32(0)
+
+    def prepare_render(self, scene):
+        self.scene = scene if isinstance(scene, GpuScene) else GpuScene(scene)
+        return self.scene
+
+    def cancel(self):
+        self.cancel_flag.value = 1
+
+    def start_render_progressive(self, target_spp, on_spp=None, spp_begin=0, out=None, moments=False, stream=None):
+        """Trace passes [spp_begin, target_spp) and return the averaged framebuffer
+        (h, w, 3) (and FP64 moments (h, w, 6) if asked). Returns None if cancelled,
+        as the reference returns false."""
+        s = self.scene.scene
+        h, w = s.height, s.width
+        dev = out is not None and _is_dev(out)
+        if out is None:
+            out = np.empty((h, w, 3), np.float32)
+        mom = np.zeros((h, w, 6), np.float64) if moments else None
+        cb = _abi.ON_SPP(lambda k, user: on_spp(k)) if on_spp else _abi.ON_SPP()
+        args = _abi.RenderArgs(spp_begin, target_spp, C.pointer(self.cancel_flag), cb, None, _ptr(out),
+                               _abi.MEM_DEVICE if dev else _abi.MEM_HOST, None if mom is None else mom.ctypes.data,
+                               _stream(stream))
+        code = load().mupsi_gpu_render(self.scene.h, C.byref(args))
+        if code == _abi.ERR_CANCELLED:
+            return None
+        check(code)
+        return (out, mom) if moments else out

@@ -1,0 +1,493 @@
+// Library core: error state, launch accounting, transforms, the batched GP-noise
+// entry points and the mesh/BVH entry points of include/mupsi_gpu.h.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "core.cuh"
+
+namespace mupsi {
+
+static thread_local std::string g_last_error;
+static std::atomic<int64_t> g_launches{0};
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+void clear_error() { g_last_error.clear(); }
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+HostM4 translate_scale(const float t[3], float s) {
+  HostM4 r;
+  std::memset(r.m, 0, sizeof r.m);
+  r.m[0] = s;
+  r.m[5] = s;
+  r.m[10] = s;
+  r.m[15] = 1.0f;
+  r.m[12] = t[0];
+  r.m[13] = t[1];
+  r.m[14] = t[2];
+  return r;
+}
+static float det3(const float a[9]) {
+  return a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) + a[2] * (a[3] * a[7] - a[4] * a[6]);
+}
+HostM4 inverse4(const HostM4& a) {
+  auto at = [&](int i, int j) { return a.m[j * 4 + i]; };
+  float cof[4][4];
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) {
+      float sub[9];
+      int ra = 0;
+      for (int r = 0; r < 4; ++r) {
+        if (r == i) continue;
+        int cb = 0;
+        for (int c = 0; c < 4; ++c) {
+          if (c == j) continue;
+          sub[ra * 3 + cb] = at(r, c);
+          ++cb;
+        }
+        ++ra;
+      }
+      float minor = det3(sub);
+      cof[i][j] = ((i + j) % 2 == 0) ? minor : -minor;
+    }
+  float det = 0.0f;
+  for (int j = 0; j < 4; ++j) det += at(0, j) * cof[0][j];
+  HostM4 r;
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) r.m[i * 4 + j] = cof[i][j] / det;
+  return r;
+}
+static bool ident(const HostM4& a, int n) {
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) {
+      float v = a.m[j * 4 + i];
+      if (i == j) {
+        float lim = 1e-5f * std::min(std::fabs(v), 1.0f);
+        if (!(std::fabs(v - 1.0f) <= lim)) return false;
+      } else if (!(std::fabs(v) <= 1e-5f)) {
+        return false;
+      }
+    }
+  return true;
+}
+bool is_identity4(const HostM4& a) { return ident(a, 4); }
+bool is_identity3(const HostM4& a) { return ident(a, 3); }
+
+KParams make_kparams(const mupsi_kernel& k) {
+  KParams p;
+  p.sigma = k.sigma;
+  p.kr = k.kernel_radius;
+  p.L2 = k.aniso[0] * k.aniso[0] + (k.aniso[1] * k.aniso[1] + k.aniso[2] * k.aniso[2]);
+  p.ppc = k.points_per_cell;
+  // Var() (gpnoise.h:31): int / std::pow(float, int) -> double, * pow(pi, 1.5), returned as float
+  float var = (float)(((double)p.ppc / std::pow((double)p.kr, 3.0)) * std::pow(M_PI, 1.5));
+  p.sqrt_var = std::sqrt(var);
+  p.k2 = (float)(-1.4426950408889634 / (double)p.L2);
+  p.c2 = -2.0f / p.L2;
+  p.c4 = 4.0f / (p.L2 * p.L2);
+  p.psi_bound = (float)((double)p.sigma * 27.0 * p.ppc / (double)p.sqrt_var);
+  p.gradh_max = (float)(std::sqrt(2.0 / (double)p.L2) * std::exp(-0.5));
+  return p;
+}
+
+int check_kernel(const mupsi_kernel* k) {
+  if (!k) return fail(MUPSI_ERR_INVALID, "kernel is null");
+  if (!(k->kernel_radius > 0.0f) || !std::isfinite(k->kernel_radius))
+    return fail(MUPSI_ERR_INVALID, "kernel_radius must be a positive finite number");
+  if (k->points_per_cell < 0 || k->points_per_cell > 4096)
+    return fail(MUPSI_ERR_INVALID, "points_per_cell must be in [0, 4096]");
+  float L2 = k->aniso[0] * k->aniso[0] + (k->aniso[1] * k->aniso[1] + k->aniso[2] * k->aniso[2]);
+  if (!(L2 > 0.0f) || !std::isfinite(L2)) return fail(MUPSI_ERR_INVALID, "aniso must have a positive norm");
+  return MUPSI_OK;
+}
+
+cudaStream_t resolve_stream(void* s) {
+  if (s) return (cudaStream_t)s;
+  static cudaStream_t internal = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] { cudaStreamCreateWithFlags(&internal, cudaStreamNonBlocking); });
+  return internal;
+}
+
+int num_sms() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+// ------------------------------------------------------------ GP noise batch
+template <bool GRAD>
+__global__ void __launch_bounds__(256) k_psi(KParams k, int64_t n, const float* __restrict__ p,
+                                             const uint32_t* __restrict__ seed, const Cond* __restrict__ cond,
+                                             float* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    v3 P = v3{p[3 * i], p[3 * i + 1], p[3 * i + 2]};
+    uint32_t s = seed[i];
+    if (GRAD) {
+      float4 f = raw_noise(k, P, s);
+      if (cond) f = add_cond(k, cond[i], P, f);
+      out[4 * i] = f.x;
+      out[4 * i + 1] = f.y;
+      out[4 * i + 2] = f.z;
+      out[4 * i + 3] = f.w;
+    } else {
+      float v = raw_noise_value(k, P, s);
+      if (cond && cond[i].active) v += cond_value(k, cond[i], P);
+      out[i] = v;
+    }
+  }
+}
+
+static int psi_common(bool grad, const mupsi_kernel* kernel, int64_t n, const float* p, const uint32_t* seed,
+                      const mupsi_cond* cond, float* out, mupsi_mem mem, void* stream) {
+  clear_error();
+  if (int e = check_kernel(kernel)) return e;
+  if (n < 0) return fail(MUPSI_ERR_INVALID, "n must be >= 0");
+  if (n == 0) return MUPSI_OK;
+  if (!p || !seed || !out) return fail(MUPSI_ERR_INVALID, "null buffer");
+  cudaStream_t st = resolve_stream(stream);
+  KParams k = make_kparams(*kernel);
+  const int ocomp = grad ? 4 : 1;
+  Staged<float> dp(st), dout(st);
+  Staged<uint32_t> ds(st);
+  Staged<mupsi_cond> dc(st);
+  MUPSI_CUDA(dp.in(p, 3 * n, mem));
+  MUPSI_CUDA(ds.in(seed, n, mem));
+  if (cond) MUPSI_CUDA(dc.in(cond, n, mem));
+  MUPSI_CUDA(dout.out(out, ocomp * n, mem));
+  int64_t blocks = std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 64);
+  const Cond* cptr = cond ? reinterpret_cast<const Cond*>(dc.ptr) : nullptr;
+  if (grad)
+    k_psi<true><<<(unsigned)blocks, 256, 0, st>>>(k, n, dp.ptr, ds.ptr, cptr, dout.ptr);
+  else
+    k_psi<false><<<(unsigned)blocks, 256, 0, st>>>(k, n, dp.ptr, ds.ptr, cptr, dout.ptr);
+  count_launch();
+  MUPSI_CUDA(cudaGetLastError());
+  MUPSI_CUDA(dout.finish());
+  MUPSI_CUDA(cudaStreamSynchronize(st));
+  return MUPSI_OK;
+}
+
+// ------------------------------------------------------------ meshes / BVH
+struct MeshStore {
+  DMesh d;
+  std::vector<void*> allocs;
+  ~MeshStore() {
+    for (void* p : allocs) cudaFree(p);
+  }
+};
+
+template <typename T>
+static cudaError_t upload(std::vector<void*>& allocs, const T* src, size_t count, const T*& dst) {
+  if (count == 0) {
+    dst = nullptr;
+    return cudaSuccess;
+  }
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+  if (e != cudaSuccess) return e;
+  allocs.push_back(p);
+  e = cudaMemcpy(p, src, count * sizeof(T), cudaMemcpyHostToDevice);
+  dst = static_cast<const T*>(p);
+  return e;
+}
+
+int make_device_mesh(const mupsi_mesh_desc& md, DMesh& d, std::vector<void*>& allocs) {
+  if (md.num_vertices < 0 || md.num_faces < 0) return fail(MUPSI_ERR_INVALID, "negative mesh size");
+  if ((md.num_vertices > 0 && !md.vertices) || (md.num_faces > 0 && !md.faces))
+    return fail(MUPSI_ERR_INVALID, "mesh arrays are null");
+  if (md.num_faces > 0x3FFFFFFF) return fail(MUPSI_ERR_INVALID, "too many faces");
+  for (int64_t i = 0; i < 3 * md.num_faces; ++i)
+    if (md.faces[i] < 0 || md.faces[i] >= md.num_vertices) return fail(MUPSI_ERR_INVALID, "face index out of range");
+  std::vector<HostNode> nodes;
+  std::vector<uint32_t> idx;
+  uint32_t root = build_bvh(md.vertices, md.faces, md.num_faces, nodes, idx);
+  // face normals and the light-sampling CDF (mesh.cpp:140-154, :308-318)
+  std::vector<float> fn(3 * md.num_faces), cdf(md.num_faces);
+  float total = 0.0f;
+  for (int64_t i = 0; i < md.num_faces; ++i) {
+    const int32_t* f = md.faces + 3 * i;
+    v3 a = ld3(md.vertices + 3 * (int64_t)f[0]), b = ld3(md.vertices + 3 * (int64_t)f[1]),
+       c = ld3(md.vertices + 3 * (int64_t)f[2]);
+    v3 n = cross(b - a, c - a);
+    float len = norm3(n);
+    v3 un = len > 1e-12f ? n / len : mk3(0, 0, 0);
+    st3(&fn[3 * i], un);
+    total += 0.5f * len;
+    cdf[i] = total;
+  }
+  if (total > 0.0f)
+    for (auto& c : cdf) c /= total;
+  std::memset(&d, 0, sizeof d);
+  const BNode* dn = nullptr;
+  cudaError_t e;
+  if ((e = upload(allocs, reinterpret_cast<const BNode*>(nodes.data()), nodes.size(), dn)) != cudaSuccess ||
+      (e = upload(allocs, idx.data(), idx.size(), d.tri_idx)) != cudaSuccess ||
+      (e = upload(allocs, md.faces, 3 * md.num_faces, d.faces)) != cudaSuccess ||
+      (e = upload(allocs, md.vertices, 3 * md.num_vertices, d.verts)) != cudaSuccess ||
+      (e = upload(allocs, fn.data(), fn.size(), d.face_n)) != cudaSuccess ||
+      (e = upload(allocs, cdf.data(), cdf.size(), d.cdf)) != cudaSuccess)
+    return fail(e == cudaErrorMemoryAllocation ? MUPSI_ERR_OOM : MUPSI_ERR_CUDA,
+                std::string("mesh upload: ") + cudaGetErrorString(e));
+  if (md.vertex_normals) {
+    if ((e = upload(allocs, md.vertex_normals, 3 * md.num_vertices, d.vert_n)) != cudaSuccess)
+      return fail(MUPSI_ERR_CUDA, std::string("mesh upload: ") + cudaGetErrorString(e));
+  }
+  d.nodes = dn;
+  d.num_nodes = (int64_t)nodes.size();
+  d.num_faces = md.num_faces;
+  d.root = root;
+  d.total_area = total;
+  HostM4 T = translate_scale(md.position, md.scale), Ti = inverse4(T);
+  std::memcpy(d.T.m, T.m, sizeof T.m);
+  std::memcpy(d.Tinv.m, Ti.m, sizeof Ti.m);
+  d.identity = is_identity4(Ti);
+  d.normal_identity = is_identity3(Ti);
+  return MUPSI_OK;
+}
+
+__global__ void k_bvh_intersect(DMesh m, int64_t n, const mupsi_ray* rays, uint32_t* out_tri, float* out_tuv,
+                                int* err) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const mupsi_ray& q = rays[i];
+    Ray r = make_ray(ld3(q.o), ld3(q.d));
+    r.nt = q.near_t;
+    r.ft = q.far_t;
+    uint32_t tri = 0;
+    float u = 0, v = 0;
+    bool ovf = false;
+    bool h = bvh_intersect(m, r, tri, u, v, ovf);
+    if (ovf) atomicOr(err, 1);
+    out_tri[i] = h ? tri : 0xFFFFFFFFu;
+    out_tuv[3 * i] = h ? r.ft : -1.0f;
+    out_tuv[3 * i + 1] = h ? u : 0.0f;
+    out_tuv[3 * i + 2] = h ? v : 0.0f;
+  }
+}
+__global__ void k_bvh_occluded(DMesh m, int64_t n, const mupsi_ray* rays, uint8_t* out, int* err) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const mupsi_ray& q = rays[i];
+    Ray r = make_ray(ld3(q.o), ld3(q.d));
+    r.nt = q.near_t;
+    r.ft = q.far_t;
+    bool ovf = false;
+    out[i] = bvh_occluded(m, r, ovf) ? 1 : 0;
+    if (ovf) atomicOr(err, 1);
+  }
+}
+__global__ void k_bvh_closest(DMesh m, int64_t n, const float* p, uint32_t* out_tri, float* out_dq, int* err) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t tri = 0xFFFFFFFFu;
+    v3 q = mk3(0, 0, 0);
+    bool ovf = false;
+    float d = bvh_closest(m, ld3(p + 3 * i), tri, q, ovf);
+    if (ovf) atomicOr(err, 1);
+    out_tri[i] = tri;
+    out_dq[4 * i] = d;
+    out_dq[4 * i + 1] = q.x;
+    out_dq[4 * i + 2] = q.y;
+    out_dq[4 * i + 3] = q.z;
+  }
+}
+__global__ void k_mesh_queries(DMesh m, int64_t n, const float* p, uint8_t* out_inside, uint32_t* out_tri,
+                               float* out_dq, int* err) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    v3 P = ld3(p + 3 * i);
+    bool ovf = false;
+    out_inside[i] = mesh_inside(m, P, ovf) ? 1 : 0;
+    uint32_t tri = 0xFFFFFFFFu;
+    v3 q = mk3(0, 0, 0);
+    out_dq[4 * i] = mesh_dist(m, P, tri, q, ovf);
+    out_tri[i] = tri;
+    out_dq[4 * i + 1] = q.x;
+    out_dq[4 * i + 2] = q.y;
+    out_dq[4 * i + 3] = q.z;
+    if (ovf) atomicOr(err, 1);
+  }
+}
+
+}  // namespace mupsi
+
+struct mupsi_mesh {
+  mupsi::MeshStore store;
+};
+
+using namespace mupsi;
+
+static int grid_for(int64_t n) { return (int)std::min<int64_t>((n + 127) / 128, (int64_t)num_sms() * 32); }
+
+// Device error word for one batch call: allocated, cleared, read back.
+struct ErrWord {
+  int* d = nullptr;
+  cudaStream_t s;
+  explicit ErrWord(cudaStream_t st) : s(st) {}
+  cudaError_t init() {
+    cudaError_t e = cudaMallocAsync((void**)&d, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    return cudaMemsetAsync(d, 0, sizeof(int), s);
+  }
+  int read() {
+    int h = 0;
+    cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    return h;
+  }
+  ~ErrWord() {
+    if (d) cudaFreeAsync(d, s);
+  }
+};
+
+extern "C" {
+
+const char* mupsi_gpu_last_error(void) { return g_last_error.c_str(); }
+int32_t mupsi_gpu_abi_version(void) { return MUPSI_GPU_ABI_VERSION; }
+int64_t mupsi_gpu_launch_count(void) { return g_launches.load(); }
+
+int mupsi_gpu_psi(const mupsi_kernel* kernel, int64_t n, const float* p, const uint32_t* seed, const mupsi_cond* cond,
+                  float* out, mupsi_mem mem, void* stream) {
+  return psi_common(true, kernel, n, p, seed, cond, out, mem, stream);
+}
+int mupsi_gpu_psi_value(const mupsi_kernel* kernel, int64_t n, const float* p, const uint32_t* seed,
+                        const mupsi_cond* cond, float* out, mupsi_mem mem, void* stream) {
+  return psi_common(false, kernel, n, p, seed, cond, out, mem, stream);
+}
+
+int mupsi_bvh_build_host(int64_t num_vertices, const float* vertices, int64_t num_faces, const int32_t* faces,
+                         uint32_t* nodes_out, uint32_t* tri_indices_out, int64_t* num_nodes, uint32_t* root) {
+  clear_error();
+  if (num_faces < 0 || num_vertices < 0) return fail(MUPSI_ERR_INVALID, "negative size");
+  if ((num_faces && (!faces || !vertices)) || !nodes_out || !tri_indices_out || !num_nodes || !root)
+    return fail(MUPSI_ERR_INVALID, "null buffer");
+  for (int64_t i = 0; i < 3 * num_faces; ++i)
+    if (faces[i] < 0 || faces[i] >= num_vertices) return fail(MUPSI_ERR_INVALID, "face index out of range");
+  std::vector<HostNode> nodes;
+  std::vector<uint32_t> idx;
+  *root = build_bvh(vertices, faces, num_faces, nodes, idx);
+  *num_nodes = (int64_t)nodes.size();
+  if (!nodes.empty()) std::memcpy(nodes_out, nodes.data(), nodes.size() * sizeof(HostNode));
+  if (!idx.empty()) std::memcpy(tri_indices_out, idx.data(), idx.size() * sizeof(uint32_t));
+  return MUPSI_OK;
+}
+
+int mupsi_gpu_mesh_create(const mupsi_mesh_desc* desc, mupsi_mesh** out) {
+  clear_error();
+  if (!desc || !out) return fail(MUPSI_ERR_INVALID, "null argument");
+  auto* m = new mupsi_mesh();
+  int e = make_device_mesh(*desc, m->store.d, m->store.allocs);
+  if (e) {
+    delete m;
+    return e;
+  }
+  *out = m;
+  return MUPSI_OK;
+}
+void mupsi_gpu_mesh_destroy(mupsi_mesh* mesh) { delete mesh; }
+
+int mupsi_gpu_bvh_intersect(const mupsi_mesh* mesh, int64_t n, const mupsi_ray* rays, uint32_t* out_tri,
+                            float* out_tuv, mupsi_mem mem, void* stream) {
+  clear_error();
+  if (!mesh || n < 0) return fail(MUPSI_ERR_INVALID, "bad argument");
+  if (n == 0) return MUPSI_OK;
+  if (!rays || !out_tri || !out_tuv) return fail(MUPSI_ERR_INVALID, "null buffer");
+  cudaStream_t st = resolve_stream(stream);
+  Staged<mupsi_ray> dr(st);
+  Staged<uint32_t> dt(st);
+  Staged<float> duv(st);
+  ErrWord err(st);
+  MUPSI_CUDA(err.init());
+  MUPSI_CUDA(dr.in(rays, n, mem));
+  MUPSI_CUDA(dt.out(out_tri, n, mem));
+  MUPSI_CUDA(duv.out(out_tuv, 3 * n, mem));
+  k_bvh_intersect<<<grid_for(n), 128, 0, st>>>(mesh->store.d, n, dr.ptr, dt.ptr, duv.ptr, err.d);
+  count_launch();
+  MUPSI_CUDA(cudaGetLastError());
+  MUPSI_CUDA(dt.finish());
+  MUPSI_CUDA(duv.finish());
+  if (err.read()) return fail(MUPSI_ERR_DEVICE_LIMIT, "BVH traversal exceeded the 64-entry stack");
+  return MUPSI_OK;
+}
+
+int mupsi_gpu_bvh_occluded(const mupsi_mesh* mesh, int64_t n, const mupsi_ray* rays, uint8_t* out, mupsi_mem mem,
+                           void* stream) {
+  clear_error();
+  if (!mesh || n < 0) return fail(MUPSI_ERR_INVALID, "bad argument");
+  if (n == 0) return MUPSI_OK;
+  if (!rays || !out) return fail(MUPSI_ERR_INVALID, "null buffer");
+  cudaStream_t st = resolve_stream(stream);
+  Staged<mupsi_ray> dr(st);
+  Staged<uint8_t> dout(st);
+  ErrWord err(st);
+  MUPSI_CUDA(err.init());
+  MUPSI_CUDA(dr.in(rays, n, mem));
+  MUPSI_CUDA(dout.out(out, n, mem));
+  k_bvh_occluded<<<grid_for(n), 128, 0, st>>>(mesh->store.d, n, dr.ptr, dout.ptr, err.d);
+  count_launch();
+  MUPSI_CUDA(cudaGetLastError());
+  MUPSI_CUDA(dout.finish());
+  if (err.read()) return fail(MUPSI_ERR_DEVICE_LIMIT, "BVH traversal exceeded the 64-entry stack");
+  return MUPSI_OK;
+}
+
+int mupsi_gpu_bvh_closest(const mupsi_mesh* mesh, int64_t n, const float* p, uint32_t* out_tri, float* out_dq,
+                          mupsi_mem mem, void* stream) {
+  clear_error();
+  if (!mesh || n < 0) return fail(MUPSI_ERR_INVALID, "bad argument");
+  if (n == 0) return MUPSI_OK;
+  if (!p || !out_tri || !out_dq) return fail(MUPSI_ERR_INVALID, "null buffer");
+  cudaStream_t st = resolve_stream(stream);
+  Staged<float> dp(st), ddq(st);
+  Staged<uint32_t> dt(st);
+  ErrWord err(st);
+  MUPSI_CUDA(err.init());
+  MUPSI_CUDA(dp.in(p, 3 * n, mem));
+  MUPSI_CUDA(dt.out(out_tri, n, mem));
+  MUPSI_CUDA(ddq.out(out_dq, 4 * n, mem));
+  k_bvh_closest<<<grid_for(n), 128, 0, st>>>(mesh->store.d, n, dp.ptr, dt.ptr, ddq.ptr, err.d);
+  count_launch();
+  MUPSI_CUDA(cudaGetLastError());
+  MUPSI_CUDA(dt.finish());
+  MUPSI_CUDA(ddq.finish());
+  if (err.read()) return fail(MUPSI_ERR_DEVICE_LIMIT, "BVH traversal exceeded the 64-entry stack");
+  return MUPSI_OK;
+}
+
+int mupsi_gpu_mesh_queries(const mupsi_mesh* mesh, int64_t n, const float* p, uint8_t* out_inside, uint32_t* out_tri,
+                           float* out_dq, mupsi_mem mem, void* stream) {
+  clear_error();
+  if (!mesh || n < 0) return fail(MUPSI_ERR_INVALID, "bad argument");
+  if (n == 0) return MUPSI_OK;
+  if (!p || !out_inside || !out_tri || !out_dq) return fail(MUPSI_ERR_INVALID, "null buffer");
+  cudaStream_t st = resolve_stream(stream);
+  Staged<float> dp(st), ddq(st);
+  Staged<uint32_t> dt(st);
+  Staged<uint8_t> di(st);
+  ErrWord err(st);
+  MUPSI_CUDA(err.init());
+  MUPSI_CUDA(dp.in(p, 3 * n, mem));
+  MUPSI_CUDA(di.out(out_inside, n, mem));
+  MUPSI_CUDA(dt.out(out_tri, n, mem));
+  MUPSI_CUDA(ddq.out(out_dq, 4 * n, mem));
+  k_mesh_queries<<<grid_for(n), 128, 0, st>>>(mesh->store.d, n, dp.ptr, di.ptr, dt.ptr, ddq.ptr, err.d);
+  count_launch();
+  MUPSI_CUDA(cudaGetLastError());
+  MUPSI_CUDA(di.finish());
+  MUPSI_CUDA(dt.finish());
+  MUPSI_CUDA(ddq.finish());
+  if (err.read()) return fail(MUPSI_ERR_DEVICE_LIMIT, "BVH traversal exceeded the 64-entry stack");
+  return MUPSI_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,342 @@
+// Rays, spheres, BVH traversal, camera and BSDF sampling on the device.
+// Each routine follows the reference function cited beside it operation for
+// operation (the library is built without FMA contraction), so hit triangle ids
+// and BVH results are bit-exact and the float results equal the reference's.
+#pragma once
+#include "dmath.cuh"
+
+#define LEAF_FLAG 0x80000000u
+#define BVH_STACK 64  // the reference's fixed traversal stack (bvh.cpp:201)
+
+// BVH::Node: AABB (min, max) + left/right|LEAF_FLAG, 32 bytes (bvh/bvh.h:26-36)
+struct __align__(16) BNode {
+  float mn[3];
+  float mx[3];
+  uint32_t left, right;
+};
+
+struct Ray {
+  v3 o, d;
+  float nt, ft;
+};
+// Ray(origin, direction) normalizes the direction (geometry/ray.h:12)
+MD Ray make_ray(v3 o, v3 d) {
+  Ray r;
+  r.o = o;
+  r.d = normalized(d);
+  r.nt = 0.0f;
+  r.ft = 3.402823466e+38f;  // FLT_MAX
+  return r;
+}
+
+// Device view of one mesh and its BVH (primitives/mesh.h, bvh/bvh.h)
+struct DMesh {
+  const BNode* nodes;
+  const uint32_t* tri_idx;
+  const int32_t* faces;   // [F*3]
+  const float* verts;     // [V*3]
+  const float* face_n;    // [F*3]
+  const float* vert_n;    // nullable [V*3]
+  const float* cdf;       // area CDF [F]
+  int64_t num_nodes, num_faces;
+  uint32_t root;
+  float total_area;
+  m4 T, Tinv;
+  int identity;           // Tinv.isIdentity()
+  int normal_identity;    // normal transform (Tinv^T 3x3) is identity
+};
+
+MD v3 vert(const DMesh& m, int32_t i) { return ld3(m.verts + 3 * (int64_t)i); }
+
+// AABB::intersect slab test (bvh/boudingbox.cpp:6-38)
+MD bool aabb_hit(const BNode& b, const Ray& r) {
+  float tmin = -INFINITY, tmax = INFINITY;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float d = get(r.d, a), o = get(r.o, a);
+    if (fabsf(d) > 1e-8f) {
+      float t1 = (b.mn[a] - o) / d;
+      float t2 = (b.mx[a] - o) / d;
+      tmin = fmax_std(tmin, fmin_std(t1, t2));
+      tmax = fmin_std(tmax, fmax_std(t1, t2));
+    } else if (o < b.mn[a] || o > b.mx[a]) {
+      return false;
+    }
+  }
+  return tmax >= tmin && tmax >= r.nt && tmin <= r.ft;
+}
+
+// Moller-Trumbore (bvh.cpp:82-111)
+MD bool ray_tri(const Ray& r, v3 v0, v3 v1, v3 v2, float& t, float& u, float& v) {
+  v3 e1 = v1 - v0, e2 = v2 - v0;
+  v3 h = cross(r.d, e2);
+  float a = dot(e1, h);
+  if (fabsf(a) < 1e-8f) return false;
+  float f = 1.0f / a;
+  v3 s = r.o - v0;
+  u = f * dot(s, h);
+  if (u < 0.0f || u > 1.0f) return false;
+  v3 q = cross(s, e1);
+  v = f * dot(r.d, q);
+  if (v < 0.0f || u + v > 1.0f) return false;
+  t = f * dot(e2, q);
+  return t > r.nt && t < r.ft;
+}
+
+MD BNode load_node(const BNode* nodes, uint32_t i) {
+  const float4* p = reinterpret_cast<const float4*>(nodes + i);
+  float4 a = __ldg(p), b = __ldg(p + 1);
+  BNode n;
+  n.mn[0] = a.x;
+  n.mn[1] = a.y;
+  n.mn[2] = a.z;
+  n.mx[0] = a.w;
+  n.mx[1] = b.x;
+  n.mx[2] = b.y;
+  n.left = __float_as_uint(b.z);
+  n.right = __float_as_uint(b.w);
+  return n;
+}
+MD int node_axis(const BNode& b) {
+  float d0 = b.mx[0] - b.mn[0], d1 = b.mx[1] - b.mn[1], d2 = b.mx[2] - b.mn[2];
+  return (d0 > d1 && d0 > d2) ? 0 : (d1 > d2 ? 1 : 2);
+}
+MD float node_centroid(const BNode& b, int a) { return (b.mn[a] + b.mx[a]) * 0.5f; }
+
+// BVH::intersect (bvh.cpp:197-250): closest hit, front-to-back by child centroid
+// along the parent's longest axis; narrows r.ft. `overflow` is set if the
+// traversal would exceed the reference's 64-entry stack.
+MD bool bvh_intersect(const DMesh& m, Ray& r, uint32_t& tri, float& uu, float& vv, bool& overflow) {
+  if (m.num_nodes == 0) return false;
+  bool hit = false;
+  uint32_t st[BVH_STACK];
+  int sp = 0;
+  st[sp++] = m.root;
+  while (sp > 0) {
+    BNode nd = load_node(m.nodes, st[--sp]);
+    if (!aabb_hit(nd, r)) continue;
+    if (nd.right & LEAF_FLAG) {
+      uint32_t start = nd.left, cnt = nd.right & ~LEAF_FLAG;
+      for (uint32_t i = start; i < start + cnt; ++i) {
+        uint32_t ti = __ldg(m.tri_idx + i);
+        const int32_t* f = m.faces + 3 * (int64_t)ti;
+        float t, u, v;
+        if (ray_tri(r, vert(m, __ldg(f)), vert(m, __ldg(f + 1)), vert(m, __ldg(f + 2)), t, u, v)) {
+          r.ft = t;
+          tri = ti;
+          uu = u;
+          vv = v;
+          hit = true;
+        }
+      }
+    } else {
+      BNode ln = load_node(m.nodes, nd.left), rn = load_node(m.nodes, nd.right);
+      int axis = node_axis(nd);
+      float lc = node_centroid(ln, axis), rc = node_centroid(rn, axis);
+      bool near_first = (get(r.d, axis) > 0) ? (lc < rc) : (lc > rc);
+      if (sp + 2 > BVH_STACK) {
+        overflow = true;
+        return hit;
+      }
+      st[sp++] = near_first ? nd.right : nd.left;
+      st[sp++] = near_first ? nd.left : nd.right;
+    }
+  }
+  return hit;
+}
+
+// BVH::occluded (bvh.cpp:254-300). The reference starts this traversal at node 0,
+// which is the first leaf of the post-order array, not the root (bvh.cpp:259);
+// that behaviour is kept so shadow rays agree with the reference.
+MD bool bvh_occluded(const DMesh& m, const Ray& r, bool& overflow) {
+  if (m.num_nodes == 0) return false;
+  uint32_t st[BVH_STACK];
+  int sp = 0;
+  st[sp++] = 0;
+  while (sp > 0) {
+    BNode nd = load_node(m.nodes, st[--sp]);
+    if (!aabb_hit(nd, r)) continue;
+    if (nd.right & LEAF_FLAG) {
+      uint32_t start = nd.left, cnt = nd.right & ~LEAF_FLAG;
+      for (uint32_t i = start; i < start + cnt; ++i) {
+        const int32_t* f = m.faces + 3 * (int64_t)__ldg(m.tri_idx + i);
+        float t, u, v;
+        if (ray_tri(r, vert(m, __ldg(f)), vert(m, __ldg(f + 1)), vert(m, __ldg(f + 2)), t, u, v)) return true;
+      }
+    } else {
+      BNode ln = load_node(m.nodes, nd.left), rn = load_node(m.nodes, nd.right);
+      int axis = node_axis(nd);
+      float lc = node_centroid(ln, axis), rc = node_centroid(rn, axis);
+      bool near_first = (get(r.d, axis) > 0) ? (lc < rc) : (lc > rc);
+      if (sp + 2 > BVH_STACK) {
+        overflow = true;
+        return false;
+      }
+      st[sp++] = near_first ? nd.right : nd.left;
+      st[sp++] = near_first ? nd.left : nd.right;
+    }
+  }
+  return false;
+}
+
+// std::max({a, 0, b}) as max_element over the list
+MD float max3_il(float a, float b, float c) {
+  float m = a;
+  if (m < b) m = b;
+  if (m < c) m = c;
+  return m;
+}
+// dist2ToAABB (bvh.cpp:20-25)
+MD float dist2_aabb(v3 p, const BNode& b) {
+  float dx = max3_il(b.mn[0] - p.x, 0.0f, p.x - b.mx[0]);
+  float dy = max3_il(b.mn[1] - p.y, 0.0f, p.y - b.mx[1]);
+  float dz = max3_il(b.mn[2] - p.z, 0.0f, p.z - b.mx[2]);
+  return dx * dx + dy * dy + dz * dz;
+}
+// dist2ToLine (bvh.cpp:27-40)
+MD float dist2_line(v3 p, v3 a, v3 b, v3& out) {
+  v3 ab = b - a, ap = p - a;
+  if (sqn(ab) < 1e-6f) {
+    out = a;
+    return sqn(ap);
+  }
+  float d = dot(ap, ab);
+  float t = d / sqn(ab);
+  t = t < 0.0f ? 0.0f : (1.0f < t ? 1.0f : t);
+  v3 proj = a + t * ab;
+  out = proj;
+  return sqn(p - proj);
+}
+// dist2ToTriangle (bvh.cpp:42-80)
+MD float dist2_tri(v3 p, v3 a, v3 b, v3 c, v3& out) {
+  v3 e1 = a - b, e2 = a - c;
+  v3 n = cross(e1, e2);
+  if (sqn(n) < 1e-6f) {
+    out = a;
+    return sqn(p - a);
+  }
+  n = normalized(n);
+  float dp = dot(p - a, n);
+  v3 pj = p - dp * n;
+  v3 ab = -e1, bc = c - b, ca = e2;
+  v3 c1 = cross(ab, pj - a), c2 = cross(bc, pj - b), c3 = cross(ca, pj - c);
+  if (dot(c1, n) >= 0 && dot(c2, n) >= 0 && dot(c3, n) >= 0) {
+    out = pj;
+    return dp * dp;
+  }
+  float mn = INFINITY, d;
+  v3 tmp;
+  if ((d = dist2_line(p, a, b, tmp)) < mn) {
+    mn = d;
+    out = tmp;
+  }
+  if ((d = dist2_line(p, b, c, tmp)) < mn) {
+    mn = d;
+    out = tmp;
+  }
+  if ((d = dist2_line(p, c, a, tmp)) < mn) {
+    mn = d;
+    out = tmp;
+  }
+  return mn;
+}
+// BVH::closest (bvh.cpp:302-353): returns sqrt of the squared distance.
+MD float bvh_closest(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overflow) {
+  if (m.num_nodes == 0) return 0.0f;
+  uint32_t st[BVH_STACK];
+  int sp = 0;
+  st[sp++] = m.root;
+  float best = 3.402823466e+38f;
+  while (sp > 0) {
+    BNode nd = load_node(m.nodes, st[--sp]);
+    if (dist2_aabb(p, nd) >= best) continue;
+    if (nd.right & LEAF_FLAG) {
+      uint32_t start = nd.left, cnt = nd.right & ~LEAF_FLAG;
+      for (uint32_t i = start; i < start + cnt; ++i) {
+        uint32_t ti = __ldg(m.tri_idx + i);
+        const int32_t* f = m.faces + 3 * (int64_t)ti;
+        v3 tmp;
+        float d = dist2_tri(p, vert(m, __ldg(f)), vert(m, __ldg(f + 1)), vert(m, __ldg(f + 2)), tmp);
+        if (d < best) {
+          best = d;
+          tri = ti;
+          q = tmp;
+        }
+      }
+    } else {
+      BNode ln = load_node(m.nodes, nd.left), rn = load_node(m.nodes, nd.right);
+      float dl = dist2_aabb(p, ln), dr = dist2_aabb(p, rn);
+      if (sp + 2 > BVH_STACK) {
+        overflow = true;
+        break;
+      }
+      if (dl < dr) {
+        if (dr < best) st[sp++] = nd.right;
+        if (dl < best) st[sp++] = nd.left;
+      } else {
+        if (dl < best) st[sp++] = nd.left;
+        if (dr < best) st[sp++] = nd.right;
+      }
+    }
+  }
+  return sqrtf(best);
+}
+
+// Mesh::inside (mesh.cpp:341-362): parity of crossings of a +x ray from p,
+// repeating BVH::intersect with nearT = last t + 1e-4 until a miss.
+MD bool mesh_inside(const DMesh& m, v3 p, bool& overflow) {
+  v3 pl = apply4(m.Tinv, p);
+  Ray r = make_ray(pl, mk3(1.0f, 0.0f, 0.0f));
+  uint32_t tri;
+  float u, v;
+  int hits = 0;
+  if (bvh_intersect(m, r, tri, u, v, overflow)) {
+    ++hits;
+    // each crossing strictly increases nearT, so the loop ends; the cap guards
+    // against a corrupted mesh only
+    for (int guard = 0; r.ft < INFINITY && guard < (1 << 20); ++guard) {
+      r.nt = r.ft + 1e-4f;
+      r.ft = INFINITY;
+      if (!bvh_intersect(m, r, tri, u, v, overflow)) break;
+      ++hits;
+    }
+  }
+  return (hits % 2) == 1;
+}
+// Mesh::distToPoint (mesh.cpp:325-339): world-space distance to the closest point
+MD float mesh_dist(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overflow) {
+  v3 pl = apply4(m.Tinv, p);
+  v3 ql = mk3(0, 0, 0);
+  bvh_closest(m, pl, tri, ql, overflow);
+  q = apply4(m.T, ql);
+  return norm3(q - p);
+}
+
+// intersectUnitSphere (sphere.cpp:11-30)
+MD float unit_sphere(float nt, float ft, v3 O, v3 D) {
+  float a = sqn(D), b = dot(O, D), c = sqn(O) - 1.0f;
+  float disc = b * b - a * c;
+  if (disc < 0.0f) return -1.0f;
+  float sq = sqrtf(disc);
+  float t = (-b - sq) / a;
+  if (t > nt && t < ft) return t;
+  t = (-b + sq) / a;
+  if (t > nt && t < ft) return t;
+  return -1.0f;
+}
+
+// TangentFrame(n) (math/sample.h:21-32)
+struct Frame {
+  v3 n, t, b;
+};
+MD Frame make_frame(v3 nn) {
+  Frame f;
+  f.n = normalized(nn);
+  float sign = copysignf(1.0f, f.n.z);
+  float a = -1.0f / (sign + f.n.z);
+  float b = f.n.x * f.n.y * a;
+  f.t = normalized(mk3(1.0f + sign * f.n.x * f.n.x * a, sign * b, -sign * f.n.x));
+  f.b = normalized(mk3(b, sign + f.n.y * f.n.y * a, -f.n.y));
+  return f;
+}
+MD v3 to_global(const Frame& f, v3 p) { return (f.t * p.x + f.b * p.y) + f.n * p.z; }

@@ -1,0 +1,141 @@
+// Sparse-convolution GP noise psi / grad psi and the Renewal+ conditioning terms
+// (the reference's gp/kernel.h:39-78, gp/gpnoise.cpp:51-87, gpnoise.h:31,44,
+// medium/gpmedium.cpp:26-41).
+//
+// Bit-exact parts (shared with the reference): the grid cell of p
+// (trunc(p/kr) with an IEEE division), the per-cell seed make_seed(cx,cy,cz,seed),
+// the PCG stream started at cell_seed + 1 (32-bit wrap), the impulse positions
+// s = cell*kr + U^3*kr and the +-1 weights, and the accumulation order
+// (dx, dy, dz, i). The Gaussian h uses the SFU exp2 (ex2.approx) on the
+// argument |p-s|^2 * (-log2(e)/L2); the reference calls glibc expf on
+// -|p-s|^2 / L2. The resulting psi differs from the reference by ~1e-7 of the
+// sum of |terms| (tested at 1e-5).
+#pragma once
+#include "dmath.cuh"
+
+struct KParams {
+  float sigma;       // kernel sigma
+  float kr;          // kernel radius = grid cell size
+  float L2;          // |aniso|^2, computed as the reference does (a0^2 + (a1^2 + a2^2))
+  float sqrt_var;    // sqrtf(float(ppc / kr^3 * pi^1.5)) (gpnoise.h:31,44)
+  float k2;          // -log2(e) / L2: exp(-r2/L2) = exp2(r2 * k2)
+  float c2;          // -2.0f / L2 (kernel.h:57)
+  float c4;          // 4.0f / (L2 * L2) (kernel.h:64)
+  float psi_bound;   // sigma * 27 * ppc / sqrt_var: |psi| <= psi_bound since |w h| <= 1
+  float gradh_max;   // max over r of |grad h| = sqrt(2/L2) * exp(-1/2)
+  int ppc;           // impulses per cell
+};
+
+MD float ex2_approx(float x) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// Grid cell of p: (p / kr).cast<int>() (gpnoise.cpp:54), truncation toward zero.
+MD void cell_of(const KParams& k, v3 p, int& cx, int& cy, int& cz) {
+  cx = (int)(p.x / k.kr);
+  cy = (int)(p.y / k.kr);
+  cz = (int)(p.z / k.kr);
+}
+
+// Impulses of one cell, visited in the reference's order. F(s, w) is called per
+// impulse with its position and sign (+1 / -1).
+template <typename F>
+MD void for_each_impulse(const KParams& k, int nx, int ny, int nz, uint32_t seed, F&& f) {
+  uint32_t cs = make_seed4((uint32_t)nx, (uint32_t)ny, (uint32_t)nz, seed);
+  uint64_t st = (uint64_t)(uint32_t)(cs + 1u);
+  const float bx = (float)nx * k.kr, by = (float)ny * k.kr, bz = (float)nz * k.kr;
+  for (int i = 0; i < k.ppc; ++i) {
+    // Vector3f(next1D(), next1D(), next1D()) as the reference's build evaluates it:
+    // constructor arguments right to left, so the first draw is z.
+    float a = pcg_next1d(st);
+    float b = pcg_next1d(st);
+    float c = pcg_next1d(st);
+    v3 s = v3{bx + c * k.kr, by + b * k.kr, bz + a * k.kr};
+    float w = pcg_next1d(st) < 0.5f ? -1.0f : 1.0f;
+    f(s, w);
+  }
+}
+
+// Unnormalised InternalNoise sums. GRAD = false computes the value only.
+template <bool GRAD>
+MD void psi_sums(const KParams& k, v3 p, uint32_t seed, float& sv, float& sx, float& sy, float& sz) {
+  int cx, cy, cz;
+  cell_of(k, p, cx, cy, cz);
+  float v = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f;
+#pragma unroll 1
+  for (int dx = -1; dx <= 1; ++dx)
+#pragma unroll 1
+    for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll 1
+      for (int dz = -1; dz <= 1; ++dz) {
+        for_each_impulse(k, cx + dx, cy + dy, cz + dz, seed, [&](v3 s, float w) {
+          v3 d = p - s;
+          float r2 = d.x * d.x + (d.y * d.y + d.z * d.z);
+          float h = ex2_approx(r2 * k.k2);
+          v = fmaf(w, h, v);  // w = +-1: w*h is exact, so this equals v + w*h
+          if (GRAD) {
+            float gs = h * k.c2;
+            gx = fmaf(w, gs * d.x, gx);
+            gy = fmaf(w, gs * d.y, gy);
+            gz = fmaf(w, gs * d.z, gz);
+          }
+        });
+      }
+  sv = v;
+  sx = gx;
+  sy = gy;
+  sz = gz;
+}
+
+// RawNoise(p, seed) = sigma * InternalNoise / sqrt(Var) (gpnoise.h:44)
+MD float4 raw_noise(const KParams& k, v3 p, uint32_t seed) {
+  float v, x, y, z;
+  psi_sums<true>(k, p, seed, v, x, y, z);
+  return make_float4((k.sigma * v) / k.sqrt_var, (k.sigma * x) / k.sqrt_var, (k.sigma * y) / k.sqrt_var,
+                     (k.sigma * z) / k.sqrt_var);
+}
+MD float raw_noise_value(const KParams& k, v3 p, uint32_t seed) {
+  float v, x, y, z;
+  psi_sums<false>(k, p, seed, v, x, y, z);
+  return (k.sigma * v) / k.sqrt_var;
+}
+
+struct Cond {
+  v3 C;
+  float u;
+  v3 g;
+  uint32_t active;
+};
+
+// h(C, p) with the accurate expf and the reference's division (kernel.h:52-54)
+MD float h_exact(const KParams& k, v3 C, v3 p) { return expf(-sqn(p - C) / k.L2); }
+
+// Value part of the conditioning: u*h(C,p) + g . grad h(C,p) (gpmedium.cpp:34-35)
+MD float cond_value(const KParams& k, const Cond& c, v3 p) {
+  float h = h_exact(k, c.C, p);
+  v3 hg = (h * k.c2) * (p - c.C);
+  return c.u * h + dot(c.g, hg);
+}
+// Conditioning terms added to (f, grad f) (gpmedium.cpp:32-39)
+MD float4 add_cond(const KParams& k, const Cond& c, v3 p, float4 f) {
+  if (!c.active) return f;
+  float h = h_exact(k, c.C, p);
+  v3 r = p - c.C;
+  v3 hg = (h * k.c2) * r;
+  f.x += c.u * h + dot(c.g, hg);
+  // H_h g = h * ((-2/L2) g + (4/L2^2)(r.g) r)
+  v3 a = k.c2 * c.g;
+  v3 b = (k.c4 * dot(r, c.g)) * r;
+  v3 Hg = h * (a + b);
+  f.y += c.u * hg.x + Hg.x;
+  f.z += c.u * hg.y + Hg.y;
+  f.w += c.u * hg.z + Hg.z;
+  return f;
+}
+// Bound on |u h + g . grad h| over all p (|h| <= 1, |grad h| <= gradh_max)
+MD float cond_bound(const KParams& k, const Cond& c) {
+  if (!c.active) return 0.0f;
+  return fabsf(c.u) + norm3(c.g) * k.gradh_max;
+}

@@ -1,0 +1,925 @@
+// Scenes, the GP-medium batch entry points and the wavefront path tracer
+// (PathTracer::trace, rendering/trace.cpp:118-213, driven like
+// Renderer::startRenderProgressive, rendering/renderer.cpp:22-49).
+//
+// Wavefront layout: a wave holds W*H*passes paths in structure-of-arrays state.
+// Each bounce iteration runs two kernels:
+//   k_march  - persistent warps march every path that is inside a GP medium;
+//              idle lanes pull the next path from the medium queue, so long and
+//              short marches never stall a warp;
+//   k_shade  - every live path: medium event (NEE, Lambertian sample, Russian
+//              roulette, Renewal+ conditioning) or surface event (scene
+//              intersection, NEE, BSDF sample, RR, medium switch) or sky; the
+//              survivors are appended to the next iteration's queues with
+//              warp-aggregated atomics.
+// Each path does exactly one bounce per iteration (or terminates), so a wave
+// takes at most max_bounce iterations. Per-sample radiance is written to a
+// buffer and summed per pixel in pass order (Framebuffer::accumulate order).
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "core.cuh"
+#include "scene.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace mupsi {
+
+// ------------------------------------------------------------ path state
+struct Paths {
+  float4* o;    // origin xyz, near_t
+  float4* d;    // direction xyz, medium index (int bits; -1 none)
+  float4* thr;  // throughput xyz
+  float4* em;   // emission xyz
+  uint2* rng;   // path sampler state (u64)
+  float4* ca;   // conditioning C xyz, u
+  float4* cb;   // conditioning g xyz, active
+  int4* meta;   // x, y, k, bounce
+  float4* ha;   // march: t, p xyz
+  float4* hb;   // march: normal xyz, exited
+  float* rad;   // final radiance [cap * 3]
+  uint32_t* q[4];       // medium queue (2 buffers), live queue (2 buffers)
+  uint32_t* counts;     // per iteration: [it*2+0] medium count, [it*2+1] live count
+  uint32_t* cursors;    // per iteration: march work cursor
+  int64_t cap;
+};
+
+MD uint64_t ld_rng(const uint2 v) { return ((uint64_t)v.y << 32) | v.x; }
+MD uint2 st_rng(uint64_t s) { return make_uint2((uint32_t)s, (uint32_t)(s >> 32)); }
+
+MD Cond load_cond(const Paths& P, uint32_t i) {
+  float4 a = P.ca[i], b = P.cb[i];
+  Cond c;
+  c.C = mk3(a.x, a.y, a.z);
+  c.u = a.w;
+  c.g = mk3(b.x, b.y, b.z);
+  c.active = __float_as_uint(b.w);
+  return c;
+}
+MD void store_cond(const Paths& P, uint32_t i, const Cond& c) {
+  P.ca[i] = make_float4(c.C.x, c.C.y, c.C.z, c.u);
+  P.cb[i] = make_float4(c.g.x, c.g.y, c.g.z, __uint_as_float(c.active));
+}
+
+// ConstantSampler seed of bounce b's medium sampler (trace.cpp:146-147)
+MD uint32_t medium_seed(const DScene* S, int x, int y, int k, int b) {
+  uint32_t s = S->gp_mode == MUPSI_GP_SINGLE_REALIZATION
+                   ? TRACE_SEED
+                   : make_seed5((uint32_t)x, (uint32_t)y, (uint32_t)k, TRACE_SEED, (uint32_t)b);
+  return constant_sampler_i(s);
+}
+
+// ------------------------------------------------------------ kernels
+__global__ void k_raygen(const DScene* __restrict__ S, Paths P, int64_t n, int pass0, const int32_t* xs,
+                         const int32_t* ys, const int32_t* ks) {
+  const int64_t wh = (int64_t)S->width * S->height;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    int x, y, k;
+    if (xs) {
+      x = xs[i];
+      y = ys[i];
+      k = ks[i];
+    } else {
+      int64_t pix = i % wh;
+      k = pass0 + (int)(i / wh);
+      x = (int)(pix % S->width);
+      y = (int)(pix / S->width);
+    }
+    uint64_t rng = pcg_seeded(make_seed4((uint32_t)x, (uint32_t)y, (uint32_t)k, TRACE_SEED));
+    Ray r = camera_ray(S, x, y);
+    P.o[i] = make_float4(r.o.x, r.o.y, r.o.z, r.nt);
+    P.d[i] = make_float4(r.d.x, r.d.y, r.d.z, __int_as_float(-1));
+    P.thr[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    P.em[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    P.rng[i] = st_rng(rng);
+    P.ca[i] = make_float4(0, 0, 0, 0);
+    P.cb[i] = make_float4(0, 0, 0, __uint_as_float(0u));
+    P.meta[i] = make_int4(x, y, k, 0);
+    P.q[2][i] = (uint32_t)i;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    P.counts[0] = 0;
+    P.counts[1] = (uint32_t)n;
+  }
+}
+
+// Persistent march over the medium queue of iteration `it`.
+__global__ void __launch_bounds__(128) k_march(const DScene* __restrict__ S, Paths P, int it) {
+  const uint32_t n = P.counts[2 * it];
+  const uint32_t* q = P.q[it & 1];
+  uint32_t* cursor = P.cursors + it;
+  const unsigned lane = threadIdx.x & 31;
+  March m;
+  uint32_t idx = 0;
+  bool active = false;
+  bool ovf = false;
+  unsigned long long steps = 0, psis = 0, marches = 0, imps = 0;
+  while (true) {
+    // refill idle lanes from the queue (warp-aggregated)
+    unsigned need = __ballot_sync(0xffffffffu, !active);
+    if (need) {
+      uint32_t base = 0;
+      int leader = __ffs(need) - 1;
+      if ((int)lane == leader) base = atomicAdd(cursor, (uint32_t)__popc(need));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (!active) {
+        uint32_t j = base + __popc(need & ((1u << lane) - 1u));
+        if (j < n) {
+          idx = q[j];
+          float4 o = P.o[idx], d = P.d[idx];
+          int4 meta = P.meta[idx];
+          int med = __float_as_int(d.w);
+          march_begin(S, m, mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), o.w, 3.402823466e+38f, med,
+                      medium_seed(S, meta.x, meta.y, meta.z, meta.w), load_cond(P, idx));
+          active = true;
+          marches++;
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) break;
+    if (active) {
+      float mu;
+      v3 p;
+      if (march_cheap(S, m, mu, p, ovf)) march_psi(S, m, mu, p);
+      if (m.status != 0) {
+        mupsi_medium_sample r;
+        march_result(S, m, r, ovf);
+        P.ha[idx] = make_float4(r.t, r.p[0], r.p[1], r.p[2]);
+        P.hb[idx] = make_float4(r.normal[0], r.normal[1], r.normal[2], __uint_as_float(r.exited));
+        steps += m.n_steps;
+        psis += m.n_psi;
+        imps += (unsigned long long)m.n_psi * 27ull * (unsigned long long)S->media[m.medium].k.ppc;
+        active = false;
+      }
+    }
+  }
+  if (ovf) atomicOr(S->err, ERR_BVH_STACK);
+  if (S->counters) {
+    for (int o = 16; o > 0; o >>= 1) {
+      steps += __shfl_down_sync(0xffffffffu, steps, o);
+      psis += __shfl_down_sync(0xffffffffu, psis, o);
+      marches += __shfl_down_sync(0xffffffffu, marches, o);
+      imps += __shfl_down_sync(0xffffffffu, imps, o);
+    }
+    if (lane == 0) {
+      atomicAdd(&S->counters[0], steps);
+      atomicAdd(&S->counters[1], psis);
+      atomicAdd(&S->counters[2], marches);
+      atomicAdd(&S->counters[3], imps);
+    }
+  }
+}
+
+// GPMedium::transmittance (gpmedium.cpp:105-129): 0 at the first sign change.
+MD float transmittance(const DScene* S, int medium, const Ray& r, uint32_t seed, const Cond& c, bool& ovf) {
+  March m;
+  march_begin(S, m, r.o, r.d, r.nt, r.ft, medium, seed, c);
+  march_full(S, m, ovf);
+  return m.status == 1 ? 0.0f : 1.0f;
+}
+
+MD void push(uint32_t* q, uint32_t* count, uint32_t v) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  uint32_t base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(count, g.size());
+  base = g.shfl(base, 0);
+  q[base + g.thread_rank()] = v;
+}
+
+// One bounce of PathTracer::trace for every live path of iteration `it`.
+__global__ void __launch_bounds__(128) k_shade(const DScene* __restrict__ S, Paths P, int it) {
+  const uint32_t n = P.counts[2 * it + 1];
+  const uint32_t* q = P.q[2 + (it & 1)];
+  uint32_t* qm_next = P.q[(it + 1) & 1];
+  uint32_t* qa_next = P.q[2 + ((it + 1) & 1)];
+  uint32_t* cm_next = P.counts + 2 * (it + 1);
+  uint32_t* ca_next = P.counts + 2 * (it + 1) + 1;
+  const bool single = S->gp_mode == MUPSI_GP_SINGLE_REALIZATION;
+  const v3 med_albedo = mk3(0.8f, 0.8f, 0.8f);  // Medium::default_bsdf_: Lambertian, albedo 0.8
+  bool ovf = false;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const uint32_t i = q[j];
+    float4 o4 = P.o[i], d4 = P.d[i], t4 = P.thr[i], e4 = P.em[i];
+    int4 meta = P.meta[i];
+    int medium = __float_as_int(d4.w);
+    uint64_t rng = ld_rng(P.rng[i]);
+    v3 thr = mk3(t4.x, t4.y, t4.z), em = mk3(e4.x, e4.y, e4.z);
+    Ray ray;
+    ray.o = mk3(o4.x, o4.y, o4.z);
+    ray.d = mk3(d4.x, d4.y, d4.z);
+    ray.nt = o4.w;
+    ray.ft = 3.402823466e+38f;
+    int bounce = meta.w;
+    bool has_hit = false, exited = true, dead = false;
+    Cond cond = load_cond(P, i);
+    if (medium >= 0) {
+      float4 hb = P.hb[i];
+      if (__float_as_uint(hb.w) == 0u) {
+        // makeSurfaceEventFromMedium (medium.cpp:8-26) + handleVolume (trace.cpp:77-116)
+        float4 ha = P.ha[i];
+        v3 Pt = mk3(ha.y, ha.z, ha.w), N = mk3(hb.x, hb.y, hb.z), wo = -ray.d;
+        LSample ls;
+        if (choose_light(S, Pt, rng, ls)) {
+          Ray sr = make_ray(Pt + N * S->eps, ls.d);
+          float bias = ls.dist - S->eps * fabsf(dot(ls.d, N));
+          sr.ft = bias * 0.99f;
+          float tr = transmittance(S, medium, sr, medium_seed(S, meta.x, meta.y, meta.z, bounce), cond, ovf);
+          v3 f = bsdf_weight(MUPSI_BSDF_LAMBERTIAN, med_albedo, ls.d, wo, N);
+          em = em + (tr * cmul(thr, cmul(f, ls.weight))) * fabsf(dot(ls.d, N));
+        }
+        v3 w;
+        v3 wi = bsdf_sample(MUPSI_BSDF_LAMBERTIAN, med_albedo, wo, N, rng, w);
+        thr = cmul(thr, w);
+        float surv = maxc(thr);
+        if (pcg_next1d(rng) > surv) {
+          dead = true;
+        } else {
+          thr = thr / surv;
+          uint32_t ns = medium_seed(S, meta.x, meta.y, meta.z, bounce + 1);
+          cond = sample_condition(S, S->media[medium], Pt, N, false, ns, !single, ovf);
+          ray = make_ray(Pt + N * S->eps, wi);
+          ray.nt = S->nearteps;
+          bounce++;
+          exited = false;
+          has_hit = true;
+        }
+      }
+    }
+    if (!dead && exited) {
+      Hit hi = scene_intersect(S, ray, ovf);
+      if (hi.prim >= 0) {
+        const DPrim& pr = S->prims[hi.prim];
+        v3 wo = -ray.d, N = hi.Ng;
+        LSample ls;
+        if (choose_light(S, hi.p, rng, ls)) {  // handleSurface NEE (trace.cpp:40-56)
+          Ray sr = make_ray(hi.p + N * S->eps, ls.d);
+          float bias = ls.dist - S->eps * fabsf(dot(ls.d, N));
+          sr.ft = bias * 0.99f;
+          if (!scene_occluded(S, sr, ovf)) {
+            v3 a = bsdf_weight(pr.bsdf, pr.albedo, ls.d, wo, N);
+            em = em + cmul(thr, cmul(a, ls.weight)) * fabsf(dot(ls.d, N));
+          }
+        }
+        v3 w;
+        v3 wi = bsdf_sample(pr.bsdf, pr.albedo, wo, N, rng, w);
+        if (pr.has_emission) em = em + cmul(thr, pr.emission * fmax_std(0.0f, dot(N, wi)));
+        thr = cmul(thr, w);
+        float surv = maxc(thr);
+        if (pcg_next1d(rng) > surv) {
+          dead = true;
+        } else {
+          thr = thr / surv;
+          bool back = dot(wi, N) < 0.0f;
+          medium = back ? pr.int_medium : pr.ext_medium;
+          float bs = back ? -1.0f : 1.0f;
+          ray = make_ray(hi.p + (bs * hi.Ng) * S->eps, wi);
+          ray.nt = S->nearteps;
+          bounce++;
+          has_hit = true;
+        }
+      } else if (S->has_sky) {
+        em = em + cmul(thr, S->sky);
+      }
+    }
+    if (!dead && has_hit && bounce < S->max_bounce) {
+      P.o[i] = make_float4(ray.o.x, ray.o.y, ray.o.z, ray.nt);
+      P.d[i] = make_float4(ray.d.x, ray.d.y, ray.d.z, __int_as_float(medium));
+      P.thr[i] = make_float4(thr.x, thr.y, thr.z, 0.0f);
+      P.em[i] = make_float4(em.x, em.y, em.z, 0.0f);
+      P.rng[i] = st_rng(rng);
+      store_cond(P, i, cond);
+      P.meta[i] = make_int4(meta.x, meta.y, meta.z, bounce);
+      push(qa_next, ca_next, i);
+      if (medium >= 0) push(qm_next, cm_next, i);
+    } else {
+      P.rad[3 * (int64_t)i] = em.x;
+      P.rad[3 * (int64_t)i + 1] = em.y;
+      P.rad[3 * (int64_t)i + 2] = em.z;
+    }
+  }
+  if (ovf) atomicOr(S->err, ERR_BVH_STACK);
+}
+
+// Per-pixel running sum over the wave's passes in pass order (framebuffer.cpp:28-35),
+// optional FP64 moments.
+__global__ void k_accumulate(const float* __restrict__ rad, int passes, int64_t wh, float* __restrict__ sum,
+                             double* __restrict__ moments) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < wh; p += (int64_t)gridDim.x * blockDim.x) {
+    float s0 = sum[3 * p], s1 = sum[3 * p + 1], s2 = sum[3 * p + 2];
+    double m[6] = {0, 0, 0, 0, 0, 0};
+    for (int k = 0; k < passes; ++k) {
+      const float* r = rad + 3 * ((int64_t)k * wh + p);
+      float a = r[0], b = r[1], c = r[2];
+      s0 += a;
+      s1 += b;
+      s2 += c;
+      if (moments) {
+        m[0] += a;
+        m[1] += b;
+        m[2] += c;
+        m[3] += (double)a * a;
+        m[4] += (double)b * b;
+        m[5] += (double)c * c;
+      }
+    }
+    sum[3 * p] = s0;
+    sum[3 * p + 1] = s1;
+    sum[3 * p + 2] = s2;
+    if (moments)
+      for (int c = 0; c < 6; ++c) moments[6 * p + c] += m[c];
+  }
+}
+
+__global__ void k_average(const float* __restrict__ sum, int64_t n3, float inv, float* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n3; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = sum[i] * inv;
+}
+
+// ---- batch kernels over a scene's medium ----
+__global__ void k_mean(const DScene* S, int medium, int64_t n, const float* p, float* out) {
+  bool ovf = false;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    float4 r = mean_value_grad(S, S->media[medium], ld3(p + 3 * i), ovf);
+    out[4 * i] = r.x;
+    out[4 * i + 1] = r.y;
+    out[4 * i + 2] = r.z;
+    out[4 * i + 3] = r.w;
+  }
+  if (ovf) atomicOr(S->err, ERR_BVH_STACK);
+}
+__global__ void k_medium_eval(const DScene* S, int medium, int64_t n, const float* p, const uint32_t* seed,
+                              const Cond* cond, float* out) {
+  bool ovf = false;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    Cond c;
+    if (cond) {
+      c = cond[i];
+    } else {
+      c.active = 0;
+    }
+    float4 r = medium_eval(S, S->media[medium], ld3(p + 3 * i), seed[i], c, ovf);
+    out[4 * i] = r.x;
+    out[4 * i + 1] = r.y;
+    out[4 * i + 2] = r.z;
+    out[4 * i + 3] = r.w;
+  }
+  if (ovf) atomicOr(S->err, ERR_BVH_STACK);
+}
+__global__ void k_sample_distance(const DScene* S, int medium, int64_t n, const mupsi_ray* rays, const uint32_t* seed,
+                                  const Cond* cond, mupsi_medium_sample* out) {
+  bool ovf = false;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    Cond c;
+    if (cond) {
+      c = cond[i];
+    } else {
+      c.active = 0;
+      c.C = mk3(0, 0, 0);
+      c.u = 0;
+      c.g = mk3(0, 0, 0);
+    }
+    const mupsi_ray& r = rays[i];
+    March m;
+    // Ray(origin, direction) normalises the direction (geometry/ray.h:12)
+    march_begin(S, m, ld3(r.o), normalized(ld3(r.d)), r.near_t, r.far_t, medium, seed[i], c);
+    march_full(S, m, ovf);
+    mupsi_medium_sample res;
+    march_result(S, m, res, ovf);
+    out[i] = res;
+  }
+  if (ovf) atomicOr(S->err, ERR_BVH_STACK);
+}
+__global__ void k_sample_condition(const DScene* S, int medium, int64_t n, const mupsi_medium_sample* smp,
+                                   const uint32_t* seed, mupsi_cond* out) {
+  bool ovf = false;
+  const bool renewal = S->gp_mode == MUPSI_GP_RENEWAL_PLUS;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const mupsi_medium_sample& s = smp[i];
+    Cond c = sample_condition(S, S->media[medium], ld3(s.p), ld3(s.normal), s.exited != 0, seed[i], renewal, ovf);
+    mupsi_cond r;
+    st3(r.C, c.C);
+    r.u_tilde = c.u;
+    st3(r.g_tilde, c.g);
+    r.active = c.active;
+    out[i] = r;
+  }
+  if (ovf) atomicOr(S->err, ERR_BVH_STACK);
+}
+
+}  // namespace mupsi
+
+using namespace mupsi;
+
+// ------------------------------------------------------------ scene handle
+struct mupsi_scene {
+  DScene h;                 // host copy (pointers are device pointers)
+  DScene* d = nullptr;      // device copy
+  std::vector<void*> allocs;
+  int width = 0, height = 0, max_bounce = 0;
+  // progressive framebuffer: running sum and passes so far
+  float* sum = nullptr;
+  int passes_done = 0;
+  int next_pass = -1;  // pass after the last one accumulated
+  // wave buffers (grow-only)
+  Paths paths{};
+  void* paths_mem = nullptr;
+  int64_t paths_cap = 0;
+  int max_iters = 0;
+  int* err = nullptr;
+  unsigned long long* counters = nullptr;
+  // profiling: per-launch event pairs, recorded while `profile` is set
+  bool profile = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_march, ev_shade;
+  size_t ev_used = 0;
+  double march_ms = 0.0, shade_ms = 0.0;
+  int64_t march_launches = 0, shade_launches = 0;
+  cudaEvent_t next_event() {
+    if (ev_used == ev_pool.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      ev_pool.push_back(e);
+    }
+    return ev_pool[ev_used++];
+  }
+  ~mupsi_scene() {
+    for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+    for (void* p : allocs) cudaFree(p);
+    if (d) cudaFree(d);
+    if (sum) cudaFree(sum);
+    if (paths_mem) cudaFree(paths_mem);
+    if (err) cudaFree(err);
+    if (counters) cudaFree(counters);
+  }
+};
+
+namespace {
+
+int build_scene(const mupsi_scene_desc* desc, mupsi_scene* s) {
+  DScene& S = s->h;
+  std::memset(&S, 0, sizeof S);
+  if (desc->width <= 0 || desc->height <= 0) return fail(MUPSI_ERR_INVALID, "width/height must be positive");
+  if ((int64_t)desc->width * desc->height > (1ll << 28)) return fail(MUPSI_ERR_INVALID, "image too large");
+  if (desc->max_bounce < 0 || desc->max_bounce > 1024) return fail(MUPSI_ERR_INVALID, "max_bounce out of range");
+  if (desc->num_primitives < 0 || desc->num_primitives > MAX_PRIMS)
+    return fail(MUPSI_ERR_INVALID, "at most 16 primitives");
+  if (desc->num_media < 0 || desc->num_media > MAX_MEDIA) return fail(MUPSI_ERR_INVALID, "at most 8 media");
+  if (desc->num_meshes < 0 || desc->num_meshes > MAX_MESHES) return fail(MUPSI_ERR_INVALID, "at most 16 meshes");
+  S.width = desc->width;
+  S.height = desc->height;
+  S.max_bounce = desc->max_bounce;
+  S.gp_mode = desc->gp_mode;
+  S.eps = desc->eps;
+  S.nearteps = desc->nearteps;
+  S.has_sky = desc->has_sky;
+  S.sky = ld3(desc->sky);
+  // Camera (camera.h:13-19)
+  S.cpos = ld3(desc->cam_pos);
+  S.cdir = normalized(ld3(desc->cam_dir));
+  v3 up = normalized(ld3(desc->cam_up));
+  S.cright = normalized(cross(S.cdir, up));
+  S.cup = normalized(cross(S.cright, S.cdir));
+  S.aspect = (float)desc->width / (float)desc->height;
+  S.tan_half = std::tan(desc->cam_fov / 2.0f);  // fov taken as radians, as camera.cpp:10-11 does
+  S.nmesh = desc->num_meshes;
+  for (int i = 0; i < desc->num_meshes; ++i)
+    if (int e = make_device_mesh(desc->meshes[i], S.meshes[i], s->allocs)) return e;
+  S.nmed = desc->num_media;
+  for (int i = 0; i < desc->num_media; ++i) {
+    const mupsi_medium_desc& m = desc->media[i];
+    if (int e = check_kernel(&m.kernel)) return e;
+    DMedium& dm = S.media[i];
+    dm.mean_type = m.mean_type;
+    dm.center = ld3(m.mean_center);
+    dm.radius = m.mean_radius;
+    dm.mesh = m.mean_mesh;
+    dm.k = make_kparams(m.kernel);
+    if (m.mean_type == MUPSI_MEAN_MESH && (m.mean_mesh < 0 || m.mean_mesh >= desc->num_meshes))
+      return fail(MUPSI_ERR_INVALID, "medium mean_mesh out of range");
+    if (m.mean_type != MUPSI_MEAN_MESH && m.mean_type != MUPSI_MEAN_SPHERE)
+      return fail(MUPSI_ERR_INVALID, "unknown mean_type");
+  }
+  S.nprim = desc->num_primitives;
+  for (int i = 0; i < desc->num_primitives; ++i) {
+    const mupsi_primitive_desc& p = desc->primitives[i];
+    DPrim& dp = S.prims[i];
+    dp.type = p.type;
+    dp.mesh = p.mesh;
+    dp.bsdf = p.bsdf;
+    dp.has_emission = p.has_emission;
+    dp.albedo = ld3(p.albedo);
+    dp.emission = ld3(p.emission);
+    dp.int_medium = p.int_medium;
+    dp.ext_medium = p.ext_medium;
+    if (p.int_medium >= desc->num_media || p.ext_medium >= desc->num_media)
+      return fail(MUPSI_ERR_INVALID, "primitive medium out of range");
+    if (p.bsdf < 0 || p.bsdf > 2) return fail(MUPSI_ERR_INVALID, "unknown bsdf");
+    HostM4 T;
+    if (p.type == MUPSI_PRIM_SPHERE) {
+      T = translate_scale(p.center, p.radius);
+    } else if (p.type == MUPSI_PRIM_MESH) {
+      if (p.mesh < 0 || p.mesh >= desc->num_meshes) return fail(MUPSI_ERR_INVALID, "primitive mesh out of range");
+      T = translate_scale(desc->meshes[p.mesh].position, desc->meshes[p.mesh].scale);
+    } else {
+      return fail(MUPSI_ERR_INVALID, "unknown primitive type");
+    }
+    HostM4 Ti = inverse4(T);
+    std::memcpy(dp.T.m, T.m, sizeof T.m);
+    std::memcpy(dp.Tinv.m, Ti.m, sizeof Ti.m);
+    dp.identity = is_identity4(Ti);
+    if (p.has_emission) S.lights[S.nlights++] = i;
+  }
+  // march step table for the trace loop's medium rays: nearT = nearteps, farT = FLT_MAX
+  {
+    float nt = desc->nearteps, ft = 2000.0f;
+    float dt = std::min(0.5f, (ft - nt) / 100.0f);
+    std::vector<float> tab;
+    float t = nt;
+    while (t < ft && tab.size() < (1u << 20)) {
+      tab.push_back(t);
+      t += dt;
+    }
+    tab.push_back(t);
+    const float* dtab = nullptr;
+    void* p = nullptr;
+    MUPSI_CUDA(cudaMalloc(&p, tab.size() * sizeof(float)));
+    s->allocs.push_back(p);
+    MUPSI_CUDA(cudaMemcpy(p, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice));
+    dtab = (const float*)p;
+    S.tab = dtab;
+    S.tab_steps = (int)tab.size() - 1;
+    S.tab_nt = nt;
+    S.tab_ft = ft;
+    S.tab_dt = dt;
+  }
+  MUPSI_CUDA(cudaMalloc(&s->err, sizeof(int)));
+  MUPSI_CUDA(cudaMemset(s->err, 0, sizeof(int)));
+  S.err = s->err;
+  MUPSI_CUDA(cudaMalloc(&s->counters, 4 * sizeof(unsigned long long)));
+  MUPSI_CUDA(cudaMemset(s->counters, 0, 4 * sizeof(unsigned long long)));
+  S.counters = nullptr;
+  MUPSI_CUDA(cudaMalloc(&s->d, sizeof(DScene)));
+  MUPSI_CUDA(cudaMemcpy(s->d, &S, sizeof(DScene), cudaMemcpyHostToDevice));
+  s->width = desc->width;
+  s->height = desc->height;
+  s->max_bounce = desc->max_bounce;
+  MUPSI_CUDA(cudaMalloc(&s->sum, (size_t)3 * desc->width * desc->height * sizeof(float)));
+  MUPSI_CUDA(cudaMemset(s->sum, 0, (size_t)3 * desc->width * desc->height * sizeof(float)));
+  return MUPSI_OK;
+}
+
+// PathTracer::trace's do-while runs at least one bounce iteration
+int wave_iters(const mupsi_scene* s) { return std::max(1, s->max_bounce); }
+
+int ensure_paths(mupsi_scene* s, int64_t cap) {
+  int iters = wave_iters(s) + 1;
+  if (cap <= s->paths_cap && iters <= s->max_iters) return MUPSI_OK;
+  if (s->paths_mem) {
+    cudaFree(s->paths_mem);
+    s->paths_mem = nullptr;
+  }
+  cap = std::max(cap, s->paths_cap);
+  size_t bytes = 0;
+  auto take = [&](size_t b) {
+    size_t off = bytes;
+    bytes += (b + 255) & ~(size_t)255;
+    return off;
+  };
+  size_t o_o = take(cap * 16), o_d = take(cap * 16), o_t = take(cap * 16), o_e = take(cap * 16),
+         o_r = take(cap * 8), o_ca = take(cap * 16), o_cb = take(cap * 16), o_m = take(cap * 16),
+         o_ha = take(cap * 16), o_hb = take(cap * 16), o_rad = take(cap * 12), o_q0 = take(cap * 4),
+         o_q1 = take(cap * 4), o_q2 = take(cap * 4), o_q3 = take(cap * 4), o_c = take((size_t)(iters + 1) * 8),
+         o_cur = take((size_t)(iters + 1) * 4);
+  char* base = nullptr;
+  MUPSI_CUDA(cudaMalloc((void**)&base, bytes));
+  s->paths_mem = base;
+  Paths& P = s->paths;
+  P.o = (float4*)(base + o_o);
+  P.d = (float4*)(base + o_d);
+  P.thr = (float4*)(base + o_t);
+  P.em = (float4*)(base + o_e);
+  P.rng = (uint2*)(base + o_r);
+  P.ca = (float4*)(base + o_ca);
+  P.cb = (float4*)(base + o_cb);
+  P.meta = (int4*)(base + o_m);
+  P.ha = (float4*)(base + o_ha);
+  P.hb = (float4*)(base + o_hb);
+  P.rad = (float*)(base + o_rad);
+  P.q[0] = (uint32_t*)(base + o_q0);
+  P.q[1] = (uint32_t*)(base + o_q1);
+  P.q[2] = (uint32_t*)(base + o_q2);
+  P.q[3] = (uint32_t*)(base + o_q3);
+  P.counts = (uint32_t*)(base + o_c);
+  P.cursors = (uint32_t*)(base + o_cur);
+  P.cap = cap;
+  s->paths_cap = cap;
+  s->max_iters = iters;
+  return MUPSI_OK;
+}
+
+int g_march_blocks = 0;
+
+// One wave: n paths, from pass0 (or explicit x/y/k arrays). Leaves radiance in P.rad.
+int run_wave(mupsi_scene* s, int64_t n, int pass0, const int32_t* xs, const int32_t* ys, const int32_t* ks,
+             cudaStream_t st) {
+  Paths& P = s->paths;
+  const int iters = wave_iters(s);
+  MUPSI_CUDA(cudaMemsetAsync(P.counts, 0, (size_t)(s->max_iters + 1) * 8, st));
+  MUPSI_CUDA(cudaMemsetAsync(P.cursors, 0, (size_t)(s->max_iters + 1) * 4, st));
+  count_launch(2);
+  int gb = (int)std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 16);
+  k_raygen<<<gb, 256, 0, st>>>(s->d, P, n, pass0, xs, ys, ks);
+  count_launch();
+  if (!g_march_blocks) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_march, 128, 0);
+    g_march_blocks = std::max(1, per_sm) * num_sms();
+  }
+  int sb = (int)std::min<int64_t>((n + 127) / 128, (int64_t)num_sms() * 16);
+  for (int it = 0; it < iters; ++it) {
+    if (s->profile) {
+      cudaEvent_t a = s->next_event(), b = s->next_event(), c = s->next_event();
+      cudaEventRecord(a, st);
+      k_march<<<g_march_blocks, 128, 0, st>>>(s->d, P, it);
+      cudaEventRecord(b, st);
+      k_shade<<<sb, 128, 0, st>>>(s->d, P, it);
+      cudaEventRecord(c, st);
+      s->ev_march.push_back({a, b});
+      s->ev_shade.push_back({b, c});
+    } else {
+      k_march<<<g_march_blocks, 128, 0, st>>>(s->d, P, it);
+      k_shade<<<sb, 128, 0, st>>>(s->d, P, it);
+    }
+    count_launch(2);
+  }
+  MUPSI_CUDA(cudaGetLastError());
+  return MUPSI_OK;
+}
+
+void collect_events(mupsi_scene* s) {
+  for (auto& pr : s->ev_march) {
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, pr.first, pr.second);
+    s->march_ms += ms;
+    s->march_launches++;
+  }
+  for (auto& pr : s->ev_shade) {
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, pr.first, pr.second);
+    s->shade_ms += ms;
+    s->shade_launches++;
+  }
+  s->ev_march.clear();
+  s->ev_shade.clear();
+  s->ev_used = 0;
+}
+
+int check_err(mupsi_scene* s, cudaStream_t st) {
+  int h = 0;
+  MUPSI_CUDA(cudaMemcpyAsync(&h, s->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  MUPSI_CUDA(cudaStreamSynchronize(st));
+  collect_events(s);
+  if (h) {
+    cudaMemsetAsync(s->err, 0, sizeof(int), st);
+    if (h & ERR_BVH_STACK) return fail(MUPSI_ERR_DEVICE_LIMIT, "BVH traversal exceeded the 64-entry stack");
+    return fail(MUPSI_ERR_DEVICE_LIMIT, "march iteration cap reached");
+  }
+  return MUPSI_OK;
+}
+
+int grid_n(int64_t n) { return (int)std::min<int64_t>((n + 127) / 128, (int64_t)num_sms() * 32); }
+
+const int64_t kDefaultWavePaths = 8ll << 20;
+
+}  // namespace
+
+extern "C" {
+
+int mupsi_gpu_scene_create(const mupsi_scene_desc* desc, mupsi_scene** out) {
+  clear_error();
+  if (!desc || !out) return fail(MUPSI_ERR_INVALID, "null argument");
+  auto* s = new mupsi_scene();
+  int e = build_scene(desc, s);
+  if (e) {
+    delete s;
+    return e;
+  }
+  *out = s;
+  return MUPSI_OK;
+}
+
+void mupsi_gpu_scene_destroy(mupsi_scene* scene) {
+  if (scene) cudaDeviceSynchronize();
+  delete scene;
+}
+
+int mupsi_gpu_mean(const mupsi_scene* scene, int32_t medium, int64_t n, const float* p, float* out, mupsi_mem mem,
+                   void* stream) {
+  clear_error();
+  if (!scene || medium < 0 || medium >= scene->h.nmed || n < 0) return fail(MUPSI_ERR_INVALID, "bad argument");
+  if (n == 0) return MUPSI_OK;
+  if (!p || !out) return fail(MUPSI_ERR_INVALID, "null buffer");
+  cudaStream_t st = resolve_stream(stream);
+  Staged<float> dp(st), dout(st);
+  MUPSI_CUDA(dp.in(p, 3 * n, mem));
+  MUPSI_CUDA(dout.out(out, 4 * n, mem));
+  k_mean<<<grid_n(n), 128, 0, st>>>(scene->d, medium, n, dp.ptr, dout.ptr);
+  count_launch();
+  MUPSI_CUDA(cudaGetLastError());
+  MUPSI_CUDA(dout.finish());
+  return check_err(const_cast<mupsi_scene*>(scene), st);
+}
+
+int mupsi_gpu_medium_eval(const mupsi_scene* scene, int32_t medium, int64_t n, const float* p, const uint32_t* seed,
+                          const mupsi_cond* cond, float* out, mupsi_mem mem, void* stream) {
+  clear_error();
+  if (!scene || medium < 0 || medium >= scene->h.nmed || n < 0) return fail(MUPSI_ERR_INVALID, "bad argument");
+  if (n == 0) return MUPSI_OK;
+  if (!p || !seed || !out) return fail(MUPSI_ERR_INVALID, "null buffer");
+  cudaStream_t st = resolve_stream(stream);
+  Staged<float> dp(st), dout(st);
+  Staged<uint32_t> ds(st);
+  Staged<mupsi_cond> dc(st);
+  MUPSI_CUDA(dp.in(p, 3 * n, mem));
+  MUPSI_CUDA(ds.in(seed, n, mem));
+  if (cond) MUPSI_CUDA(dc.in(cond, n, mem));
+  MUPSI_CUDA(dout.out(out, 4 * n, mem));
+  k_medium_eval<<<grid_n(n), 128, 0, st>>>(scene->d, medium, n, dp.ptr, ds.ptr,
+                                           cond ? reinterpret_cast<const Cond*>(dc.ptr) : nullptr, dout.ptr);
+  count_launch();
+  MUPSI_CUDA(cudaGetLastError());
+  MUPSI_CUDA(dout.finish());
+  return check_err(const_cast<mupsi_scene*>(scene), st);
+}
+
+int mupsi_gpu_sample_distance(const mupsi_scene* scene, int32_t medium, int64_t n, const mupsi_ray* rays,
+                              const uint32_t* seed, const mupsi_cond* cond, mupsi_medium_sample* out, mupsi_mem mem,
+                              void* stream) {
+  clear_error();
+  if (!scene || medium < 0 || medium >= scene->h.nmed || n < 0) return fail(MUPSI_ERR_INVALID, "bad argument");
+  if (n == 0) return MUPSI_OK;
+  if (!rays || !seed || !out) return fail(MUPSI_ERR_INVALID, "null buffer");
+  cudaStream_t st = resolve_stream(stream);
+  Staged<mupsi_ray> dr(st);
+  Staged<uint32_t> ds(st);
+  Staged<mupsi_cond> dc(st);
+  Staged<mupsi_medium_sample> dout(st);
+  MUPSI_CUDA(dr.in(rays, n, mem));
+  MUPSI_CUDA(ds.in(seed, n, mem));
+  if (cond) MUPSI_CUDA(dc.in(cond, n, mem));
+  MUPSI_CUDA(dout.out(out, n, mem));
+  k_sample_distance<<<grid_n(n), 128, 0, st>>>(scene->d, medium, n, dr.ptr, ds.ptr,
+                                               cond ? reinterpret_cast<const Cond*>(dc.ptr) : nullptr, dout.ptr);
+  count_launch();
+  MUPSI_CUDA(cudaGetLastError());
+  MUPSI_CUDA(dout.finish());
+  return check_err(const_cast<mupsi_scene*>(scene), st);
+}
+
+int mupsi_gpu_sample_condition(const mupsi_scene* scene, int32_t medium, int64_t n, const mupsi_medium_sample* samples,
+                               const uint32_t* seed, mupsi_cond* out, mupsi_mem mem, void* stream) {
+  clear_error();
+  if (!scene || medium < 0 || medium >= scene->h.nmed || n < 0) return fail(MUPSI_ERR_INVALID, "bad argument");
+  if (n == 0) return MUPSI_OK;
+  if (!samples || !seed || !out) return fail(MUPSI_ERR_INVALID, "null buffer");
+  cudaStream_t st = resolve_stream(stream);
+  Staged<mupsi_medium_sample> dsm(st);
+  Staged<uint32_t> ds(st);
+  Staged<mupsi_cond> dout(st);
+  MUPSI_CUDA(dsm.in(samples, n, mem));
+  MUPSI_CUDA(ds.in(seed, n, mem));
+  MUPSI_CUDA(dout.out(out, n, mem));
+  k_sample_condition<<<grid_n(n), 128, 0, st>>>(scene->d, medium, n, dsm.ptr, ds.ptr, dout.ptr);
+  count_launch();
+  MUPSI_CUDA(cudaGetLastError());
+  MUPSI_CUDA(dout.finish());
+  return check_err(const_cast<mupsi_scene*>(scene), st);
+}
+
+int mupsi_gpu_trace_samples(mupsi_scene* scene, int64_t n, const int32_t* x, const int32_t* y, const int32_t* k,
+                            float* out_rgb, mupsi_mem mem, void* stream) {
+  clear_error();
+  if (!scene || n < 0) return fail(MUPSI_ERR_INVALID, "bad argument");
+  if (n == 0) return MUPSI_OK;
+  if (!x || !y || !k || !out_rgb) return fail(MUPSI_ERR_INVALID, "null buffer");
+  if (n > kDefaultWavePaths * 4) return fail(MUPSI_ERR_INVALID, "too many samples in one call");
+  cudaStream_t st = resolve_stream(stream);
+  if (int e = ensure_paths(scene, n)) return e;
+  Staged<int32_t> dx(st), dy(st), dk(st);
+  MUPSI_CUDA(dx.in(x, n, mem));
+  MUPSI_CUDA(dy.in(y, n, mem));
+  MUPSI_CUDA(dk.in(k, n, mem));
+  if (int e = run_wave(scene, n, 0, dx.ptr, dy.ptr, dk.ptr, st)) return e;
+  if (mem == MUPSI_MEM_DEVICE) {
+    MUPSI_CUDA(cudaMemcpyAsync(out_rgb, scene->paths.rad, n * 12, cudaMemcpyDeviceToDevice, st));
+  } else {
+    MUPSI_CUDA(cudaMemcpyAsync(out_rgb, scene->paths.rad, n * 12, cudaMemcpyDeviceToHost, st));
+  }
+  return check_err(scene, st);
+}
+
+int mupsi_gpu_render(mupsi_scene* scene, const mupsi_render_args* a) {
+  clear_error();
+  if (!scene || !a) return fail(MUPSI_ERR_INVALID, "null argument");
+  if (a->spp_begin < 0 || a->spp_end < a->spp_begin) return fail(MUPSI_ERR_INVALID, "bad pass range");
+  cudaStream_t st = resolve_stream(a->stream);
+  const int64_t wh = (int64_t)scene->width * scene->height;
+  // a call that does not start where the previous one ended starts a new image
+  if (a->spp_begin == 0 || a->spp_begin != scene->next_pass) {
+    MUPSI_CUDA(cudaMemsetAsync(scene->sum, 0, wh * 12, st));
+    scene->passes_done = 0;
+  }
+  double* dmom = nullptr;
+  if (a->moments_out) {
+    MUPSI_CUDA(cudaMallocAsync((void**)&dmom, wh * 6 * sizeof(double), st));
+    MUPSI_CUDA(cudaMemsetAsync(dmom, 0, wh * 6 * sizeof(double), st));
+  }
+  int total = a->spp_end - a->spp_begin;
+  int per_wave = (int)std::max<int64_t>(1, std::min<int64_t>(total, kDefaultWavePaths / wh));
+  if (total > 0) {
+    if (int e = ensure_paths(scene, (int64_t)per_wave * wh)) return e;
+  }
+  int rc = MUPSI_OK;
+  for (int k0 = a->spp_begin; k0 < a->spp_end; k0 += per_wave) {
+    if (a->cancel && *a->cancel) {
+      rc = fail(MUPSI_ERR_CANCELLED, "render cancelled");
+      break;
+    }
+    int passes = std::min(per_wave, a->spp_end - k0);
+    if ((rc = run_wave(scene, (int64_t)passes * wh, k0, nullptr, nullptr, nullptr, st))) break;
+    k_accumulate<<<grid_n(wh), 128, 0, st>>>(scene->paths.rad, passes, wh, scene->sum, dmom);
+    count_launch();
+    scene->passes_done += passes;
+    scene->next_pass = k0 + passes;
+    if (a->on_spp) {
+      cudaError_t e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) {
+        rc = fail(MUPSI_ERR_CUDA, cudaGetErrorString(e));
+        break;
+      }
+      a->on_spp(k0 + passes, a->user);
+    }
+  }
+  if (rc == MUPSI_OK && a->rgb_out && scene->passes_done > 0) {
+    float inv = 1.0f / (float)scene->passes_done;
+    if (a->out_mem == MUPSI_MEM_DEVICE) {
+      k_average<<<grid_n(wh * 3), 128, 0, st>>>(scene->sum, wh * 3, inv, a->rgb_out);
+      count_launch();
+    } else {
+      float* tmp = nullptr;
+      MUPSI_CUDA(cudaMallocAsync((void**)&tmp, wh * 12, st));
+      k_average<<<grid_n(wh * 3), 128, 0, st>>>(scene->sum, wh * 3, inv, tmp);
+      count_launch();
+      MUPSI_CUDA(cudaMemcpyAsync(a->rgb_out, tmp, wh * 12, cudaMemcpyDeviceToHost, st));
+      MUPSI_CUDA(cudaFreeAsync(tmp, st));
+    }
+  }
+  if (dmom) {
+    if (rc == MUPSI_OK) MUPSI_CUDA(cudaMemcpyAsync(a->moments_out, dmom, wh * 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    MUPSI_CUDA(cudaFreeAsync(dmom, st));
+  }
+  int e = check_err(scene, st);
+  return rc ? rc : e;
+}
+
+int mupsi_gpu_scene_profile(mupsi_scene* scene, int32_t enable) {
+  clear_error();
+  if (!scene) return fail(MUPSI_ERR_INVALID, "null scene");
+  MUPSI_CUDA(cudaDeviceSynchronize());
+  collect_events(scene);
+  scene->profile = enable != 0;
+  scene->h.counters = enable ? scene->counters : nullptr;
+  MUPSI_CUDA(cudaMemcpy(scene->d, &scene->h, sizeof(DScene), cudaMemcpyHostToDevice));
+  return MUPSI_OK;
+}
+
+int mupsi_gpu_scene_stats(mupsi_scene* scene, mupsi_render_stats* out, int32_t reset) {
+  clear_error();
+  if (!scene || !out) return fail(MUPSI_ERR_INVALID, "null argument");
+  MUPSI_CUDA(cudaDeviceSynchronize());
+  collect_events(scene);
+  unsigned long long c[4] = {0, 0, 0, 0};
+  MUPSI_CUDA(cudaMemcpy(c, scene->counters, sizeof c, cudaMemcpyDeviceToHost));
+  out->march_steps = c[0];
+  out->psi_evals = c[1];
+  out->marches = c[2];
+  out->impulse_evals = c[3];
+  out->march_ms = scene->march_ms;
+  out->shade_ms = scene->shade_ms;
+  out->march_launches = scene->march_launches;
+  out->shade_launches = scene->shade_launches;
+  if (reset) {
+    MUPSI_CUDA(cudaMemset(scene->counters, 0, sizeof c));
+    scene->march_ms = scene->shade_ms = 0.0;
+    scene->march_launches = scene->shade_launches = 0;
+  }
+  return MUPSI_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,515 @@
+// Device scene and the per-ray routines of the GPIS trace loop: mean functions,
+// the GP medium march (GPMedium::sampleDistance), Renewal+ conditioning,
+// surface intersection, light sampling and BSDF sampling.
+#pragma once
+#include "dmath.cuh"
+#include "geom.cuh"
+#include "gp.cuh"
+
+#define MAX_PRIMS 16
+#define MAX_MEDIA 8
+#define MAX_MESHES 16
+#define TRACE_SEED 42u  // Renderer passes 42 as the hash seed (renderer.cpp:37)
+
+struct DPrim {
+  int type, mesh, bsdf, has_emission;
+  v3 albedo, emission;
+  int int_medium, ext_medium;
+  int identity;
+  m4 T, Tinv;
+};
+struct DMedium {
+  int mean_type;
+  int mesh;
+  v3 center;
+  float radius;
+  KParams k;
+};
+
+// error bits raised by device code
+#define ERR_BVH_STACK 1
+#define ERR_MARCH_GUARD 2
+
+struct DScene {
+  int width, height, max_bounce, gp_mode;
+  v3 cpos, cdir, cright, cup;
+  float tan_half, aspect;
+  float eps, nearteps;
+  int has_sky;
+  v3 sky;
+  int nprim, nmed, nmesh, nlights;
+  int lights[MAX_PRIMS];
+  DPrim prims[MAX_PRIMS];
+  DMedium media[MAX_MEDIA];
+  DMesh meshes[MAX_MESHES];
+  // t_k of the march for rays with near_t == tab_nt and far_t clamped to tab_ft
+  const float* tab;
+  int tab_steps;  // K: tab[K] >= tab_ft, tab[k] < tab_ft for k < K
+  float tab_nt, tab_ft, tab_dt;
+  int* err;
+  unsigned long long* counters;  // nullable: [0] march steps visited, [1] psi evaluations, [2] marches
+};
+
+// ------------------------------------------------------------ mean functions
+// SphereMeanFunction / MeshMeanFunction::eval (meanfunction.cpp:13-26)
+MD float mean_value(const DScene* S, const DMedium& md, v3 p, bool& ovf) {
+  if (md.mean_type == MUPSI_MEAN_SPHERE) return norm3(p - md.center) - md.radius;
+  const DMesh& m = S->meshes[md.mesh];
+  float inside = mesh_inside(m, p, ovf) ? -1.0f : 1.0f;
+  uint32_t tri;
+  v3 q;
+  return inside * mesh_dist(m, p, tri, q, ovf);
+}
+// eval + gradient (meanfunction.cpp:13-39); the mesh gradient reuses the single
+// inside/closest query of the value (the reference repeats both queries).
+MD float4 mean_value_grad(const DScene* S, const DMedium& md, v3 p, bool& ovf) {
+  if (md.mean_type == MUPSI_MEAN_SPHERE) {
+    v3 g = normalized(p - md.center);
+    return make_float4(norm3(p - md.center) - md.radius, g.x, g.y, g.z);
+  }
+  const DMesh& m = S->meshes[md.mesh];
+  float inside = mesh_inside(m, p, ovf) ? -1.0f : 1.0f;
+  uint32_t tri = 0;
+  v3 q;
+  float d = mesh_dist(m, p, tri, q, ovf);
+  v3 g;
+  if (d < 1e-6f) {
+    g = ld3(m.face_n + 3 * (int64_t)tri);
+    if (!m.normal_identity) g = normalized(apply3t(m.Tinv, g));
+  } else {
+    g = normalized(inside * (p - q));
+  }
+  return make_float4(inside * d, g.x, g.y, g.z);
+}
+
+// GPMedium::evalWithGradient(p, seed, state) (gpmedium.cpp:19-41)
+MD float4 medium_eval(const DScene* S, const DMedium& md, v3 p, uint32_t seed, const Cond& c, bool& ovf) {
+  float4 mu = mean_value_grad(S, md, p, ovf);
+  float4 nz = raw_noise(md.k, p, seed);
+  float4 f = make_float4(mu.x + nz.x, mu.y + nz.y, mu.z + nz.z, mu.w + nz.w);
+  return add_cond(md.k, c, p, f);
+}
+
+// ------------------------------------------------------------------ march
+// GPMedium::sampleDistance (gpmedium.cpp:46-103). The reference steps t from
+// nearT by dt (sequential float adds) while t < min(farT, 2000), evaluates
+// f = mu + psi + conditioning at every step and stops at the first step whose
+// sign(f > 0) differs from that of f at the ray origin with |f_origin - f| > 1e-6.
+// Its refinement loop (gpmedium.cpp:67-73) computes an unused value and is not
+// reproduced. Hit t is the step's t; the normal is normalize(grad f) there.
+//
+// Two exact work skips, both of which leave every output unchanged:
+//  * |psi + conditioning| <= B for every p (|w h| <= 1 per impulse, |h| <= 1,
+//    |grad h| <= gradh_max), so a step with |mu| > B has sign(f) = sign(mu)
+//    and needs no psi evaluation;
+//  * mu is a distance (1-Lipschitz along the unit ray), so after a step with
+//    |mu| > B every later step within (|mu| - B) of it keeps that sign too and
+//    is not evaluated at all. Step t values still come from the reference's
+//    sequential additions (a precomputed table for the render's rays).
+struct March {
+  v3 o, d;
+  float nt, ft, dt;
+  uint32_t seed;
+  Cond c;
+  float B;        // bound on |psi + conditioning| with rounding slack
+  float t;
+  int k;
+  bool use_tab;
+  bool init;      // f at the origin not known yet
+  bool fprev_pos;
+  bool fprev_big; // |f_origin| > B: its value never decides the 1e-6 test
+  float fprev;
+  int status;     // 0 running, 1 hit, 2 exited
+  int medium;
+  uint32_t n_steps, n_psi;  // work counters: steps visited (mean evaluated), psi evaluations
+};
+
+// o, d: the Ray's origin and (already normalised) direction
+MD void march_begin(const DScene* S, March& m, v3 o, v3 d, float near_t, float far_t, int medium, uint32_t seed,
+                    const Cond& c) {
+  m.o = o;
+  m.d = d;
+  m.nt = near_t;
+  m.ft = fmin_std(far_t, 2000.0f);
+  m.dt = fmin_std(0.5f, (m.ft - m.nt) / 100.0f);
+  m.seed = seed;
+  m.c = c;
+  const KParams& k = S->media[medium].k;
+  m.B = (k.psi_bound + cond_bound(k, c)) * 1.00001f + 1e-6f;
+  m.t = m.nt;
+  m.k = 0;
+  m.use_tab = S->tab && m.nt == S->tab_nt && m.ft == S->tab_ft && m.dt == S->tab_dt;
+  m.init = true;
+  m.fprev_pos = false;
+  m.fprev_big = false;
+  m.fprev = 0.0f;
+  m.status = 0;
+  m.medium = medium;
+  m.n_steps = 0;
+  m.n_psi = 0;
+}
+
+// first step index after m.k whose t is >= target (at least m.k + 1)
+MD void march_advance(const DScene* S, March& m, float target) {
+  if (m.use_tab) {
+    const int K = S->tab_steps;
+    int kk = m.k + 1;
+    if (target > m.t) {
+      float est = ceilf((target - m.nt) / m.dt) - 1.0f;
+      if (est > (float)kk) kk = est < (float)K ? (int)est : K;
+    }
+    if (kk > K) kk = K;
+    while (kk > m.k + 1 && __ldg(S->tab + kk - 1) >= target) --kk;
+    while (kk < K && __ldg(S->tab + kk) < target) ++kk;
+    m.k = kk;
+    m.t = __ldg(S->tab + kk);
+  } else {
+    // sequential t += dt, as the reference steps. If t + dt rounds back to t
+    // the reference's loop never ends; here the march stops as exited and
+    // raises ERR_MARCH_GUARD, and the add count is capped as well.
+    const float t0 = m.t;
+    int guard = 0;
+    do {
+      m.t += m.dt;
+      m.k++;
+    } while (m.t < target && m.t < m.ft && ++guard < (1 << 22));
+    if (m.t == t0 || guard >= (1 << 22)) {
+      atomicOr(S->err, ERR_MARCH_GUARD);
+      m.status = 2;
+    }
+  }
+}
+
+// Phase A: move through steps that need no psi evaluation. Returns true when
+// the current point needs psi (origin if m.init, else step k); mu is returned.
+MD bool march_cheap(const DScene* S, March& m, float& mu, v3& p, bool& ovf) {
+  const DMedium& md = S->media[m.medium];
+  if (m.init) {
+    p = m.o;
+    mu = mean_value(S, md, p, ovf);
+    if (fabsf(mu) * 0.999999f > m.B) {
+      m.fprev_pos = mu > 0.0f;
+      m.fprev_big = true;
+      m.init = false;
+    } else {
+      return true;
+    }
+  }
+  for (int guard = 0; guard < 1 << 16; ++guard) {
+    if (!(m.t < m.ft)) {
+      m.status = 2;
+      return false;
+    }
+    p = m.o + m.d * m.t;
+    mu = mean_value(S, md, p, ovf);
+    m.n_steps++;
+    if (fabsf(mu) * 0.999999f > m.B) {
+      if ((mu > 0.0f) != m.fprev_pos) {  // sign(f) = sign(mu) differs: hit here
+        m.status = 1;
+        return false;
+      }
+      float target = m.t + (fabsf(mu) - m.B) * 0.9999f - 1e-2f;
+      march_advance(S, m, target);
+      if (m.status != 0) return false;
+    } else {
+      return true;
+    }
+  }
+  atomicOr(S->err, ERR_MARCH_GUARD);
+  m.status = 2;
+  return false;
+}
+
+// Phase B: f at the pending point (value only); decides hit or next step.
+MD void march_psi(const DScene* S, March& m, float mu, v3 p) {
+  const DMedium& md = S->media[m.medium];
+  m.n_psi++;
+  float f = mu + raw_noise_value(md.k, p, m.seed);
+  if (m.c.active) f += cond_value(md.k, m.c, p);
+  if (m.init) {
+    m.fprev = f;
+    m.fprev_pos = f > 0.0f;
+    m.init = false;
+    return;
+  }
+  if ((f > 0.0f) != m.fprev_pos && (m.fprev_big || (double)fabsf(m.fprev - f) > 1e-6)) {
+    m.status = 1;
+    return;
+  }
+  march_advance(S, m, -INFINITY);
+}
+
+// hit point and normal of a finished march
+MD void march_result(const DScene* S, const March& m, mupsi_medium_sample& out, bool& ovf) {
+  out.exited = m.status == 1 ? 0u : 1u;
+  out.t = m.t;
+  if (m.status == 1) {
+    v3 p = m.o + m.d * m.t;
+    float4 f = medium_eval(S, S->media[m.medium], p, m.seed, m.c, ovf);
+    v3 n = normalized(mk3(f.y, f.z, f.w));
+    st3(out.p, p);
+    st3(out.normal, n);
+  } else {
+    st3(out.p, mk3(0, 0, 0));
+    st3(out.normal, mk3(0, 0, 0));
+  }
+}
+
+// Whole march in one thread (batch entry, transmittance).
+MD void march_full(const DScene* S, March& m, bool& ovf) {
+  for (int guard = 0; m.status == 0 && guard < 1 << 16; ++guard) {
+    float mu;
+    v3 p;
+    if (march_cheap(S, m, mu, p, ovf)) march_psi(S, m, mu, p);
+  }
+  if (m.status == 0) {
+    atomicOr(S->err, ERR_MARCH_GUARD);
+    m.status = 2;
+  }
+}
+
+// GPMedium::sampleCondition (gpmedium.cpp:133-161)
+MD Cond sample_condition(const DScene* S, const DMedium& md, v3 P, v3 N, bool exited, uint32_t seed, bool renewal,
+                         bool& ovf) {
+  Cond c;
+  c.active = 0;
+  c.C = mk3(0, 0, 0);
+  c.u = 0.0f;
+  c.g = mk3(0, 0, 0);
+  if (renewal && !exited) {
+    c.active = 1;
+    c.C = P;
+    float4 psi = raw_noise(md.k, P, seed);
+    float4 mu = mean_value_grad(S, md, P, ovf);
+    c.u = -mu.x / md.k.sigma - psi.x;
+    float s = -md.k.L2 / 2.0f;  // oneOverSecondDerivative (kernel.h:66-68)
+    c.g = s * ((N - mk3(mu.y, mu.z, mu.w)) - mk3(psi.y, psi.z, psi.w));
+  }
+  return c;
+}
+
+// --------------------------------------------------------------- surfaces
+struct Hit {
+  int prim;
+  float t;
+  v3 p, Ng;
+};
+
+// Scene::intersect (scene.cpp:25-39) with Sphere/Mesh intersect and intersectInfo
+MD Hit scene_intersect(const DScene* S, Ray& r, bool& ovf) {
+  Hit hi;
+  hi.prim = -1;
+  float mint = 3.402823466e+38f;
+  uint32_t tri = 0;
+  float bu = 0.0f, bv = 0.0f;
+  for (int i = 0; i < S->nprim; ++i) {
+    const DPrim& p = S->prims[i];
+    bool h = false;
+    uint32_t ltri = 0;
+    float lu = 0.0f, lv = 0.0f;
+    if (p.type == MUPSI_PRIM_SPHERE) {
+      v3 O = r.o, D = r.d;
+      if (!p.identity) {
+        O = apply4(p.Tinv, O);
+        D = apply3(p.Tinv, D);
+      }
+      float t = unit_sphere(r.nt, r.ft, O, D);
+      if (t >= 0.0f) {
+        r.ft = t;
+        h = true;
+      }
+    } else {
+      const DMesh& m = S->meshes[p.mesh];
+      Ray lr = r;
+      float tc = 1.0f;
+      if (!p.identity) {  // mesh.cpp:185-209
+        v3 lo = apply4(p.Tinv, r.o);
+        v3 ld = apply3(p.Tinv, r.d);
+        float len = norm3(ld);
+        tc = norm3(apply3(p.T, ld / len));
+        lr = make_ray(lo, ld);
+        lr.nt = r.nt * len;
+        lr.ft = r.ft * len;
+      }
+      if (bvh_intersect(m, lr, ltri, lu, lv, ovf)) {
+        r.ft = lr.ft * tc;
+        h = true;
+      }
+    }
+    if (h && r.ft < mint) {
+      mint = r.ft;
+      hi.prim = i;
+      hi.t = r.ft;
+      hi.p = r.o + r.d * r.ft;
+      tri = ltri;
+      bu = lu;
+      bv = lv;
+    }
+  }
+  if (hi.prim >= 0) {
+    const DPrim& p = S->prims[hi.prim];
+    if (p.type == MUPSI_PRIM_SPHERE) {  // sphere.cpp:56-76
+      v3 pl = p.identity ? hi.p : apply4(p.Tinv, hi.p);
+      v3 ln = normalized(pl);
+      hi.Ng = p.identity ? ln : normalized(apply3t(p.Tinv, ln));
+    } else {  // mesh.cpp:211-234
+      const DMesh& m = S->meshes[p.mesh];
+      v3 ln;
+      if (!m.vert_n) {
+        ln = ld3(m.face_n + 3 * (int64_t)tri);
+      } else {
+        const int32_t* f = m.faces + 3 * (int64_t)tri;
+        float w = 1.0f - bu - bv;
+        v3 n = (w * ld3(m.vert_n + 3 * (int64_t)f[0]) + bu * ld3(m.vert_n + 3 * (int64_t)f[1])) +
+               bv * ld3(m.vert_n + 3 * (int64_t)f[2]);
+        float len = norm3(n);
+        ln = len > 1e-12f ? n / len : ld3(m.face_n + 3 * (int64_t)tri);
+      }
+      hi.Ng = p.identity ? ln : normalized(apply3t(p.Tinv, ln));
+    }
+  }
+  return hi;
+}
+
+// Scene::occluded (scene.cpp:41-48)
+MD bool scene_occluded(const DScene* S, const Ray& r, bool& ovf) {
+  for (int i = 0; i < S->nprim; ++i) {
+    const DPrim& p = S->prims[i];
+    if (p.type == MUPSI_PRIM_SPHERE) {
+      v3 O = r.o, D = r.d;
+      if (!p.identity) {
+        O = apply4(p.Tinv, O);
+        D = apply3(p.Tinv, D);
+      }
+      if (unit_sphere(r.nt, r.ft, O, D) >= 0.0f) return true;
+    } else {
+      const DMesh& m = S->meshes[p.mesh];
+      if (p.identity) {
+        if (bvh_occluded(m, r, ovf)) return true;
+      } else {
+        v3 lo = apply4(p.Tinv, r.o);
+        v3 ld = apply3(p.Tinv, r.d);
+        float len = norm3(ld);
+        Ray lr = make_ray(lo, ld);
+        lr.nt = r.nt * len;
+        lr.ft = r.ft * len;
+        if (bvh_occluded(m, lr, ovf)) return true;
+      }
+    }
+  }
+  return false;
+}
+
+struct LSample {
+  v3 weight, d;
+  float dist, pdf;
+};
+
+// Scene::chooseLight (scene.cpp:50-61), Sphere::sampleDirect (sphere.cpp:91-133),
+// Mesh::sampleDirect (mesh.cpp:252-297)
+MD bool choose_light(const DScene* S, v3 p, uint64_t& rng, LSample& ls) {
+  if (S->nprim == 0 || S->nlights == 0) return false;
+  uint32_t li = pcg_next(rng) % (uint32_t)S->nlights;
+  const DPrim& pr = S->prims[S->lights[li]];
+  if (pr.type == MUPSI_PRIM_SPHERE) {
+    v3 pl = pr.identity ? p : apply4(pr.Tinv, p);
+    v3 dir = -pl;
+    float dist2 = sqn(dir);
+    float d2 = dist2 - 1.0f;
+    if (d2 < 1e-6f) return false;
+    float d = sqrtf(d2);
+    float dist = sqrtf(dist2);
+    dir = dir / dist;
+    float ct = d / dist;
+    float x1 = pcg_next1d(rng), x2 = pcg_next1d(rng);
+    float phi = (float)((double)(x1 * 2.0f) * 3.14159265358979323846);
+    float z = x2 * (1.0f - ct) + ct;
+    float rr = sqrtf(fmax_std(1.0f - z * z, 0.0f));
+    v3 sd = mk3(cosf(phi) * rr, sinf(phi) * rr, z);
+    float Bq = dist * sd.z;
+    float det = sqrtf(fmax_std(Bq * Bq - d2, 0.0f));
+    ls.dist = Bq - det;
+    Frame fr = make_frame(dir);
+    ls.d = to_global(fr, sd);
+    if (!pr.identity) {
+      v3 spl = pl + ls.d * ls.dist;
+      v3 wd = apply4(pr.T, spl) - p;
+      ls.dist = norm3(wd);
+      ls.d = wd / ls.dist;
+    }
+    ls.pdf = (float)(1.0 / (2.0 * 3.14159265358979323846 * (double)(1.0f - ct)));
+    ls.weight = pr.emission / fmax_std(ls.pdf, 1e-6f);
+    return true;
+  }
+  const DMesh& m = S->meshes[pr.mesh];
+  if (m.num_faces == 0 || m.total_area <= 0.0f) return false;
+  float rnd = pcg_next1d(rng);
+  int64_t lo = 0, hi = m.num_faces;
+  while (lo < hi) {
+    int64_t mid = lo + (hi - lo) / 2;
+    if (m.cdf[mid] < rnd)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  int64_t fi = lo >= m.num_faces ? m.num_faces - 1 : lo;
+  float r1 = pcg_next1d(rng), r2 = pcg_next1d(rng);
+  float sr1 = sqrtf(r1);
+  float bu = 1.0f - sr1, bv = r2 * sr1;
+  const int32_t* f = m.faces + 3 * fi;
+  v3 v0 = vert(m, f[0]);
+  v3 pt = (v0 + (vert(m, f[1]) - v0) * bu) + (vert(m, f[2]) - v0) * bv;
+  if (!pr.identity) pt = apply4(pr.T, pt);
+  v3 dir = pt - p;
+  float dist = sqrtf(sqn(dir));
+  ls.d = dir / dist;
+  ls.dist = dist;
+  ls.pdf = 1.0f / m.total_area;
+  ls.weight = pr.emission / fmax_std(ls.pdf, 1e-6f);
+  return true;
+}
+
+// Bsdf::weight toward the light (bsdf.cpp:14-77)
+MD v3 bsdf_weight(int kind, v3 albedo, v3 wi, v3 wo, v3 n) {
+  if (kind == MUPSI_BSDF_LAMBERTIAN) {
+    float cd = dot(wi, n);
+    float pdf = (float)((double)fmax_std(cd, 0.0f) / 3.14159265358979323846);
+    if (pdf == 0.0f) return mk3(0, 0, 0);
+    v3 ev = (albedo * cd) / 3.14159265f;  // Vector3f / M_PI divides by (float)M_PI
+    return ev / pdf;
+  }
+  if (kind == MUPSI_BSDF_NULL) return dot(wi, -wo) > 0.999f ? mk3(1, 1, 1) : mk3(0, 0, 0);
+  v3 wr = (2.0f * dot(wi, n)) * n - wi;
+  return dot(wr, wo) > 0.999f ? mk3(1, 1, 1) : mk3(0, 0, 0);
+}
+
+// Bsdf::sample (bsdf.cpp:23-79): returns wi, sets the weight
+MD v3 bsdf_sample(int kind, v3 albedo, v3 wo, v3 n, uint64_t& rng, v3& weight) {
+  if (kind == MUPSI_BSDF_LAMBERTIAN) {
+    float r1 = pcg_next1d(rng), r2 = pcg_next1d(rng);
+    float phi = (float)(2.0 * 3.14159265358979323846 * (double)r1);
+    float ct = sqrtf(1.0f - r2);
+    float st = sqrtf(r2);
+    // the reference's build evaluates these cos/sin in double precision
+    double sp, cp;
+    sincos((double)phi, &sp, &cp);
+    v3 lw = mk3((float)((double)st * cp), (float)((double)st * sp), ct);
+    Frame fr = make_frame(n);
+    weight = albedo;
+    return to_global(fr, lw);
+  }
+  weight = mk3(1, 1, 1);
+  if (kind == MUPSI_BSDF_NULL) return -wo;
+  return (2.0f * dot(wo, n)) * n - wo;
+}
+
+// Camera::generateRay (camera.cpp:5-20)
+MD Ray camera_ray(const DScene* S, int x, int y) {
+  float cx = ((float)x + 0.5f) / (float)S->width;
+  float cy = ((float)y + 0.5f) / (float)S->height;
+  float nx = (2.0f * cx - 1.0f) * S->aspect * S->tan_half;
+  float ny = (2.0f * cy - 1.0f) * S->tan_half;
+  v3 dc = normalized(mk3(nx, ny, 1.0f));
+  v3 w = normalized((S->cright * dc.x + S->cup * dc.y) + S->cdir * dc.z);
+  return make_ray(S->cpos, normalized(w));
+}

@@ -1,0 +1,70 @@
+"""ctypes binding of libmupsi_gpu.so (include/mupsi_gpu.h).
+
+The product path has no CPU fallback: if the library is missing or no CUDA
+device is present, loading fails with an exception.
+"""
+import ctypes as C
+import os
+
+from . import _abi
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libmupsi_gpu.so")
+
+_lib = None
+
+
+class MupsiError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"mupsi error {code}: {msg}")
+        self.code = code
+
+
+def _setup(L):
+    vp, i64, i32, u32 = C.c_void_p, C.c_int64, C.c_int32, C.c_uint32
+    L.mupsi_gpu_last_error.restype = C.c_char_p
+    L.mupsi_gpu_abi_version.restype = i32
+    L.mupsi_gpu_launch_count.restype = i64
+    L.mupsi_gpu_psi.argtypes = [C.POINTER(_abi.Kernel), i64, vp, vp, vp, vp, C.c_int, vp]
+    L.mupsi_gpu_psi_value.argtypes = [C.POINTER(_abi.Kernel), i64, vp, vp, vp, vp, C.c_int, vp]
+    L.mupsi_bvh_build_host.argtypes = [i64, vp, i64, vp, vp, vp, C.POINTER(i64), C.POINTER(u32)]
+    L.mupsi_gpu_mesh_create.argtypes = [C.POINTER(_abi.MeshDesc), C.POINTER(vp)]
+    L.mupsi_gpu_mesh_destroy.argtypes = [vp]
+    L.mupsi_gpu_mesh_destroy.restype = None
+    L.mupsi_gpu_bvh_intersect.argtypes = [vp, i64, vp, vp, vp, C.c_int, vp]
+    L.mupsi_gpu_bvh_occluded.argtypes = [vp, i64, vp, vp, C.c_int, vp]
+    L.mupsi_gpu_bvh_closest.argtypes = [vp, i64, vp, vp, vp, C.c_int, vp]
+    L.mupsi_gpu_mesh_queries.argtypes = [vp, i64, vp, vp, vp, vp, C.c_int, vp]
+    L.mupsi_gpu_scene_create.argtypes = [C.POINTER(_abi.SceneDesc), C.POINTER(vp)]
+    L.mupsi_gpu_scene_destroy.argtypes = [vp]
+    L.mupsi_gpu_scene_destroy.restype = None
+    L.mupsi_gpu_mean.argtypes = [vp, i32, i64, vp, vp, C.c_int, vp]
+    L.mupsi_gpu_medium_eval.argtypes = [vp, i32, i64, vp, vp, vp, vp, C.c_int, vp]
+    L.mupsi_gpu_sample_distance.argtypes = [vp, i32, i64, vp, vp, vp, vp, C.c_int, vp]
+    L.mupsi_gpu_sample_condition.argtypes = [vp, i32, i64, vp, vp, vp, C.c_int, vp]
+    L.mupsi_gpu_trace_samples.argtypes = [vp, i64, vp, vp, vp, vp, C.c_int, vp]
+    L.mupsi_gpu_render.argtypes = [vp, C.POINTER(_abi.RenderArgs)]
+    L.mupsi_gpu_scene_profile.argtypes = [vp, i32]
+    L.mupsi_gpu_scene_stats.argtypes = [vp, C.POINTER(_abi.RenderStats), i32]
+    return L
+
+
+def load():
+    """Load libmupsi_gpu.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} is missing: build it with `python -m mupsi_b200.build`")
+        _lib = _setup(C.CDLL(LIB_PATH))
+        if _lib.mupsi_gpu_abi_version() != 1:
+            raise RuntimeError("libmupsi_gpu.so ABI version mismatch")
+    return _lib
+
+
+def check(code):
+    if code != _abi.OK:
+        raise MupsiError(code, load().mupsi_gpu_last_error().decode())
+    return code
+
+
+def launch_count():
+    return load().mupsi_gpu_launch_count()

@@ -140,7 +140,7 @@ class PortOracle:
         p = _f(p)
         n = len(p)
         out = np.zeros((n, 4), np.float64)
-        absv = np.zeros(n, np.float64)
+        absv = np.zeros((n, 4), np.float64)
         self.L.mo_psi_f64(C.byref(kernel), n, p, _u(seed), out, absv.ctypes.data)
         return out, absv
 

@@ -333,7 +333,7 @@ void mo_psi_f64(const mupsi_kernel* kk, int64_t n, const float* p, const uint32_
   for (int64_t q = 0; q < n; ++q) {
     v3 P = vload(p + 3 * q);
     int cx = (int)(P.x / k.kr), cy = (int)(P.y / k.kr), cz = (int)(P.z / k.kr);
-    double sv = 0, sg[3] = {0, 0, 0}, sa = 0;
+    double sv = 0, sg[3] = {0, 0, 0}, sa = 0, sga[3] = {0, 0, 0};
     for (int dx = -1; dx <= 1; ++dx)
       for (int dy = -1; dy <= 1; ++dy)
         for (int dz = -1; dz <= 1; ++dz) {
@@ -350,12 +350,18 @@ void mo_psi_f64(const mupsi_kernel* kk, int64_t n, const float* p, const uint32_
             double h = exp(-(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) / L2);
             sv += w * h;
             sa += h;
-            for (int c = 0; c < 3; ++c) sg[c] += w * h * (-2.0 / L2) * d[c];
+            for (int c = 0; c < 3; ++c) {
+              sg[c] += w * h * (-2.0 / L2) * d[c];
+              sga[c] += fabs(h * (-2.0 / L2) * d[c]);
+            }
           }
         }
     out[4 * q] = sv * scale;
     for (int c = 0; c < 3; ++c) out[4 * q + 1 + c] = sg[c] * scale;
-    if (out_abs) out_abs[q] = sa * fabs(scale);
+    if (out_abs) {
+      out_abs[4 * q] = sa * fabs(scale);
+      for (int c = 0; c < 3; ++c) out_abs[4 * q + 1 + c] = sga[c] * fabs(scale);
+    }
   }
 }
 

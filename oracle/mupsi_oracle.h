@@ -33,8 +33,9 @@ void mo_constant_sampler(uint32_t seed, float* x, float* y, uint32_t* i);
 void mo_psi(const mupsi_kernel* k, int64_t n, const float* p, const uint32_t* seed, const mupsi_cond* cond,
             float* out);
 /* Same impulses (positions from FP32 as the reference computes them), sums in FP64.
- * out[n*4] doubles; also out_abs[n] = sum over impulses of |w*h| * sigma/sqrt(Var)
- * (the conditioning scale of the value sum), nullable. */
+ * out[n*4] doubles; also out_abs[n*4] (nullable) = the sums of the absolute values
+ * of the terms of each output times sigma/sqrt(Var): the scale against which a
+ * sum's rounding error is measured. */
 void mo_psi_f64(const mupsi_kernel* k, int64_t n, const float* p, const uint32_t* seed, double* out,
                 double* out_abs);
 /* Impulse listing for one (p, seed): positions s[27*ppc*3], weights w[27*ppc],

@@ -1,0 +1,158 @@
+"""Generate the golden fixtures from the reference's own sources.
+
+Runs the reference compiled from source (oracle/_ref/libmupsi_ref_parity.so,
+built by `make -C oracle ref` from the reference tree) on seeded synthetic
+inputs and stores inputs and outputs as .npz files next to this script. The
+reference ships no tests or golden vectors, so these fixtures are what pins
+the CPU oracle (oracle/libmupsi_oracle.so) in the CPU-only test suite.
+
+    python tests/golden/make_golden.py
+"""
+import json
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), "..", ".."))
+sys.path.insert(0, ROOT)
+from oracle import bind  # noqa: E402
+from mupsi_b200 import scene as S  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+FMAX = np.finfo(np.float32).max
+
+
+def psi_sweep(R, rng):
+    """ConfigGP-noise sweep points: L in {0.5,1,4} x aniso {(1,1,1),(1,1,4)} x ppc {1,3,8}."""
+    out = {}
+    n = 96
+    for L in (0.5, 1.0, 4.0):
+        for an in ((1, 1, 1), (1, 1, 4)):
+            for ppc in (1, 3, 8):
+                k = bind.kernel_struct(1.0, L, an, ppc)
+                p = rng.uniform(-150, 150, (n, 3)).astype(np.float32)
+                # include negative coordinates near cell boundaries (trunc vs floor)
+                p[:8] = (np.round(p[:8] / L) * L).astype(np.float32)
+                p[8:16] = -np.abs(p[8:16]) * 1e-3
+                s = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+                key = f"L{L}_a{an[2]}_p{ppc}"
+                out[key + "_p"] = p
+                out[key + "_seed"] = s
+                out[key + "_psi"] = R.psi(k, p, s)
+    return out
+
+
+def main():
+    R = bind.RefOracle("ref")
+    rng = np.random.default_rng(20261203)
+    data = {}
+    # math/random.h: make_seed, Random stream, ConstantSampler
+    args = rng.integers(-2**31, 2**31, (64, 5)).astype(np.int64)
+    data["seed_args"] = args
+    data["seed4"] = np.array([R.make_seed4(*map(int, a[:4])) for a in args], np.uint32)
+    data["seed5"] = np.array([R.make_seed5(*map(int, a)) for a in args], np.uint32)
+    seeds = np.array([0, 1, 42, 2**32 - 1, 123456789], np.uint64)
+    data["rng_seeds"] = seeds
+    data["rng_u32"] = np.stack([R.random_stream(int(s), 16)[0] for s in seeds])
+    data["rng_f32"] = np.stack([R.random_stream(int(s), 16)[1] for s in seeds])
+    data["cs_seeds"] = seeds.astype(np.uint32)
+    cs = [R.constant_sampler(int(s) & 0xFFFFFFFF) for s in seeds]
+    data["cs_xy"] = np.array([[c[0], c[1]] for c in cs], np.float32)
+    data["cs_i"] = np.array([c[2] for c in cs], np.uint32)
+    np.savez_compressed(os.path.join(OUT, "random.npz"), **data)
+
+    np.savez_compressed(os.path.join(OUT, "psi_sweep.npz"), **psi_sweep(R, rng))
+
+    # BVH on a displaced icosphere (level 3, 1280 faces)
+    v, f = S.displaced_icosphere(3, seed=7)
+    h, nodes, idx, root = R.bvh_build(v, f)
+    n = 512
+    o = rng.uniform(-400, 400, (n, 3)).astype(np.float32)
+    o[:, 2] -= 300
+    tgt = (rng.normal(size=(n, 3)) * 40 + np.array([0, 0, -300])).astype(np.float32)
+    d = (tgt - o).astype(np.float32)
+    d[n // 2:] = rng.normal(size=(n - n // 2, 3)).astype(np.float32)
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, :3], rays[:, 3:6], rays[:, 7] = o, d, FMAX
+    rays[::7, 6] = 50.0  # some nonzero nearT
+    tri, tuv = R.bvh_intersect(h, rays)
+    occ = R.bvh_occluded(h, rays)
+    q = (rng.uniform(-120, 120, (n, 3)) + np.array([0, 0, -300])).astype(np.float32)
+    ctri, cdq = R.bvh_closest(h, q)
+    td = tempfile.mkdtemp()
+    obj = os.path.join(td, "mesh.obj")
+    S.save_obj(obj, v, f)
+    kmesh = bind.kernel_struct(1.0, 2.0, (1, 1, 1), 3)
+    mh = R.medium_create(1, kmesh, obj_path=obj)
+    ins, mtri, mdq = R.mesh_queries(mh, q)
+    mean = R.mean(mh, q)
+    seeds = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+    cond = np.zeros((n, 8), np.float32)
+    cond[:, :3] = q + rng.normal(size=(n, 3)).astype(np.float32)
+    cond[:, 3] = rng.normal(size=n)
+    cond[:, 4:7] = rng.normal(size=(n, 3))
+    cond[::2, 7] = 1
+    meval = R.medium_eval(mh, q, seeds, cond)
+    np.savez_compressed(os.path.join(OUT, "bvh_mesh.npz"), verts=v, faces=f, nodes=nodes, tri_idx=idx,
+                        root=np.uint32(root), rays=rays, hit_tri=tri, hit_tuv=tuv, occluded=occ, points=q,
+                        closest_tri=ctri, closest_dq=cdq, inside=ins, mesh_tri=mtri, mesh_dq=mdq, mean=mean,
+                        seeds=seeds, cond=cond, medium_eval=meval)
+
+    # sphere-mean medium: march and conditioning (config 0 kernel)
+    k1 = bind.kernel_struct(1.0, 1.0, (1, 1, 1), 3)
+    sh = R.medium_create(0, k1, center=(0, 0, -500), radius=70.0)
+    m = 128
+    o = (rng.uniform(-60, 60, (m, 3)) + np.array([0, 0, -380])).astype(np.float32)
+    tgt = (np.array([0, 0, -500]) + rng.normal(size=(m, 3)) * 30).astype(np.float32)
+    d = (tgt - o).astype(np.float32)
+    d[m // 2:] = rng.normal(size=(m - m // 2, 3)).astype(np.float32)
+    rays = np.zeros((m, 8), np.float32)
+    rays[:, :3], rays[:, 3:6], rays[:, 6], rays[:, 7] = o, d, np.float32(1.5e-3), FMAX
+    mseeds = rng.integers(0, 2**32, m, dtype=np.uint64).astype(np.uint32)
+    mcond = np.zeros((m, 8), np.float32)
+    mcond[:, :3] = o + rng.normal(size=(m, 3)).astype(np.float32) * 2
+    mcond[:, 3] = rng.normal(size=m)
+    mcond[:, 4:7] = rng.normal(size=(m, 3))
+    mcond[m // 2:, 7] = 1
+    sd = R.sample_distance(sh, rays, mseeds, mcond)
+    hits = np.concatenate([sd[:, :1], sd[:, 2:8]], axis=1)
+    sc = R.sample_condition(sh, hits, mseeds, True)
+    sp = (rng.uniform(-100, 100, (m, 3)) + np.array([0, 0, -500])).astype(np.float32)
+    seval = R.medium_eval(sh, sp, mseeds, mcond)
+    np.savez_compressed(os.path.join(OUT, "medium_sphere.npz"), rays=rays, seeds=mseeds, cond=mcond,
+                        sample_distance=sd, sample_condition=sc, points=sp, medium_eval=seval)
+
+    # full trace loop: configuration-0 scene at 24x24, passes 0..2
+    sc0 = S.config0_scene(24, 24, 3)
+    j, _ = sc0.to_json()
+    jp = os.path.join(td, "c0.json")
+    json.dump(j, open(jp, "w"))
+    rh = R.scene_load(jp, sky=1.0)
+    xs, ys, ks = np.meshgrid(np.arange(24), np.arange(24), np.arange(3), indexing="ij")
+    xs, ys, ks = xs.ravel().astype(np.int32), ys.ravel().astype(np.int32), ks.ravel().astype(np.int32)
+    rad = R.trace(rh, xs, ys, ks)
+    fb = R.render(rh, 3)
+    np.savez_compressed(os.path.join(OUT, "trace_c0.npz"), x=xs, y=ys, k=ks, radiance=rad, framebuffer=fb)
+
+    # mesh-mean scene with a Lambertian floor: level-2 mesh at 16x16, 2 passes
+    scm = S.config_mesh_scene(level=2, width=16, height=16, spp=2, seed=5)
+    objs = []
+    for i, mm in enumerate(scm.meshes):
+        pth = os.path.join(td, f"m{i}.obj")
+        S.save_obj(pth, mm.vertices, mm.faces)
+        objs.append(pth)
+    j, extra = scm.to_json(objs)
+    jp = os.path.join(td, "cm.json")
+    json.dump(j, open(jp, "w"))
+    rh = R.scene_load(jp, sky=1.0, extra_meshes=extra)
+    xs, ys, ks = np.meshgrid(np.arange(16), np.arange(16), np.arange(2), indexing="ij")
+    xs, ys, ks = xs.ravel().astype(np.int32), ys.ravel().astype(np.int32), ks.ravel().astype(np.int32)
+    rad = R.trace(rh, xs, ys, ks)
+    np.savez_compressed(os.path.join(OUT, "trace_mesh.npz"), x=xs, y=ys, k=ks, radiance=rad)
+    print("fixtures written to", OUT)
+
+
+if __name__ == "__main__":
+    main()
