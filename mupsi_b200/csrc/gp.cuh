@@ -58,35 +58,77 @@ MD void for_each_impulse(const KParams& k, int nx, int ny, int nz, uint32_t seed
   }
 }
 
-// Unnormalised InternalNoise sums. GRAD = false computes the value only.
+// Unnormalised InternalNoise sums over neighbour cells [c0, c1) of the 27, in
+// the reference's (dx, dy, dz) order (cell c = 9(dx+1) + 3(dy+1) + (dz+1)).
+// GRAD = false computes the value only.
 template <bool GRAD>
-MD void psi_sums(const KParams& k, v3 p, uint32_t seed, float& sv, float& sx, float& sy, float& sz) {
+MD void psi_sums_range(const KParams& k, v3 p, uint32_t seed, int c0, int c1, float& sv, float& sx, float& sy,
+                       float& sz) {
   int cx, cy, cz;
   cell_of(k, p, cx, cy, cz);
   float v = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f;
 #pragma unroll 1
-  for (int dx = -1; dx <= 1; ++dx)
-#pragma unroll 1
-    for (int dy = -1; dy <= 1; ++dy)
-#pragma unroll 1
-      for (int dz = -1; dz <= 1; ++dz) {
-        for_each_impulse(k, cx + dx, cy + dy, cz + dz, seed, [&](v3 s, float w) {
-          v3 d = p - s;
-          float r2 = d.x * d.x + (d.y * d.y + d.z * d.z);
-          float h = ex2_approx(r2 * k.k2);
-          v = fmaf(w, h, v);  // w = +-1: w*h is exact, so this equals v + w*h
-          if (GRAD) {
-            float gs = h * k.c2;
-            gx = fmaf(w, gs * d.x, gx);
-            gy = fmaf(w, gs * d.y, gy);
-            gz = fmaf(w, gs * d.z, gz);
-          }
-        });
+  for (int c = c0; c < c1; ++c) {
+    const int dx = c / 9 - 1, dy = (c / 3) % 3 - 1, dz = c % 3 - 1;
+    for_each_impulse(k, cx + dx, cy + dy, cz + dz, seed, [&](v3 s, float w) {
+      v3 d = p - s;
+      float r2 = d.x * d.x + (d.y * d.y + d.z * d.z);
+      float h = ex2_approx(r2 * k.k2);
+      v = fmaf(w, h, v);  // w = +-1: w*h is exact, so this equals v + w*h
+      if (GRAD) {
+        float gs = h * k.c2;
+        gx = fmaf(w, gs * d.x, gx);
+        gy = fmaf(w, gs * d.y, gy);
+        gz = fmaf(w, gs * d.z, gz);
       }
+    });
+  }
   sv = v;
   sx = gx;
   sy = gy;
   sz = gz;
+}
+template <bool GRAD>
+MD void psi_sums(const KParams& k, v3 p, uint32_t seed, float& sv, float& sx, float& sy, float& sz) {
+  psi_sums_range<GRAD>(k, p, seed, 0, 27, sv, sx, sy, sz);
+}
+
+// A group of G lanes (G a power of two, lanes gbase..gbase+G-1 of the warp)
+// shares one evaluation: lane `sub` sums a contiguous block of the 27 cells and
+// the block sums are added with a butterfly over the group, so every lane of the
+// group ends with the same total. With G = 1 this is the sequential sum above.
+struct Group {
+  int G, sub;
+  unsigned mask;
+};
+MD float group_sum(const Group& g, float v) {
+  for (int off = 1; off < g.G; off <<= 1) v += __shfl_xor_sync(g.mask, v, off, g.G);
+  return v;
+}
+MD void group_cells(const Group& g, int& c0, int& c1) {
+  const int per = (27 + g.G - 1) / g.G;
+  c0 = min(27, g.sub * per);
+  c1 = min(27, c0 + per);
+}
+MD float raw_noise_value_group(const KParams& k, v3 p, uint32_t seed, const Group& g) {
+  int c0, c1;
+  group_cells(g, c0, c1);
+  float v, x, y, z;
+  psi_sums_range<false>(k, p, seed, c0, c1, v, x, y, z);
+  v = group_sum(g, v);
+  return (k.sigma * v) / k.sqrt_var;
+}
+MD float4 raw_noise_group(const KParams& k, v3 p, uint32_t seed, const Group& g) {
+  int c0, c1;
+  group_cells(g, c0, c1);
+  float v, x, y, z;
+  psi_sums_range<true>(k, p, seed, c0, c1, v, x, y, z);
+  v = group_sum(g, v);
+  x = group_sum(g, x);
+  y = group_sum(g, y);
+  z = group_sum(g, z);
+  return make_float4((k.sigma * v) / k.sqrt_var, (k.sigma * x) / k.sqrt_var, (k.sigma * y) / k.sqrt_var,
+                     (k.sigma * z) / k.sqrt_var);
 }
 
 // RawNoise(p, seed) = sigma * InternalNoise / sqrt(Var) (gpnoise.h:44)

@@ -109,27 +109,38 @@ __global__ void k_raygen(const DScene* __restrict__ S, Paths P, int64_t n, int p
   }
 }
 
-// Persistent march over the medium queue of iteration `it`.
+// Persistent march over the medium queue of iteration `it`. Each ray is
+// marched by a group of G lanes that share its psi sums: G = 4 while the queue
+// fills the resident threads, larger (up to 32) as the queue shrinks, so the
+// late bounces' few long marches finish up to 8x sooner than on one lane.
 __global__ void __launch_bounds__(128) k_march(const DScene* __restrict__ S, Paths P, int it) {
   const uint32_t n = P.counts[2 * it];
   const uint32_t* q = P.q[it & 1];
   uint32_t* cursor = P.cursors + it;
   const unsigned lane = threadIdx.x & 31;
+  const uint64_t resident = (uint64_t)gridDim.x * blockDim.x;
+  Group grp;
+  grp.G = 4;
+  while (grp.G < 32 && (uint64_t)n * (uint64_t)(2 * grp.G) <= resident) grp.G <<= 1;
+  grp.sub = (int)(lane & (unsigned)(grp.G - 1));
+  const unsigned gbase = lane & ~(unsigned)(grp.G - 1);
+  grp.mask = grp.G == 32 ? 0xffffffffu : (((1u << grp.G) - 1u) << gbase);
   March m;
   uint32_t idx = 0;
   bool active = false;
   bool ovf = false;
   unsigned long long steps = 0, psis = 0, marches = 0, imps = 0;
   while (true) {
-    // refill idle lanes from the queue (warp-aggregated)
-    unsigned need = __ballot_sync(0xffffffffu, !active);
+    // refill idle groups from the queue (warp-aggregated over group leaders)
+    unsigned need = __ballot_sync(0xffffffffu, !active && grp.sub == 0);
     if (need) {
       uint32_t base = 0;
       int leader = __ffs(need) - 1;
       if ((int)lane == leader) base = atomicAdd(cursor, (uint32_t)__popc(need));
       base = __shfl_sync(0xffffffffu, base, leader);
+      uint32_t j = base + __popc(need & ((1u << lane) - 1u));
+      j = __shfl_sync(0xffffffffu, j, (int)gbase);
       if (!active) {
-        uint32_t j = base + __popc(need & ((1u << lane) - 1u));
         if (j < n) {
           idx = q[j];
           float4 o = P.o[idx], d = P.d[idx];
@@ -138,7 +149,7 @@ __global__ void __launch_bounds__(128) k_march(const DScene* __restrict__ S, Pat
           march_begin(S, m, mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), o.w, 3.402823466e+38f, med,
                       medium_seed(S, meta.x, meta.y, meta.z, meta.w), load_cond(P, idx));
           active = true;
-          marches++;
+          if (grp.sub == 0) marches++;
         }
       }
     }
@@ -146,15 +157,17 @@ __global__ void __launch_bounds__(128) k_march(const DScene* __restrict__ S, Pat
     if (active) {
       float mu;
       v3 p;
-      if (march_cheap(S, m, mu, p, ovf)) march_psi(S, m, mu, p);
+      if (march_cheap(S, m, mu, p, ovf)) march_psi(S, m, mu, p, grp);
       if (m.status != 0) {
         mupsi_medium_sample r;
-        march_result(S, m, r, ovf);
-        P.ha[idx] = make_float4(r.t, r.p[0], r.p[1], r.p[2]);
-        P.hb[idx] = make_float4(r.normal[0], r.normal[1], r.normal[2], __uint_as_float(r.exited));
-        steps += m.n_steps;
-        psis += m.n_psi;
-        imps += (unsigned long long)m.n_psi * 27ull * (unsigned long long)S->media[m.medium].k.ppc;
+        march_result(S, m, r, ovf, grp);
+        if (grp.sub == 0) {
+          P.ha[idx] = make_float4(r.t, r.p[0], r.p[1], r.p[2]);
+          P.hb[idx] = make_float4(r.normal[0], r.normal[1], r.normal[2], __uint_as_float(r.exited));
+          steps += m.n_steps;
+          psis += m.n_psi;
+          imps += (unsigned long long)m.n_psi * 27ull * (unsigned long long)S->media[m.medium].k.ppc;
+        }
         active = false;
       }
     }
@@ -390,7 +403,7 @@ __global__ void k_sample_distance(const DScene* S, int medium, int64_t n, const 
     march_begin(S, m, ld3(r.o), normalized(ld3(r.d)), r.near_t, r.far_t, medium, seed[i], c);
     march_full(S, m, ovf);
     mupsi_medium_sample res;
-    march_result(S, m, res, ovf);
+    march_result(S, m, res, ovf, single_lane());
     out[i] = res;
   }
   if (ovf) atomicOr(S->err, ERR_BVH_STACK);

@@ -220,11 +220,12 @@ MD bool march_cheap(const DScene* S, March& m, float& mu, v3& p, bool& ovf) {
   return false;
 }
 
-// Phase B: f at the pending point (value only); decides hit or next step.
-MD void march_psi(const DScene* S, March& m, float mu, v3 p) {
+// Phase B: f at the pending point (value only); decides hit or next step. The
+// psi sum is shared by the lanes of group g (all of which hold the same march).
+MD void march_psi(const DScene* S, March& m, float mu, v3 p, const Group& g) {
   const DMedium& md = S->media[m.medium];
   m.n_psi++;
-  float f = mu + raw_noise_value(md.k, p, m.seed);
+  float f = mu + raw_noise_value_group(md.k, p, m.seed, g);
   if (m.c.active) f += cond_value(md.k, m.c, p);
   if (m.init) {
     m.fprev = f;
@@ -239,13 +240,23 @@ MD void march_psi(const DScene* S, March& m, float mu, v3 p) {
   march_advance(S, m, -INFINITY);
 }
 
+// GPMedium::evalWithGradient with the psi sum shared by group g
+MD float4 medium_eval_group(const DScene* S, const DMedium& md, v3 p, uint32_t seed, const Cond& c, bool& ovf,
+                            const Group& g) {
+  float4 mu = mean_value_grad(S, md, p, ovf);
+  float4 nz = raw_noise_group(md.k, p, seed, g);
+  float4 f = make_float4(mu.x + nz.x, mu.y + nz.y, mu.z + nz.z, mu.w + nz.w);
+  return add_cond(md.k, c, p, f);
+}
+
 // hit point and normal of a finished march
-MD void march_result(const DScene* S, const March& m, mupsi_medium_sample& out, bool& ovf) {
+// (an exited march leaves t, p and normal zero: sampleDistance does not write them)
+MD void march_result(const DScene* S, const March& m, mupsi_medium_sample& out, bool& ovf, const Group& g) {
   out.exited = m.status == 1 ? 0u : 1u;
-  out.t = m.t;
+  out.t = m.status == 1 ? m.t : 0.0f;
   if (m.status == 1) {
     v3 p = m.o + m.d * m.t;
-    float4 f = medium_eval(S, S->media[m.medium], p, m.seed, m.c, ovf);
+    float4 f = medium_eval_group(S, S->media[m.medium], p, m.seed, m.c, ovf, g);
     v3 n = normalized(mk3(f.y, f.z, f.w));
     st3(out.p, p);
     st3(out.normal, n);
@@ -255,12 +266,21 @@ MD void march_result(const DScene* S, const March& m, mupsi_medium_sample& out, 
   }
 }
 
+MD Group single_lane() {
+  Group g;
+  g.G = 1;
+  g.sub = 0;
+  g.mask = __activemask();
+  return g;
+}
+
 // Whole march in one thread (batch entry, transmittance).
 MD void march_full(const DScene* S, March& m, bool& ovf) {
+  const Group g = single_lane();
   for (int guard = 0; m.status == 0 && guard < 1 << 16; ++guard) {
     float mu;
     v3 p;
-    if (march_cheap(S, m, mu, p, ovf)) march_psi(S, m, mu, p);
+    if (march_cheap(S, m, mu, p, ovf)) march_psi(S, m, mu, p, g);
   }
   if (m.status == 0) {
     atomicOr(S->err, ERR_MARCH_GUARD);
