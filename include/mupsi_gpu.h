@@ -253,6 +253,23 @@ typedef struct {
 } mupsi_render_args;
 int mupsi_gpu_render(mupsi_scene* scene, const mupsi_render_args* args);
 
+/* Allocation-free variant of mupsi_gpu_trace_samples, for callers that cannot
+ * allocate device memory while they render: a render thread that must not
+ * block on the device-wide synchronisation cudaMalloc/cudaFree can imply, or a
+ * host whose allocator owns the GPU's memory budget. It has no counterpart in
+ * the reference. The path state lives in one static device array of the library
+ * (about 3 MB, held by every GPU that loads the library until exit), so:
+ *   - n is at most 16384 samples per call (larger n returns MUPSI_ERR_INVALID);
+ *   - x, y, k and out_rgb must be device memory; nothing is staged or allocated;
+ *   - the first call on a device looks up the array's device address; make that
+ *     first call before any stream capture on that device;
+ *   - all calls share the array: calls that overlap on the GPU (other streams or
+ *     host threads) race on it and must be serialised by the caller;
+ *   - stream NULL means the default stream (no internal stream is created).
+ * The scene itself is created with mupsi_gpu_scene_create beforehand. */
+int mupsi_gpu_trace_samples_noalloc(mupsi_scene* scene, int64_t n, const int32_t* x, const int32_t* y,
+                                    const int32_t* k, float* out_rgb, void* stream);
+
 /* ------------------------------------------------------ instrumentation -- */
 
 /* Work and device time of the wavefront kernels, for roofline reporting. The

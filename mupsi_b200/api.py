@@ -273,6 +273,17 @@ class GpuScene:
         res[:, 7] = out.view(np.uint32)[:, 7].astype(np.float32)
         return res
 
+    def trace_noalloc(self, x, y, k, out, stream=None):
+        """PathTracer::trace for at most 16384 samples without any device
+        allocation: x, y, k (int32) and out ((n, 3) float32) must be CUDA tensors.
+        Calls share one static scratch array; do not overlap them on the GPU."""
+        for a in (x, y, k, out):
+            if not _is_dev(a):
+                raise ValueError("trace_noalloc takes CUDA tensors only")
+        check(load().mupsi_gpu_trace_samples_noalloc(self.h, x.shape[0], _ptr(x), _ptr(y), _ptr(k), _ptr(out),
+                                                     _stream(stream)))
+        return out
+
     def profile(self, enable=True):
         """Count march work and time the wavefront kernels with CUDA events."""
         check(load().mupsi_gpu_scene_profile(self.h, 1 if enable else 0))

@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -710,6 +711,75 @@ int grid_n(int64_t n) { return (int)std::min<int64_t>((n + 127) / 128, (int64_t)
 
 const int64_t kDefaultWavePaths = 8ll << 20;
 
+// ---------------------------------------------------------------------------
+// Allocation-free trace (mupsi_gpu_trace_samples_noalloc). Some hosts cannot
+// call cudaMalloc while they render: a render thread that must not block on
+// the device-wide synchronisation cudaMalloc/cudaFree can imply, or a host that
+// owns the GPU's memory budget through its own allocator. For them the wave's
+// path state lives in one fixed device array, sized for kNoAllocMaxSamples
+// samples per call and held by every GPU that loads this library until the
+// process exits. Calls share the array: counters are cleared at the start of
+// each call, and two calls that overlap on the GPU (different streams or host
+// threads) race on it.
+constexpr int64_t kNoAllocMaxSamples = 16384;
+constexpr int kNoAllocMaxIters = 1025;  // max_bounce <= 1024, plus one
+constexpr size_t na_align(size_t b) { return (b + 255) & ~(size_t)255; }
+constexpr size_t kNoAllocBytes =
+    10 * na_align(kNoAllocMaxSamples * 16) + na_align(kNoAllocMaxSamples * 8) + na_align(kNoAllocMaxSamples * 12) +
+    4 * na_align(kNoAllocMaxSamples * 4) + na_align((size_t)(kNoAllocMaxIters + 1) * 8) +
+    na_align((size_t)(kNoAllocMaxIters + 1) * 4);
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[256] = {};
+
+// Device address of the scratch array on the current device, looked up once per
+// device (the first call on a device does this set-up).
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  MUPSI_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 256) return fail(MUPSI_ERR_UNSUPPORTED, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(MUPSI_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return MUPSI_OK;
+}
+
+// Path-state view over the scratch array (same layout as ensure_paths).
+Paths noalloc_paths(void* base_ptr) {
+  char* base = static_cast<char*>(base_ptr);
+  size_t off = 0;
+  auto take = [&](size_t b) {
+    char* p = base + off;
+    off += na_align(b);
+    return p;
+  };
+  const int64_t cap = kNoAllocMaxSamples;
+  Paths P;
+  P.o = (float4*)take(cap * 16);
+  P.d = (float4*)take(cap * 16);
+  P.thr = (float4*)take(cap * 16);
+  P.em = (float4*)take(cap * 16);
+  P.rng = (uint2*)take(cap * 8);
+  P.ca = (float4*)take(cap * 16);
+  P.cb = (float4*)take(cap * 16);
+  P.meta = (int4*)take(cap * 16);
+  P.ha = (float4*)take(cap * 16);
+  P.hb = (float4*)take(cap * 16);
+  P.rad = (float*)take(cap * 12);
+  for (int i = 0; i < 4; ++i) P.q[i] = (uint32_t*)take(cap * 4);
+  P.counts = (uint32_t*)take((size_t)(kNoAllocMaxIters + 1) * 8);
+  P.cursors = (uint32_t*)take((size_t)(kNoAllocMaxIters + 1) * 4);
+  P.cap = cap;
+  return P;
+}
+
 }  // namespace
 
 extern "C" {
@@ -899,6 +969,51 @@ int mupsi_gpu_render(mupsi_scene* scene, const mupsi_render_args* a) {
   }
   int e = check_err(scene, st);
   return rc ? rc : e;
+}
+
+// Allocation-free variant of mupsi_gpu_trace_samples (no counterpart in the
+// reference): same kernels and results, path state in the library's static
+// scratch array, device buffers only, at most kNoAllocMaxSamples samples.
+int mupsi_gpu_trace_samples_noalloc(mupsi_scene* scene, int64_t n, const int32_t* x, const int32_t* y,
+                                    const int32_t* k, float* out_rgb, void* stream) {
+  clear_error();
+  if (!scene || n < 0) return fail(MUPSI_ERR_INVALID, "bad argument");
+  if (n > kNoAllocMaxSamples)
+    return fail(MUPSI_ERR_INVALID, "trace_samples_noalloc: n = " + std::to_string(n) + " exceeds the maximum of " +
+                                       std::to_string(kNoAllocMaxSamples) + " samples per call");
+  if (n == 0) return MUPSI_OK;
+  if (!x || !y || !k || !out_rgb) return fail(MUPSI_ERR_INVALID, "null buffer");
+  for (const void* ptr : {(const void*)x, (const void*)y, (const void*)k, (const void*)out_rgb}) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess || at.type != cudaMemoryTypeDevice) {
+      cudaGetLastError();
+      return fail(MUPSI_ERR_INVALID, "trace_samples_noalloc takes device buffers only");
+    }
+  }
+  void* scratch = nullptr;
+  if (int e = noalloc_scratch(&scratch)) return e;
+  cudaStream_t st = (cudaStream_t)stream;  // NULL: the default stream (no stream is created here)
+  Paths P = noalloc_paths(scratch);
+  const int iters = std::max(1, scene->max_bounce);
+  // the array keeps the previous call's contents: clear the queue counters and cursors
+  MUPSI_CUDA(cudaMemsetAsync(P.counts, 0, (size_t)(iters + 1) * 8, st));
+  MUPSI_CUDA(cudaMemsetAsync(P.cursors, 0, (size_t)(iters + 1) * 4, st));
+  int gb = (int)std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 16);
+  k_raygen<<<gb, 256, 0, st>>>(scene->d, P, n, 0, x, y, k);
+  if (!g_march_blocks) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_march, 128, 0);
+    g_march_blocks = std::max(1, per_sm) * num_sms();
+  }
+  int sb = (int)std::min<int64_t>((n + 127) / 128, (int64_t)num_sms() * 16);
+  for (int it = 0; it < iters; ++it) {
+    k_march<<<g_march_blocks, 128, 0, st>>>(scene->d, P, it);
+    k_shade<<<sb, 128, 0, st>>>(scene->d, P, it);
+  }
+  count_launch(1 + 2 * iters);
+  MUPSI_CUDA(cudaGetLastError());
+  MUPSI_CUDA(cudaMemcpyAsync(out_rgb, P.rad, n * 12, cudaMemcpyDeviceToDevice, st));
+  return check_err(scene, st);
 }
 
 int mupsi_gpu_scene_profile(mupsi_scene* scene, int32_t enable) {

@@ -43,6 +43,7 @@ def _setup(L):
     L.mupsi_gpu_sample_condition.argtypes = [vp, i32, i64, vp, vp, vp, C.c_int, vp]
     L.mupsi_gpu_trace_samples.argtypes = [vp, i64, vp, vp, vp, vp, C.c_int, vp]
     L.mupsi_gpu_render.argtypes = [vp, C.POINTER(_abi.RenderArgs)]
+    L.mupsi_gpu_trace_samples_noalloc.argtypes = [vp, i64, vp, vp, vp, vp, vp]
     L.mupsi_gpu_scene_profile.argtypes = [vp, i32]
     L.mupsi_gpu_scene_stats.argtypes = [vp, C.POINTER(_abi.RenderStats), i32]
     return L
