@@ -212,14 +212,16 @@ def run_gpu(args):
     gs = GpuScene(sc)
     rend = GpuRenderer()
     rend.prepare_render(gs)
+    from mupsi_b200.multigpu import combine, pass_range
     fb = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    pass0 = rank * SPP
+    # weak scaling: SPP passes per rank, SPP * world passes in the whole image
+    pass0, pass1 = pass_range(SPP * world, world, rank)
 
     def step():
-        rend.start_render_progressive(pass0 + SPP, spp_begin=pass0, out=fb)
+        rend.start_render_progressive(pass1, spp_begin=pass0, out=fb)
         if world > 1:
-            dist.all_reduce(fb)
+            combine(fb, pass1 - pass0, SPP * world)
 
     for _ in range(args.warmup):
         flush.fill_(1)
@@ -257,7 +259,7 @@ def run_gpu(args):
     gs.stats(reset=True)
     for _ in range(2):
         flush.fill_(3)
-        rend.start_render_progressive(pass0 + SPP, spp_begin=pass0, out=fb)
+        rend.start_render_progressive(pass1, spp_begin=pass0, out=fb)
     st = gs.stats(reset=True)
     gs.profile(False)
     peaks, peak_kind = _peaks()
@@ -285,7 +287,7 @@ def run_gpu(args):
         g2 = GpuScene(sc)
         r2 = GpuRenderer()
         r2.prepare_render(g2)
-        r2.start_render_progressive(pass0 + SPP, spp_begin=pass0, out=host_fb)
+        r2.start_render_progressive(pass1, spp_begin=pass0, out=host_fb)
         g2.close()
         if i >= args.warmup:
             e2e_times.append(time.perf_counter() - t0)

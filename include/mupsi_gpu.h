@@ -284,6 +284,13 @@ typedef struct {
   double shade_ms;        /* device time of the shading kernels */
   int64_t march_launches;
   int64_t shade_launches;
+  /* first wave after profiling was enabled, per bounce iteration (up to 16):
+   * rays in the medium queue, live paths, march kernel time */
+  uint32_t iter_medium[16];
+  uint32_t iter_live[16];
+  float iter_march_ms[16];
+  uint64_t mean_evals;    /* exact mesh-mean evaluations inside marches */
+  uint64_t parity_casts;  /* of which needed the Mesh::inside parity cast */
 } mupsi_render_stats;
 /* enable != 0 starts counting work and timing kernels on later renders. */
 int mupsi_gpu_scene_profile(mupsi_scene* scene, int32_t enable);

@@ -141,4 +141,9 @@ class RenderStats(C.Structure):
         ("shade_ms", C.c_double),
         ("march_launches", C.c_int64),
         ("shade_launches", C.c_int64),
+        ("iter_medium", C.c_uint32 * 16),
+        ("iter_live", C.c_uint32 * 16),
+        ("iter_march_ms", C.c_float * 16),
+        ("mean_evals", C.c_uint64),
+        ("parity_casts", C.c_uint64),
     ]

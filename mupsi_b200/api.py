@@ -291,7 +291,11 @@ class GpuScene:
     def stats(self, reset=False):
         st = _abi.RenderStats()
         check(load().mupsi_gpu_scene_stats(self.h, C.byref(st), 1 if reset else 0))
-        return {f: getattr(st, f) for f, _ in _abi.RenderStats._fields_}
+        out = {}
+        for f, _ in _abi.RenderStats._fields_:
+            v = getattr(st, f)
+            out[f] = list(v) if hasattr(v, "__len__") else v
+        return out
 
     def trace(self, x, y, k, stream=None):
         """PathTracer::trace(pixel (x, y), ctx, 42, k) for n samples -> (n, 3) radiance."""

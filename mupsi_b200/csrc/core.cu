@@ -93,7 +93,18 @@ KParams make_kparams(const mupsi_kernel& k) {
   p.k2 = (float)(-1.4426950408889634 / (double)p.L2);
   p.c2 = -2.0f / p.L2;
   p.c4 = 4.0f / (p.L2 * p.L2);
-  p.psi_bound = (float)((double)p.sigma * 27.0 * p.ppc / (double)p.sqrt_var);
+  p.psi_scale = (float)((double)p.sigma * p.ppc / (double)p.sqrt_var);
+  // max over positions a in [0, kr] of 1 + exp(-a^2/L2) + exp(-(kr - a)^2/L2): the
+  // largest per-axis factor of psi_bound_at (the cube is the largest bound)
+  double smax = 0.0;
+  for (int i = 0; i <= 4096; ++i) {
+    double a = (double)p.kr * i / 4096.0;
+    double s = 1.0 + std::exp(-a * a / p.L2) + std::exp(-((double)p.kr - a) * ((double)p.kr - a) / p.L2);
+    smax = std::max(smax, s);
+  }
+  // the grid maximum can undershoot the true maximum by O(kr^2 / 4096^2 / L2)
+  smax = std::min(3.0, smax * (1.0 + 1e-6));
+  p.psi_bound = (float)((double)p.sigma * p.ppc / (double)p.sqrt_var * smax * smax * smax);
   p.gradh_max = (float)(std::sqrt(2.0 / (double)p.L2) * std::exp(-0.5));
   return p;
 }

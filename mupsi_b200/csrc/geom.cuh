@@ -241,12 +241,17 @@ MD float dist2_tri(v3 p, v3 a, v3 b, v3 c, v3& out) {
   return mn;
 }
 // BVH::closest (bvh.cpp:302-353): returns sqrt of the squared distance.
-MD float bvh_closest(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overflow) {
+// best_init (FLT_MAX in the reference) may be any value above the true squared
+// distance: boxes farther than it are pruned from the start and the same
+// minimum is found (`found` reports whether a triangle beat best_init).
+MD float bvh_closest(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overflow, float best_init = 3.402823466e+38f,
+                     bool* found = nullptr) {
   if (m.num_nodes == 0) return 0.0f;
   uint32_t st[BVH_STACK];
   int sp = 0;
   st[sp++] = m.root;
-  float best = 3.402823466e+38f;
+  float best = best_init;
+  if (found) *found = false;
   while (sp > 0) {
     BNode nd = load_node(m.nodes, st[--sp]);
     if (dist2_aabb(p, nd) >= best) continue;
@@ -261,6 +266,7 @@ MD float bvh_closest(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overflow)
           best = d;
           tri = ti;
           q = tmp;
+          if (found) *found = true;
         }
       }
     } else {
@@ -310,6 +316,28 @@ MD float mesh_dist(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overflow) {
   bvh_closest(m, pl, tri, ql, overflow);
   q = apply4(m.T, ql);
   return norm3(q - p);
+}
+
+// Number of surface crossings of the segment o + d t, t in (t0, t1), counted
+// as Mesh::inside counts them along its +x ray (the next search starts 1e-4
+// past the previous hit). For a closed mesh an odd count flips inside/outside.
+MD int segment_crossings(const DMesh& m, v3 o, v3 d, float t0, float t1, bool& overflow) {
+  Ray r;
+  r.o = o;
+  r.d = d;
+  r.nt = t0;
+  r.ft = t1;
+  uint32_t tri;
+  float u, v;
+  int n = 0;
+  for (int guard = 0; guard < 64; ++guard) {
+    if (!bvh_intersect(m, r, tri, u, v, overflow)) break;
+    ++n;
+    r.nt = r.ft + 1e-4f;
+    r.ft = t1;
+    if (!(r.nt < r.ft)) break;
+  }
+  return n;
 }
 
 // intersectUnitSphere (sphere.cpp:11-30)

@@ -11,6 +11,8 @@
 // -|p-s|^2 / L2. The resulting psi differs from the reference by ~1e-7 of the
 // sum of |terms| (tested at 1e-5).
 #pragma once
+#include <climits>
+
 #include "dmath.cuh"
 
 struct KParams {
@@ -21,8 +23,9 @@ struct KParams {
   float k2;          // -log2(e) / L2: exp(-r2/L2) = exp2(r2 * k2)
   float c2;          // -2.0f / L2 (kernel.h:57)
   float c4;          // 4.0f / (L2 * L2) (kernel.h:64)
-  float psi_bound;   // sigma * 27 * ppc / sqrt_var: |psi| <= psi_bound since |w h| <= 1
+  float psi_bound;   // max over p of psi_bound_at(p) (<= sigma * 27 * ppc / sqrt_var)
   float gradh_max;   // max over r of |grad h| = sqrt(2/L2) * exp(-1/2)
+  float psi_scale;   // sigma * ppc / sqrt_var
   int ppc;           // impulses per cell
 };
 
@@ -131,6 +134,86 @@ MD float4 raw_noise_group(const KParams& k, v3 p, uint32_t seed, const Group& g)
                      (k.sigma * z) / k.sqrt_var);
 }
 
+// ---- impulse cache for marches --------------------------------------------
+// Consecutive march steps of one ray share most of their 27 neighbour cells
+// (dt = 0.5 against cells of size kr). A lane group keeps the impulses of the
+// current 3x3x3 window in shared memory, one slot per cell of a mod-3 torus
+// (slot = (cx mod 3, cy mod 3, cz mod 3)): moving the window by one cell
+// replaces exactly the 9 slots of the layer it leaves. Lane `sub` owns the
+// slots s with s % G == sub, so no slot is shared between lanes. A slot holds
+// its cell's coordinates and ppc (s.x, s.y, s.z, w) records, computed exactly
+// as for_each_impulse computes them.
+#define CACHE_MAX_PPC 3
+struct ImpCache {
+  int* tag;      // [27 * 3]: cell coordinates held by each slot
+  float4* imp;   // [27 * CACHE_MAX_PPC]
+};
+// per lane group: the float4 records first, then the tags; a multiple of 16 so
+// every group's records start 16-byte aligned
+constexpr int kCacheBytes = ((27 * CACHE_MAX_PPC * 16 + 27 * 3 * 4) + 15) / 16 * 16;
+static_assert(kCacheBytes % 16 == 0, "lane-group cache stride must keep float4 alignment");
+
+MD int mod3(int x) { return ((x % 3) + 3) % 3; }
+MD void cache_clear(ImpCache c, const Group& g) {
+  for (int s = g.sub; s < 27; s += g.G) c.tag[3 * s] = INT_MIN;
+}
+template <bool GRAD>
+MD void psi_sums_cached(const KParams& k, v3 p, uint32_t seed, const Group& g, ImpCache c, float& sv, float& sx,
+                        float& sy, float& sz) {
+  int cx, cy, cz;
+  cell_of(k, p, cx, cy, cz);
+  float v = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f;
+#pragma unroll 1
+  for (int s = g.sub; s < 27; s += g.G) {
+    // the cell of the window [c-1, c+1]^3 that maps to slot s
+    const int ax = cx - 1 + mod3(s / 9 - (cx - 1));
+    const int ay = cy - 1 + mod3((s / 3) % 3 - (cy - 1));
+    const int az = cz - 1 + mod3(s % 3 - (cz - 1));
+    int* t = c.tag + 3 * s;
+    float4* I = c.imp + CACHE_MAX_PPC * s;
+    if (t[0] != ax || t[1] != ay || t[2] != az) {
+      int i = 0;
+      for_each_impulse(k, ax, ay, az, seed, [&](v3 q, float w) { I[i++] = make_float4(q.x, q.y, q.z, w); });
+      t[0] = ax;
+      t[1] = ay;
+      t[2] = az;
+    }
+    for (int i = 0; i < k.ppc; ++i) {
+      const float4 q = I[i];
+      v3 d = p - mk3(q.x, q.y, q.z);
+      float r2 = d.x * d.x + (d.y * d.y + d.z * d.z);
+      float h = ex2_approx(r2 * k.k2);
+      v = fmaf(q.w, h, v);
+      if (GRAD) {
+        float gs = h * k.c2;
+        gx = fmaf(q.w, gs * d.x, gx);
+        gy = fmaf(q.w, gs * d.y, gy);
+        gz = fmaf(q.w, gs * d.z, gz);
+      }
+    }
+  }
+  sv = v;
+  sx = gx;
+  sy = gy;
+  sz = gz;
+}
+MD float raw_noise_value_cached(const KParams& k, v3 p, uint32_t seed, const Group& g, ImpCache c) {
+  float v, x, y, z;
+  psi_sums_cached<false>(k, p, seed, g, c, v, x, y, z);
+  v = group_sum(g, v);
+  return (k.sigma * v) / k.sqrt_var;
+}
+MD float4 raw_noise_cached(const KParams& k, v3 p, uint32_t seed, const Group& g, ImpCache c) {
+  float v, x, y, z;
+  psi_sums_cached<true>(k, p, seed, g, c, v, x, y, z);
+  v = group_sum(g, v);
+  x = group_sum(g, x);
+  y = group_sum(g, y);
+  z = group_sum(g, z);
+  return make_float4((k.sigma * v) / k.sqrt_var, (k.sigma * x) / k.sqrt_var, (k.sigma * y) / k.sqrt_var,
+                     (k.sigma * z) / k.sqrt_var);
+}
+
 // RawNoise(p, seed) = sigma * InternalNoise / sqrt(Var) (gpnoise.h:44)
 MD float4 raw_noise(const KParams& k, v3 p, uint32_t seed) {
   float v, x, y, z;
@@ -180,4 +263,36 @@ MD float4 add_cond(const KParams& k, const Cond& c, v3 p, float4 f) {
 MD float cond_bound(const KParams& k, const Cond& c) {
   if (!c.active) return 0.0f;
   return fabsf(c.u) + norm3(c.g) * k.gradh_max;
+}
+// ... and at p: with r = |p - C|, h = exp(-r^2/L2) and |grad h| = h 2r/L2
+MD float cond_bound_at(const KParams& k, const Cond& c, v3 p) {
+  if (!c.active) return 0.0f;
+  float r2 = sqn(p - c.C);
+  float h = ex2_approx(r2 * k.k2);
+  return (fabsf(c.u) + norm3(c.g) * (2.0f * sqrtf(r2) / k.L2)) * h;
+}
+
+// Bound on |psi(p)|. Every impulse of neighbour cell (cx+dx, cy+dy, cz+dz) lies
+// in the box [cx+dx, cx+dx+1] x ... (times kr), and h factorises over the axes,
+// so sum |w h| <= ppc * (sum_dx hx)(sum_dy hy)(sum_dz hz) with hx the largest
+// exp(-(p.x - s.x)^2/L2) over the box's x range: 9 exponentials instead of the
+// 27*ppc of psi itself.
+MD float psi_bound_at(const KParams& k, v3 p) {
+  int c[3];
+  cell_of(k, p, c[0], c[1], c[2]);
+  float prod = 1.0f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float pa = get(p, a);
+    float sum = 0.0f;
+#pragma unroll
+    for (int d = -1; d <= 1; ++d) {
+      const float lo = (float)(c[a] + d) * k.kr;
+      const float hi = lo + k.kr;
+      const float dist = fmaxf(0.0f, fmaxf(lo - pa, pa - hi));
+      sum += ex2_approx(dist * dist * k.k2);
+    }
+    prod *= sum;
+  }
+  return k.psi_scale * prod;
 }

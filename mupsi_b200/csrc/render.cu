@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -114,23 +115,31 @@ __global__ void k_raygen(const DScene* __restrict__ S, Paths P, int64_t n, int p
 // marched by a group of G lanes that share its psi sums: G = 4 while the queue
 // fills the resident threads, larger (up to 32) as the queue shrinks, so the
 // late bounces' few long marches finish up to 8x sooner than on one lane.
+template <bool CACHE, int MK>
 __global__ void __launch_bounds__(128) k_march(const DScene* __restrict__ S, Paths P, int it) {
+  extern __shared__ __align__(16) unsigned char smem[];
   const uint32_t n = P.counts[2 * it];
   const uint32_t* q = P.q[it & 1];
   uint32_t* cursor = P.cursors + it;
   const unsigned lane = threadIdx.x & 31;
   const uint64_t resident = (uint64_t)gridDim.x * blockDim.x;
   Group grp;
-  grp.G = 4;
+  grp.G = S->min_group;
   while (grp.G < 32 && (uint64_t)n * (uint64_t)(2 * grp.G) <= resident) grp.G <<= 1;
   grp.sub = (int)(lane & (unsigned)(grp.G - 1));
   const unsigned gbase = lane & ~(unsigned)(grp.G - 1);
   grp.mask = grp.G == 32 ? 0xffffffffu : (((1u << grp.G) - 1u) << gbase);
+  ImpCache cache;
+  if (CACHE) {  // this group's slot table (G >= 4: at most 32 groups per block)
+    unsigned char* base = smem + (size_t)(threadIdx.x / grp.G) * kCacheBytes;
+    cache.tag = reinterpret_cast<int*>(base + 27 * CACHE_MAX_PPC * 16);
+    cache.imp = reinterpret_cast<float4*>(base);
+  }
   March m;
   uint32_t idx = 0;
   bool active = false;
   bool ovf = false;
-  unsigned long long steps = 0, psis = 0, marches = 0, imps = 0;
+  unsigned long long steps = 0, psis = 0, marches = 0, imps = 0, mus = 0, pars = 0;
   while (true) {
     // refill idle groups from the queue (warp-aggregated over group leaders)
     unsigned need = __ballot_sync(0xffffffffu, !active && grp.sub == 0);
@@ -149,6 +158,7 @@ __global__ void __launch_bounds__(128) k_march(const DScene* __restrict__ S, Pat
           int med = __float_as_int(d.w);
           march_begin(S, m, mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), o.w, 3.402823466e+38f, med,
                       medium_seed(S, meta.x, meta.y, meta.z, meta.w), load_cond(P, idx));
+          if (CACHE) cache_clear(cache, grp);
           active = true;
           if (grp.sub == 0) marches++;
         }
@@ -156,18 +166,19 @@ __global__ void __launch_bounds__(128) k_march(const DScene* __restrict__ S, Pat
     }
     if (!__any_sync(0xffffffffu, active)) break;
     if (active) {
-      float mu;
       v3 p;
-      if (march_cheap(S, m, mu, p, ovf)) march_psi(S, m, mu, p, grp);
+      if (march_cheap<MK>(S, m, p, ovf)) march_psi<MK>(S, m, p, grp, ovf, CACHE ? &cache : nullptr);
       if (m.status != 0) {
         mupsi_medium_sample r;
-        march_result(S, m, r, ovf, grp);
+        march_result<MK>(S, m, r, ovf, grp, CACHE ? &cache : nullptr);
         if (grp.sub == 0) {
           P.ha[idx] = make_float4(r.t, r.p[0], r.p[1], r.p[2]);
           P.hb[idx] = make_float4(r.normal[0], r.normal[1], r.normal[2], __uint_as_float(r.exited));
           steps += m.n_steps;
           psis += m.n_psi;
           imps += (unsigned long long)m.n_psi * 27ull * (unsigned long long)S->media[m.medium].k.ppc;
+          mus += m.n_mu;
+          pars += m.n_par;
         }
         active = false;
       }
@@ -180,12 +191,16 @@ __global__ void __launch_bounds__(128) k_march(const DScene* __restrict__ S, Pat
       psis += __shfl_down_sync(0xffffffffu, psis, o);
       marches += __shfl_down_sync(0xffffffffu, marches, o);
       imps += __shfl_down_sync(0xffffffffu, imps, o);
+      mus += __shfl_down_sync(0xffffffffu, mus, o);
+      pars += __shfl_down_sync(0xffffffffu, pars, o);
     }
     if (lane == 0) {
       atomicAdd(&S->counters[0], steps);
       atomicAdd(&S->counters[1], psis);
       atomicAdd(&S->counters[2], marches);
       atomicAdd(&S->counters[3], imps);
+      atomicAdd(&S->counters[4], mus);
+      atomicAdd(&S->counters[5], pars);
     }
   }
 }
@@ -454,6 +469,10 @@ struct mupsi_scene {
   size_t ev_used = 0;
   double march_ms = 0.0, shade_ms = 0.0;
   int64_t march_launches = 0, shade_launches = 0;
+  // first profiled wave: queue sizes and march time per bounce iteration
+  bool iter_pending = false, iter_done = false;
+  std::vector<uint32_t> iter_counts;
+  std::vector<float> iter_march_ms;
   cudaEvent_t next_event() {
     if (ev_used == ev_pool.size()) {
       cudaEvent_t e;
@@ -474,6 +493,12 @@ struct mupsi_scene {
 };
 
 namespace {
+
+bool desc_cacheable(const mupsi_scene_desc* desc) {
+  for (int i = 0; i < desc->num_media; ++i)
+    if (desc->media[i].kernel.points_per_cell > CACHE_MAX_PPC) return false;
+  return true;
+}
 
 int build_scene(const mupsi_scene_desc* desc, mupsi_scene* s) {
   DScene& S = s->h;
@@ -505,6 +530,18 @@ int build_scene(const mupsi_scene_desc* desc, mupsi_scene* s) {
   for (int i = 0; i < desc->num_meshes; ++i)
     if (int e = make_device_mesh(desc->meshes[i], S.meshes[i], s->allocs)) return e;
   S.nmed = desc->num_media;
+  // lane groups share psi sums; a mesh mean's BVH queries would run on every
+  // lane of a group, so scenes with mesh means start from single-lane marches
+  // lane groups of >= 4 share psi sums and, when every medium has at most
+  // CACHE_MAX_PPC impulses per cell, keep the impulse window in shared memory
+  S.min_group = 4;
+  S.sphere_only = 1;
+  for (int i = 0; i < desc->num_media; ++i)
+    if (desc->media[i].mean_type != MUPSI_MEAN_SPHERE) S.sphere_only = 0;
+  // The shared-memory impulse cache measured slower than regenerating impulses
+  // (the march is latency- rather than issue-bound); it stays selectable.
+  S.cache = 0;
+  if (const char* e = std::getenv("MUPSI_MARCH_CACHE")) S.cache = (std::atoi(e) != 0) && desc_cacheable(desc);
   for (int i = 0; i < desc->num_media; ++i) {
     const mupsi_medium_desc& m = desc->media[i];
     if (int e = check_kernel(&m.kernel)) return e;
@@ -516,6 +553,28 @@ int build_scene(const mupsi_scene_desc* desc, mupsi_scene* s) {
     dm.k = make_kparams(m.kernel);
     if (m.mean_type == MUPSI_MEAN_MESH && (m.mean_mesh < 0 || m.mean_mesh >= desc->num_meshes))
       return fail(MUPSI_ERR_INVALID, "medium mean_mesh out of range");
+    dm.bs_c = mk3(0, 0, 0);
+    dm.bs_r = INFINITY;
+    if (m.mean_type == MUPSI_MEAN_MESH && desc->meshes[m.mean_mesh].num_vertices > 0) {
+      // bounding sphere of the world-space vertices: centre of their box, radius
+      // to the farthest vertex, in double with slack for the float comparisons
+      const mupsi_mesh_desc& md = desc->meshes[m.mean_mesh];
+      double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+      auto world = [&](int64_t v, int a) { return (double)md.position[a] + (double)md.scale * md.vertices[3 * v + a]; };
+      for (int64_t v = 0; v < md.num_vertices; ++v)
+        for (int a = 0; a < 3; ++a) {
+          lo[a] = std::min(lo[a], world(v, a));
+          hi[a] = std::max(hi[a], world(v, a));
+        }
+      double c[3] = {(lo[0] + hi[0]) / 2, (lo[1] + hi[1]) / 2, (lo[2] + hi[2]) / 2}, r2 = 0.0;
+      for (int64_t v = 0; v < md.num_vertices; ++v) {
+        double d2 = 0.0;
+        for (int a = 0; a < 3; ++a) d2 += (world(v, a) - c[a]) * (world(v, a) - c[a]);
+        r2 = std::max(r2, d2);
+      }
+      dm.bs_c = mk3((float)c[0], (float)c[1], (float)c[2]);
+      dm.bs_r = (float)(std::sqrt(r2) * (1.0 + 1e-5) + 1e-3 * (1.0 + std::fabs(c[0]) + std::fabs(c[1]) + std::fabs(c[2])));
+    }
     if (m.mean_type != MUPSI_MEAN_MESH && m.mean_type != MUPSI_MEAN_SPHERE)
       return fail(MUPSI_ERR_INVALID, "unknown mean_type");
   }
@@ -575,8 +634,8 @@ int build_scene(const mupsi_scene_desc* desc, mupsi_scene* s) {
   MUPSI_CUDA(cudaMalloc(&s->err, sizeof(int)));
   MUPSI_CUDA(cudaMemset(s->err, 0, sizeof(int)));
   S.err = s->err;
-  MUPSI_CUDA(cudaMalloc(&s->counters, 4 * sizeof(unsigned long long)));
-  MUPSI_CUDA(cudaMemset(s->counters, 0, 4 * sizeof(unsigned long long)));
+  MUPSI_CUDA(cudaMalloc(&s->counters, 8 * sizeof(unsigned long long)));
+  MUPSI_CUDA(cudaMemset(s->counters, 0, 8 * sizeof(unsigned long long)));
   S.counters = nullptr;
   MUPSI_CUDA(cudaMalloc(&s->d, sizeof(DScene)));
   MUPSI_CUDA(cudaMemcpy(s->d, &S, sizeof(DScene), cudaMemcpyHostToDevice));
@@ -637,7 +696,36 @@ int ensure_paths(mupsi_scene* s, int64_t cap) {
   return MUPSI_OK;
 }
 
-int g_march_blocks = 0;
+// Persistent march grid: resident blocks per SM x SMs, for the cached (dynamic
+// shared memory: one slot table per lane group of 4) or uncached kernel.
+struct MarchLaunch {
+  void (*fn)(const DScene*, Paths, int);
+  int blocks;
+  size_t smem;
+};
+// variant: bit 0 = impulse cache, bit 1 = sphere means only
+MarchLaunch march_launch(bool cache, bool sphere_only) {
+  static MarchLaunch ml[4] = {};
+  const int v = (cache ? 1 : 0) | (sphere_only ? 2 : 0);
+  MarchLaunch& m = ml[v];
+  if (!m.blocks) {
+    switch (v) {
+      case 0: m.fn = k_march<false, MEAN_ANY>; break;
+      case 1: m.fn = k_march<true, MEAN_ANY>; break;
+      case 2: m.fn = k_march<false, MEAN_SPHERE_ONLY>; break;
+      default: m.fn = k_march<true, MEAN_SPHERE_ONLY>; break;
+    }
+    m.smem = cache ? (size_t)(128 / 4) * kCacheBytes : 0;
+    if (cache) cudaFuncSetAttribute(m.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m.smem);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, m.fn, 128, m.smem);
+    m.blocks = std::max(1, per_sm) * num_sms();
+  }
+  return m;
+}
+void launch_march(const MarchLaunch& ml, const DScene* d, const Paths& P, int it, cudaStream_t st) {
+  ml.fn<<<ml.blocks, 128, ml.smem, st>>>(d, P, it);
+}
 
 // One wave: n paths, from pass0 (or explicit x/y/k arrays). Leaves radiance in P.rad.
 int run_wave(mupsi_scene* s, int64_t n, int pass0, const int32_t* xs, const int32_t* ys, const int32_t* ks,
@@ -650,24 +738,20 @@ int run_wave(mupsi_scene* s, int64_t n, int pass0, const int32_t* xs, const int3
   int gb = (int)std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 16);
   k_raygen<<<gb, 256, 0, st>>>(s->d, P, n, pass0, xs, ys, ks);
   count_launch();
-  if (!g_march_blocks) {
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_march, 128, 0);
-    g_march_blocks = std::max(1, per_sm) * num_sms();
-  }
+  const MarchLaunch ml = march_launch(s->h.cache != 0, s->h.sphere_only != 0);
   int sb = (int)std::min<int64_t>((n + 127) / 128, (int64_t)num_sms() * 16);
   for (int it = 0; it < iters; ++it) {
     if (s->profile) {
       cudaEvent_t a = s->next_event(), b = s->next_event(), c = s->next_event();
       cudaEventRecord(a, st);
-      k_march<<<g_march_blocks, 128, 0, st>>>(s->d, P, it);
+      launch_march(ml, s->d, P, it, st);
       cudaEventRecord(b, st);
       k_shade<<<sb, 128, 0, st>>>(s->d, P, it);
       cudaEventRecord(c, st);
       s->ev_march.push_back({a, b});
       s->ev_shade.push_back({b, c});
     } else {
-      k_march<<<g_march_blocks, 128, 0, st>>>(s->d, P, it);
+      launch_march(ml, s->d, P, it, st);
       k_shade<<<sb, 128, 0, st>>>(s->d, P, it);
     }
     count_launch(2);
@@ -677,11 +761,18 @@ int run_wave(mupsi_scene* s, int64_t n, int pass0, const int32_t* xs, const int3
 }
 
 void collect_events(mupsi_scene* s) {
+  bool first = s->iter_pending && !s->iter_done;
   for (auto& pr : s->ev_march) {
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, pr.first, pr.second);
     s->march_ms += ms;
     s->march_launches++;
+    if (first && (int)s->iter_march_ms.size() < s->max_iters) s->iter_march_ms.push_back(ms);
+  }
+  if (first && !s->ev_march.empty()) {
+    s->iter_counts.resize(2 * (size_t)(s->max_iters + 1));
+    cudaMemcpy(s->iter_counts.data(), s->paths.counts, s->iter_counts.size() * 4, cudaMemcpyDeviceToHost);
+    s->iter_done = true;
   }
   for (auto& pr : s->ev_shade) {
     float ms = 0.0f;
@@ -1000,14 +1091,10 @@ int mupsi_gpu_trace_samples_noalloc(mupsi_scene* scene, int64_t n, const int32_t
   MUPSI_CUDA(cudaMemsetAsync(P.cursors, 0, (size_t)(iters + 1) * 4, st));
   int gb = (int)std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 16);
   k_raygen<<<gb, 256, 0, st>>>(scene->d, P, n, 0, x, y, k);
-  if (!g_march_blocks) {
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_march, 128, 0);
-    g_march_blocks = std::max(1, per_sm) * num_sms();
-  }
+  const MarchLaunch ml = march_launch(scene->h.cache != 0, scene->h.sphere_only != 0);
   int sb = (int)std::min<int64_t>((n + 127) / 128, (int64_t)num_sms() * 16);
   for (int it = 0; it < iters; ++it) {
-    k_march<<<g_march_blocks, 128, 0, st>>>(scene->d, P, it);
+    launch_march(ml, scene->d, P, it, st);
     k_shade<<<sb, 128, 0, st>>>(scene->d, P, it);
   }
   count_launch(1 + 2 * iters);
@@ -1022,6 +1109,10 @@ int mupsi_gpu_scene_profile(mupsi_scene* scene, int32_t enable) {
   MUPSI_CUDA(cudaDeviceSynchronize());
   collect_events(scene);
   scene->profile = enable != 0;
+  scene->iter_pending = enable != 0;
+  scene->iter_done = false;
+  scene->iter_counts.clear();
+  scene->iter_march_ms.clear();
   scene->h.counters = enable ? scene->counters : nullptr;
   MUPSI_CUDA(cudaMemcpy(scene->d, &scene->h, sizeof(DScene), cudaMemcpyHostToDevice));
   return MUPSI_OK;
@@ -1032,16 +1123,23 @@ int mupsi_gpu_scene_stats(mupsi_scene* scene, mupsi_render_stats* out, int32_t r
   if (!scene || !out) return fail(MUPSI_ERR_INVALID, "null argument");
   MUPSI_CUDA(cudaDeviceSynchronize());
   collect_events(scene);
-  unsigned long long c[4] = {0, 0, 0, 0};
+  unsigned long long c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   MUPSI_CUDA(cudaMemcpy(c, scene->counters, sizeof c, cudaMemcpyDeviceToHost));
   out->march_steps = c[0];
   out->psi_evals = c[1];
   out->marches = c[2];
   out->impulse_evals = c[3];
+  out->mean_evals = c[4];
+  out->parity_casts = c[5];
   out->march_ms = scene->march_ms;
   out->shade_ms = scene->shade_ms;
   out->march_launches = scene->march_launches;
   out->shade_launches = scene->shade_launches;
+  for (int i = 0; i < 16; ++i) {
+    out->iter_medium[i] = 2 * i < (int)scene->iter_counts.size() ? scene->iter_counts[2 * i] : 0;
+    out->iter_live[i] = 2 * i + 1 < (int)scene->iter_counts.size() ? scene->iter_counts[2 * i + 1] : 0;
+    out->iter_march_ms[i] = i < (int)scene->iter_march_ms.size() ? scene->iter_march_ms[i] : 0.0f;
+  }
   if (reset) {
     MUPSI_CUDA(cudaMemset(scene->counters, 0, sizeof c));
     scene->march_ms = scene->shade_ms = 0.0;

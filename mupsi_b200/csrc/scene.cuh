@@ -23,6 +23,8 @@ struct DMedium {
   int mesh;
   v3 center;
   float radius;
+  v3 bs_c;     // mesh mean: bounding sphere of the world-space mesh (with slack)
+  float bs_r;
   KParams k;
 };
 
@@ -48,11 +50,21 @@ struct DScene {
   float tab_nt, tab_ft, tab_dt;
   int* err;
   unsigned long long* counters;  // nullable: [0] march steps visited, [1] psi evaluations, [2] marches
+  int min_group;                 // smallest lane group per march
+  int cache;                     // marches keep impulses in shared memory (every medium has ppc <= 3)
+  int sphere_only;               // every mean is a sphere: the march kernel without BVH code
 };
 
 // ------------------------------------------------------------ mean functions
 // SphereMeanFunction / MeshMeanFunction::eval (meanfunction.cpp:13-26)
+// MK: MEAN_ANY dispatches on the medium's mean type at run time; MEAN_SPHERE_ONLY
+// compiles the sphere mean alone (a kernel for scenes without mesh means
+// carries no BVH code and keeps its registers).
+#define MEAN_ANY (-1)
+#define MEAN_SPHERE_ONLY 0
+template <int MK = MEAN_ANY>
 MD float mean_value(const DScene* S, const DMedium& md, v3 p, bool& ovf) {
+  if constexpr (MK == MEAN_SPHERE_ONLY) return norm3(p - md.center) - md.radius;
   if (md.mean_type == MUPSI_MEAN_SPHERE) return norm3(p - md.center) - md.radius;
   const DMesh& m = S->meshes[md.mesh];
   float inside = mesh_inside(m, p, ovf) ? -1.0f : 1.0f;
@@ -62,11 +74,13 @@ MD float mean_value(const DScene* S, const DMedium& md, v3 p, bool& ovf) {
 }
 // eval + gradient (meanfunction.cpp:13-39); the mesh gradient reuses the single
 // inside/closest query of the value (the reference repeats both queries).
+template <int MK = MEAN_ANY>
 MD float4 mean_value_grad(const DScene* S, const DMedium& md, v3 p, bool& ovf) {
-  if (md.mean_type == MUPSI_MEAN_SPHERE) {
+  if (MK == MEAN_SPHERE_ONLY || md.mean_type == MUPSI_MEAN_SPHERE) {
     v3 g = normalized(p - md.center);
     return make_float4(norm3(p - md.center) - md.radius, g.x, g.y, g.z);
   }
+  if constexpr (MK == MEAN_SPHERE_ONLY) return make_float4(0, 0, 0, 0);
   const DMesh& m = S->meshes[md.mesh];
   float inside = mesh_inside(m, p, ovf) ? -1.0f : 1.0f;
   uint32_t tri = 0;
@@ -111,7 +125,7 @@ struct March {
   float nt, ft, dt;
   uint32_t seed;
   Cond c;
-  float B;        // bound on |psi + conditioning| with rounding slack
+  float B;        // bound on |psi + conditioning| at every p, with rounding slack
   float t;
   int k;
   bool use_tab;
@@ -121,7 +135,16 @@ struct March {
   float fprev;
   int status;     // 0 running, 1 hit, 2 exited
   int medium;
-  uint32_t n_steps, n_psi;  // work counters: steps visited (mean evaluated), psi evaluations
+  uint32_t n_steps, n_psi;  // work counters: steps visited, psi evaluations
+  uint32_t n_mu, n_par;     // mesh means: exact evaluations, parity casts among them
+  // Lazy mean (meshes, where mu costs BVH traversals): the last exact mu and
+  // its ray parameter bound |mu| at any later step; mu is only evaluated when
+  // that bound cannot decide the sign of f.
+  bool lazy;
+  float mu_j, t_j;
+  // pending step between the two phases
+  bool pend_exact;  // pend_mu holds the exact mean at the pending point
+  float pend_mu, pend_lb, pend_sgn;
 };
 
 // o, d: the Ray's origin and (already normalised) direction
@@ -147,6 +170,49 @@ MD void march_begin(const DScene* S, March& m, v3 o, v3 d, float near_t, float f
   m.medium = medium;
   m.n_steps = 0;
   m.n_psi = 0;
+  m.n_mu = 0;
+  m.n_par = 0;
+  m.lazy = S->media[medium].mean_type == MUPSI_MEAN_MESH;
+  m.mu_j = 0.0f;
+  m.t_j = 0.0f;
+  m.pend_exact = false;
+  m.pend_mu = 0.0f;
+  m.pend_lb = 0.0f;
+}
+
+// Lower bound on |mu| at ray parameter t from the last exact value: mu is a
+// distance along a unit-speed ray (1-Lipschitz); the slack covers the rounding
+// of p = o + d t and of the distance computation.
+MD float mu_lower(const March& m, float t) { return fabsf(m.mu_j) - fabsf(t - m.t_j) * 1.0001f - 1e-2f; }
+
+// Exact mean at p = o + d t after an exact value mu_j at t_j on the same ray.
+// For a mesh (MeshMeanFunction::eval = inside ? -dist : dist):
+//  * dist: BVH::closest started from the bound (|mu_j| + |t - t_j|)^2 on the
+//    squared distance instead of FLT_MAX (same minimum, fewer nodes);
+//  * sign: when |t - t_j| < |mu_j| no surface lies between the two points and
+//    the sign is mu_j's; otherwise the crossings of the march segment flip it
+//    (for a closed mesh the parity test of Mesh::inside changes exactly there).
+// mu_j == 0 (on the surface) or a transformed mesh use the full queries.
+template <int MK = MEAN_ANY>
+MD float mean_exact(const DScene* S, March& m, v3 p, float t, bool& ovf) {
+  const DMedium& md = S->media[m.medium];
+  if constexpr (MK == MEAN_SPHERE_ONLY) return mean_value<MK>(S, md, p, ovf);
+  if (!m.lazy) return mean_value(S, md, p, ovf);
+  m.n_mu++;
+  const DMesh& mesh = S->meshes[md.mesh];
+  if (m.mu_j == 0.0f || !mesh.identity) {
+    m.n_par++;
+    return mean_value(S, md, p, ovf);
+  }
+  float sign = m.mu_j > 0.0f ? 1.0f : -1.0f;
+  if (mu_lower(m, t) <= 0.0f && (segment_crossings(mesh, m.o, m.d, m.t_j, t, ovf) & 1)) sign = -sign;
+  float ub = fabsf(m.mu_j) + fabsf(t - m.t_j) * 1.0001f + 1e-2f;
+  uint32_t tri;
+  v3 q = mk3(0, 0, 0);
+  bool found = false;
+  bvh_closest(mesh, p, tri, q, ovf, ub * ub * 1.0001f + 1e-4f, &found);
+  if (!found) bvh_closest(mesh, p, tri, q, ovf);  // the bound was too tight: full query
+  return sign * norm3(q - p);
 }
 
 // first step index after m.k whose t is >= target (at least m.k + 1)
@@ -180,18 +246,37 @@ MD void march_advance(const DScene* S, March& m, float target) {
   }
 }
 
+// Bound on |psi + conditioning| at p (with rounding slack).
+MD float noise_bound_at(const KParams& k, const Cond& c, v3 p) {
+  return psi_bound_at(k, p) * 1.001f + cond_bound_at(k, c, p) * 1.001f + 2e-5f;
+}
+
 // Phase A: move through steps that need no psi evaluation. Returns true when
-// the current point needs psi (origin if m.init, else step k); mu is returned.
-MD bool march_cheap(const DScene* S, March& m, float& mu, v3& p, bool& ovf) {
+// the current point (origin if m.init, else step k) needs psi, with p set and
+// the pending mean state (pend_*) filled.
+//
+// At a step with a lower bound lb on |mu|: lb > B (the bound over all p) lets the
+// march jump to the first step that may have |mu| <= B; lb > noise_bound_at(p)
+// settles this step's sign without psi. For a mesh mean lb comes from the last
+// exact mu (Lipschitz) or the mesh's bounding sphere, and mu is re-evaluated
+// (BVH) only when that is stale and cannot settle the step.
+template <int MK = MEAN_ANY>
+MD bool march_cheap(const DScene* S, March& m, v3& p, bool& ovf) {
   const DMedium& md = S->media[m.medium];
   if (m.init) {
     p = m.o;
-    mu = mean_value(S, md, p, ovf);
-    if (fabsf(mu) * 0.999999f > m.B) {
+    float mu = mean_value<MK>(S, md, p, ovf);
+    m.mu_j = mu;
+    m.t_j = 0.0f;  // p(0) = o exactly
+    if (fabsf(mu) * 0.999999f > noise_bound_at(md.k, m.c, p)) {
       m.fprev_pos = mu > 0.0f;
       m.fprev_big = true;
       m.init = false;
     } else {
+      m.pend_exact = true;
+      m.pend_mu = mu;
+      m.pend_lb = fabsf(mu);
+      m.pend_sgn = mu;
       return true;
     }
   }
@@ -201,19 +286,60 @@ MD bool march_cheap(const DScene* S, March& m, float& mu, v3& p, bool& ovf) {
       return false;
     }
     p = m.o + m.d * m.t;
-    mu = mean_value(S, md, p, ovf);
     m.n_steps++;
-    if (fabsf(mu) * 0.999999f > m.B) {
-      if ((mu > 0.0f) != m.fprev_pos) {  // sign(f) = sign(mu) differs: hit here
+    float lb, sgn, mu = 0.0f;
+    bool exact = MK == MEAN_SPHERE_ONLY || !m.lazy;
+    if (exact) {
+      mu = mean_value<MK>(S, md, p, ovf);
+      m.mu_j = mu;
+      m.t_j = m.t;
+      lb = fabsf(mu);
+      sgn = mu;
+    } else {
+      lb = mu_lower(m, m.t);
+      sgn = m.mu_j;
+      // outside the mesh's bounding sphere every point of the mesh is farther
+      // than |p - c| - r, and the parity test reports outside
+      float lbs = norm3(p - md.bs_c) - md.bs_r;
+      if (lbs > lb) {
+        lb = lbs;
+        sgn = 1.0f;
+      }
+      // a stale bound far from the last exact value: re-evaluate mu (BVH) so
+      // a long jump can follow; near the surface the psi comparison decides
+      if (lb * 0.999999f <= m.B && m.t - m.t_j >= fmaxf(16.0f, fabsf(m.mu_j))) {
+        mu = mean_exact<MK>(S, m, p, m.t, ovf);
+        m.mu_j = mu;
+        m.t_j = m.t;
+        lb = fabsf(mu);
+        sgn = mu;
+        exact = true;
+      }
+    }
+    if (lb * 0.999999f > m.B) {
+      if ((sgn > 0.0f) != m.fprev_pos) {  // sign(f) = sign(mu) differs: hit here
         m.status = 1;
         return false;
       }
-      float target = m.t + (fabsf(mu) - m.B) * 0.9999f - 1e-2f;
-      march_advance(S, m, target);
+      // mu is 1-Lipschitz: every step before `target` keeps |mu| > B
+      march_advance(S, m, m.t + (lb - m.B) * 0.9999f - 2e-2f);
       if (m.status != 0) return false;
-    } else {
-      return true;
+      continue;
     }
+    if (lb * 0.999999f > noise_bound_at(md.k, m.c, p)) {  // this step's sign is sign(mu)
+      if ((sgn > 0.0f) != m.fprev_pos) {
+        m.status = 1;
+        return false;
+      }
+      march_advance(S, m, -INFINITY);
+      if (m.status != 0) return false;
+      continue;
+    }
+    m.pend_exact = exact;
+    m.pend_mu = mu;
+    m.pend_lb = lb;
+    m.pend_sgn = sgn;
+    return true;
   }
   atomicOr(S->err, ERR_MARCH_GUARD);
   m.status = 2;
@@ -222,11 +348,34 @@ MD bool march_cheap(const DScene* S, March& m, float& mu, v3& p, bool& ovf) {
 
 // Phase B: f at the pending point (value only); decides hit or next step. The
 // psi sum is shared by the lanes of group g (all of which hold the same march).
-MD void march_psi(const DScene* S, March& m, float mu, v3 p, const Group& g) {
+template <int MK = MEAN_ANY>
+MD void march_psi(const DScene* S, March& m, v3 p, const Group& g, bool& ovf, const ImpCache* cache = nullptr) {
   const DMedium& md = S->media[m.medium];
   m.n_psi++;
-  float f = mu + raw_noise_value_group(md.k, p, m.seed, g);
-  if (m.c.active) f += cond_value(md.k, m.c, p);
+  float q = cache ? raw_noise_value_cached(md.k, p, m.seed, g, *cache) : raw_noise_value_group(md.k, p, m.seed, g);
+  float c = m.c.active ? cond_value(md.k, m.c, p) : 0.0f;
+  float f;
+  if (m.pend_exact) {
+    f = m.pend_mu + q;
+    if (m.c.active) f += c;
+  } else {
+    // |mu| >= pend_lb > |psi + cond| (with rounding slack) gives sign(f) = sign(mu)
+    // and |f| > 1e-6 without evaluating the mean
+    float s = (fabsf(q) + fabsf(c)) * 1.00001f + 1e-5f;
+    if (m.pend_lb * 0.999999f > s) {
+      if ((m.pend_sgn > 0.0f) != m.fprev_pos) {
+        m.status = 1;
+        return;
+      }
+      march_advance(S, m, -INFINITY);
+      return;
+    }
+    float mu = mean_exact<MK>(S, m, p, m.t, ovf);
+    m.mu_j = mu;
+    m.t_j = m.t;
+    f = mu + q;
+    if (m.c.active) f += c;
+  }
   if (m.init) {
     m.fprev = f;
     m.fprev_pos = f > 0.0f;
@@ -241,22 +390,25 @@ MD void march_psi(const DScene* S, March& m, float mu, v3 p, const Group& g) {
 }
 
 // GPMedium::evalWithGradient with the psi sum shared by group g
+template <int MK = MEAN_ANY>
 MD float4 medium_eval_group(const DScene* S, const DMedium& md, v3 p, uint32_t seed, const Cond& c, bool& ovf,
-                            const Group& g) {
-  float4 mu = mean_value_grad(S, md, p, ovf);
-  float4 nz = raw_noise_group(md.k, p, seed, g);
+                            const Group& g, const ImpCache* cache = nullptr) {
+  float4 mu = mean_value_grad<MK>(S, md, p, ovf);
+  float4 nz = cache ? raw_noise_cached(md.k, p, seed, g, *cache) : raw_noise_group(md.k, p, seed, g);
   float4 f = make_float4(mu.x + nz.x, mu.y + nz.y, mu.z + nz.z, mu.w + nz.w);
   return add_cond(md.k, c, p, f);
 }
 
 // hit point and normal of a finished march
 // (an exited march leaves t, p and normal zero: sampleDistance does not write them)
-MD void march_result(const DScene* S, const March& m, mupsi_medium_sample& out, bool& ovf, const Group& g) {
+template <int MK = MEAN_ANY>
+MD void march_result(const DScene* S, const March& m, mupsi_medium_sample& out, bool& ovf, const Group& g,
+                     const ImpCache* cache = nullptr) {
   out.exited = m.status == 1 ? 0u : 1u;
   out.t = m.status == 1 ? m.t : 0.0f;
   if (m.status == 1) {
     v3 p = m.o + m.d * m.t;
-    float4 f = medium_eval_group(S, S->media[m.medium], p, m.seed, m.c, ovf, g);
+    float4 f = medium_eval_group<MK>(S, S->media[m.medium], p, m.seed, m.c, ovf, g, cache);
     v3 n = normalized(mk3(f.y, f.z, f.w));
     st3(out.p, p);
     st3(out.normal, n);
@@ -278,9 +430,8 @@ MD Group single_lane() {
 MD void march_full(const DScene* S, March& m, bool& ovf) {
   const Group g = single_lane();
   for (int guard = 0; m.status == 0 && guard < 1 << 16; ++guard) {
-    float mu;
     v3 p;
-    if (march_cheap(S, m, mu, p, ovf)) march_psi(S, m, mu, p, g);
+    if (march_cheap(S, m, p, ovf)) march_psi(S, m, p, g, ovf);
   }
   if (m.status == 0) {
     atomicOr(S->err, ERR_MARCH_GUARD);
