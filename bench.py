@@ -42,6 +42,7 @@ def _args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=8.0, help="CPU work per reference/baseline step")
+    ap.add_argument("--extras", type=int, default=1, help="also time configurations 1 and 2 (single GPU)")
     return ap.parse_args()
 
 
@@ -181,6 +182,17 @@ def _peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
 
 
+def _profiled_traffic():
+    """dram read + write bytes of the profiled k_march launch (profiles/k_march_config0.md)."""
+    try:
+        for line in open(os.path.join(ROOT, "profiles", "k_march_config0.md")):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return int(line.split(":", 1)[1])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
 # Source-level operations per impulse evaluation of the march's psi sum (the
 # roofline unit): 4 PCG32 steps at 10 integer ops each (64-bit multiply-add as
 # three 32-bit multiply-adds plus carry, xorshift, rotate), 4 mantissa-trick
@@ -268,7 +280,8 @@ def run_gpu(args):
     peak_gimp = sms * 4 * 32 * mhz * 1e6 / OPS_PER_IMPULSE / 1e9  # 4 schedulers x 32 lanes, 1 issue/clock
     achieved = st["impulse_evals"] / (st["march_ms"] / 1000.0) / 1e9 if st["march_ms"] > 0 else 0.0
     roof = {"bound": "issue", "kernel": "k_march", "achieved": achieved, "peak": peak_gimp,
-            "unit": "Gimpulse-evals/s", "frac": achieved / peak_gimp, "traffic": None,
+            "unit": "Gimpulse-evals/s", "frac": achieved / peak_gimp, "traffic": _profiled_traffic(),
+            "traffic_note": "DRAM bytes of the bounce-1 k_march launch from profiles/k_march_config0.md",
             "peak_basis": f"{sms} SMs x 128 lanes x {mhz:.0f} MHz ({peak_kind} sm_max_mhz) / {OPS_PER_IMPULSE} "
                           f"ops per impulse", "march_share": st["march_ms"] / max(1e-9, st["march_ms"] + st["shade_ms"]),
             "launches": st["march_launches"], "ms_per_launch": st["march_ms"] / max(1, st["march_launches"]),
@@ -298,6 +311,8 @@ def run_gpu(args):
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
     e2e_val = SAMPLES_PER_STEP * world * len(e2e_times) / e2e_t.item()
 
+    extras = run_extras(args) if (rank == 0 and world == 1 and args.extras) else None
+
     cpu = None
     if rank == 0 and world == 1:
         r = cpu_rate(args.cpu_seconds, sc, steps=1, warmup=0)
@@ -311,10 +326,76 @@ def run_gpu(args):
                 "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": desc_bytes,
                         "d2h_bytes_per_step": W * H * 3 * 4},
                 "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clk}
+        if extras:
+            line["extras"] = extras
         print(json.dumps(line), flush=True)
     gs.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def run_extras(args):
+    """Configuration 1 (psi microbench: 2^24 points, 18 sweep points, psi + grad psi +
+    Renewal+ conditioning) and configuration 2 (displaced-icosphere mesh mean, 81,920
+    triangles, 512x512x64) on the same GPU, device-timed with CUDA events."""
+    import torch
+    from mupsi_b200 import scene as S
+    from mupsi_b200.api import GpuRenderer, GpuScene, SparseGPNoiseGenerator, SparseSEKernel
+
+    out = {}
+    n = 1 << 24
+    g = torch.Generator(device="cuda").manual_seed(0)
+    p = (torch.rand((n, 3), device="cuda", generator=g) * 300 - 150).contiguous()
+    seed = torch.randint(0, 2**31 - 1, (n,), device="cuda", generator=g, dtype=torch.int32)
+    d = torch.randn((n, 3), device="cuda", generator=g)
+    d = d / d.norm(dim=1, keepdim=True)
+    cond = torch.zeros((n, 8), device="cuda")
+    res = torch.empty((n, 4), device="cuda")
+    sweep = {}
+    imps = 0
+    total_ms = 0.0
+    for L in (0.5, 1.0, 4.0):
+        for az in (1.0, 4.0):
+            for ppc in (1, 3, 8):
+                cond[:, :3] = p + d * torch.rand((n, 1), device="cuda", generator=g) * 3 * L
+                cond[:, 3] = torch.randn(n, device="cuda", generator=g)
+                gg = torch.randn((n, 3), device="cuda", generator=g)
+                cond[:, 4:7] = gg / gg.norm(dim=1, keepdim=True) * torch.randn((n, 1), device="cuda", generator=g)
+                cond[:, 7] = 1
+                gen = SparseGPNoiseGenerator(SparseSEKernel(1.0, L, (1, 1, az)), ppc)
+                for _ in range(2):
+                    gen.raw_noise(p, seed, cond=cond, out=res)
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                gen.raw_noise(p, seed, cond=cond, out=res)
+                e1.record()
+                e1.synchronize()
+                ms = e0.elapsed_time(e1)
+                total_ms += ms
+                imps += n * 27 * ppc
+                sweep[f"L{L}_aniso{az:g}_ppc{ppc}"] = {"ms": round(ms, 3), "Gqueries_s": round(n / ms / 1e6, 3)}
+    out["config1_psi"] = {"queries_per_point": n, "points": 18, "total_ms": round(total_ms, 2),
+                          "Gimpulse_evals_s": round(imps / total_ms / 1e6, 1), "sweep": sweep}
+    del p, seed, d, cond, res
+    sc = S.config_mesh_scene(level=6, width=512, height=512, spp=64)
+    gs = GpuScene(sc)
+    r = GpuRenderer()
+    r.prepare_render(gs)
+    fb = torch.empty((512, 512, 3), device="cuda")
+    r.start_render_progressive(2, out=fb)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    r.start_render_progressive(64, out=fb)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    out["config2_mesh"] = {"workload": "displaced icosphere level 6 (81,920 triangles) mesh mean, 512x512x64, "
+                                       "length_scale 2, floor quad", "ms": round(ms, 1),
+                           "samples_per_s": 512 * 512 * 64 / (ms / 1000.0)}
+    gs.close()
+    return out
 
 
 def main():

@@ -458,6 +458,7 @@ struct mupsi_scene {
   // wave buffers (grow-only)
   Paths paths{};
   void* paths_mem = nullptr;
+  size_t paths_bytes = 0;
   int64_t paths_cap = 0;
   int max_iters = 0;
   int* err = nullptr;
@@ -481,16 +482,63 @@ struct mupsi_scene {
     }
     return ev_pool[ev_used++];
   }
-  ~mupsi_scene() {
+  ~mupsi_scene();
+};
+
+namespace {
+
+// Path-state buffers outlive their scenes in a small per-device pool, so a
+// host that creates a scene per frame does not pay a cudaMalloc/cudaFree of a
+// few hundred MB every time.
+struct PoolEntry {
+  int dev;
+  void* ptr;
+  size_t bytes;
+};
+std::mutex g_pool_mu;
+std::vector<PoolEntry> g_pool;
+constexpr size_t kPoolKeep = 4;
+
+void* pool_take(size_t bytes, size_t* got) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  int best = -1;
+  for (int i = 0; i < (int)g_pool.size(); ++i)
+    if (g_pool[i].dev == dev && g_pool[i].bytes >= bytes && (best < 0 || g_pool[i].bytes < g_pool[best].bytes))
+      best = i;
+  if (best < 0) return nullptr;
+  void* p = g_pool[best].ptr;
+  *got = g_pool[best].bytes;
+  g_pool.erase(g_pool.begin() + best);
+  return p;
+}
+void pool_give(void* p, size_t bytes) {
+  if (!p) return;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  g_pool.push_back({dev, p, bytes});
+  while (g_pool.size() > kPoolKeep) {  // drop the smallest
+    size_t k = 0;
+    for (size_t i = 1; i < g_pool.size(); ++i)
+      if (g_pool[i].bytes < g_pool[k].bytes) k = i;
+    cudaFree(g_pool[k].ptr);
+    g_pool.erase(g_pool.begin() + (long)k);
+  }
+}
+
+}  // namespace
+
+mupsi_scene::~mupsi_scene() {
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     for (void* p : allocs) cudaFree(p);
     if (d) cudaFree(d);
     if (sum) cudaFree(sum);
-    if (paths_mem) cudaFree(paths_mem);
+    if (paths_mem) pool_give(paths_mem, paths_bytes);
     if (err) cudaFree(err);
     if (counters) cudaFree(counters);
-  }
-};
+}
 
 namespace {
 
@@ -654,7 +702,7 @@ int ensure_paths(mupsi_scene* s, int64_t cap) {
   int iters = wave_iters(s) + 1;
   if (cap <= s->paths_cap && iters <= s->max_iters) return MUPSI_OK;
   if (s->paths_mem) {
-    cudaFree(s->paths_mem);
+    pool_give(s->paths_mem, s->paths_bytes);
     s->paths_mem = nullptr;
   }
   cap = std::max(cap, s->paths_cap);
@@ -669,9 +717,14 @@ int ensure_paths(mupsi_scene* s, int64_t cap) {
          o_ha = take(cap * 16), o_hb = take(cap * 16), o_rad = take(cap * 12), o_q0 = take(cap * 4),
          o_q1 = take(cap * 4), o_q2 = take(cap * 4), o_q3 = take(cap * 4), o_c = take((size_t)(iters + 1) * 8),
          o_cur = take((size_t)(iters + 1) * 4);
-  char* base = nullptr;
-  MUPSI_CUDA(cudaMalloc((void**)&base, bytes));
+  size_t got = 0;
+  char* base = static_cast<char*>(pool_take(bytes, &got));
+  if (!base) {
+    MUPSI_CUDA(cudaMalloc((void**)&base, bytes));
+    got = bytes;
+  }
   s->paths_mem = base;
+  s->paths_bytes = got;
   Paths& P = s->paths;
   P.o = (float4*)(base + o_o);
   P.d = (float4*)(base + o_d);
