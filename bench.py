@@ -395,7 +395,47 @@ def run_extras(args):
                                        "length_scale 2, floor quad", "ms": round(ms, 1),
                            "samples_per_s": 512 * 512 * 64 / (ms / 1000.0)}
     gs.close()
+    out["config4_batch"] = run_batch()
     return out
+
+
+def run_batch():
+    """Configuration 4: 64 seeded uneven sphere-mean instances (resolution 64^2..512^2,
+    4-64 spp, max_bounce 2-10, length_scale U(0.25, 4), 1/3/8 points per cell, half
+    single_realization) rendered as one batch: shared wave queues, one captured graph
+    per bounce count, launch shapes from mupsi_b200/tuning.json. Device time from
+    the batch's CUDA events (first wave start to each instance's last wave)."""
+    import torch
+    from mupsi_b200 import scene as S
+    from mupsi_b200.api import GpuBatch, get_tuning
+
+    scenes = S.batch_scenes(64)
+    spp = [s.spp for s in scenes]
+    paths = sum(s.width * s.height * s.spp for s in scenes)
+    b = GpuBatch(scenes)
+    b.render([max(1, k // 8) for k in spp])  # warm-up: graphs captured, buffers sized
+    res = {}
+    for graphs in (True, False):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, done = b.render(spp, use_graphs=graphs)
+        wall = time.perf_counter() - t0
+        ms = float(np.max(done))
+        info = b.info()
+        res["graphs" if graphs else "no_graphs"] = {
+            "ms": round(ms, 2), "samples_per_s": paths / (ms / 1000.0), "wall_s": round(wall, 3),
+            "waves": info["waves"], "graph_launches": info["graph_launches"]}
+        if graphs:
+            res["done_ms"] = [round(float(x), 2) for x in done]
+    done = np.array(res["done_ms"])
+    b.close()
+    return {"workload": "64 instances of batch_scenes(seed 4): res {64..512}^2, spp 4-64, max_bounce 2-10, "
+                        "length U(0.25,4), ppc {1,3,8}, sphere mean r U(20,100) in 1.8r null sphere, "
+                        "half single_realization", "path_samples": paths,
+            "samples_per_s": res["graphs"]["samples_per_s"], "ms": res["graphs"]["ms"],
+            "completion_ms": {"min": float(done.min()), "median": float(np.median(done)),
+                              "max": float(done.max()), "mean": float(done.mean())},
+            "tuning": get_tuning(), **res}
 
 
 def main():

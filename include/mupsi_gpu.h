@@ -297,6 +297,61 @@ int mupsi_gpu_scene_profile(mupsi_scene* scene, int32_t enable);
 /* Copy the accumulated statistics; reset != 0 clears them afterwards. */
 int mupsi_gpu_scene_stats(mupsi_scene* scene, mupsi_render_stats* out, int32_t reset);
 
+/* ------------------------------------------------------------------ tuning
+ * Launch shapes of the wave kernels, process-wide. No reference counterpart
+ * (the reference's OpenMP loop has no launch shapes); the values come from the
+ * project's autotuner (mupsi_b200/autotune.py writes mupsi_b200/tuning.json,
+ * which the Python layer applies on import). */
+typedef struct mupsi_tuning {
+  int32_t march_block; /* threads per block of the persistent march: 32, 64, 96 or 128 */
+  int32_t min_group;   /* smallest lane group sharing one ray's psi sums: 4, 8, 16 or 32 */
+  int32_t shade_block; /* threads per block of the shading kernel: a multiple of 32 in [32, 128] */
+  int32_t wave_paths;  /* paths in flight per wave (the queue tile); 0 = 8 Mi */
+} mupsi_tuning;
+int mupsi_gpu_set_tuning(const mupsi_tuning* t);
+int mupsi_gpu_get_tuning(mupsi_tuning* out);
+
+/* ------------------------------------------------------------------ batch
+ * Several scene instances rendered together (no reference counterpart: the
+ * reference renders one scene per Renderer::startRenderProgressive). Every
+ * wave is one persistent launch sequence over a shared path queue whose paths
+ * carry their instance id, so instances of different sizes, pass counts and
+ * bounce limits fill the GPU together. Each instance's image equals what
+ * mupsi_gpu_render(scene, spp_begin = 0, spp_end = spp[i]) returns.
+ * The batch refers to the scenes (it does not own them); destroy the batch
+ * before its scenes. */
+typedef struct mupsi_batch mupsi_batch;
+int mupsi_gpu_batch_create(int32_t num_scenes, mupsi_scene* const* scenes, mupsi_batch** out);
+int mupsi_gpu_batch_destroy(mupsi_batch* batch);
+
+typedef struct mupsi_batch_args {
+  const int32_t* spp;           /* [num_scenes] passes per instance (>= 0), host memory */
+  float* const* rgb_out;        /* [num_scenes] averaged image per instance (h*w*3) or NULL entries */
+  mupsi_mem out_mem;            /* where every rgb_out buffer lives */
+  const volatile int32_t* cancel; /* nullable, polled between waves */
+  float* done_ms;               /* nullable [num_scenes]: completion time of each instance (the
+                                   end of the wave holding its last passes) in ms from the
+                                   start of the first wave, by CUDA events; 0 for spp 0 */
+  int32_t use_graphs;           /* != 0: each wave replays a captured CUDA graph */
+  int32_t schedule;             /* MUPSI_SCHEDULE_*: order in which instances enter waves */
+  void* stream;                 /* cudaStream_t or NULL */
+} mupsi_batch_args;
+enum {
+  MUPSI_SCHEDULE_SHORTEST_FIRST = 0, /* instances by ascending paths (least mean completion time) */
+  MUPSI_SCHEDULE_IN_ORDER = 1        /* instances in the order given */
+};
+int mupsi_gpu_batch_render(mupsi_batch* batch, const mupsi_batch_args* args);
+
+/* Waves and kernel launches of the last batch_render. */
+typedef struct mupsi_batch_info {
+  int32_t waves;
+  int32_t graph_launches;    /* waves replayed from a graph */
+  int32_t graphs_captured;   /* graph captures (instantiations or updates) */
+  int32_t max_iters;         /* largest bounce-iteration count of a wave */
+  int64_t paths;             /* path samples traced */
+} mupsi_batch_info;
+int mupsi_gpu_batch_info(const mupsi_batch* batch, mupsi_batch_info* out);
+
 #ifdef __cplusplus
 }
 #endif

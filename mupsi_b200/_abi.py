@@ -147,3 +147,39 @@ class RenderStats(C.Structure):
         ("mean_evals", C.c_uint64),
         ("parity_casts", C.c_uint64),
     ]
+
+
+class Tuning(C.Structure):
+    _fields_ = [
+        ("march_block", C.c_int32),
+        ("min_group", C.c_int32),
+        ("shade_block", C.c_int32),
+        ("wave_paths", C.c_int32),
+    ]
+
+
+class BatchArgs(C.Structure):
+    _fields_ = [
+        ("spp", C.POINTER(C.c_int32)),
+        ("rgb_out", C.POINTER(C.c_void_p)),
+        ("out_mem", C.c_int32),
+        ("cancel", C.POINTER(C.c_int32)),
+        ("done_ms", C.POINTER(C.c_float)),
+        ("use_graphs", C.c_int32),
+        ("schedule", C.c_int32),
+        ("stream", C.c_void_p),
+    ]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [
+        ("waves", C.c_int32),
+        ("graph_launches", C.c_int32),
+        ("graphs_captured", C.c_int32),
+        ("max_iters", C.c_int32),
+        ("paths", C.c_int64),
+    ]
+
+
+SCHEDULE_SHORTEST_FIRST = 0
+SCHEDULE_IN_ORDER = 1

@@ -7,6 +7,8 @@ Errors raise MupsiError with the library's message, the counterpart of the
 reference's bool + std::cerr returns.
 """
 import ctypes as C
+import json
+import os
 
 import numpy as np
 
@@ -200,10 +202,50 @@ class DeviceMesh:
         return ins, tri, dq
 
 
+TUNING_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning.json")
+_TUNING_KEYS = ("march_block", "min_group", "shade_block", "wave_paths")
+_tuning_applied = False
+
+
+def get_tuning():
+    """The launch shapes in use (mupsi_gpu_get_tuning) as a dict."""
+    t = _abi.Tuning()
+    check(load().mupsi_gpu_get_tuning(C.byref(t)))
+    return {k: getattr(t, k) for k in _TUNING_KEYS}
+
+
+def set_tuning(**kw):
+    """Change some launch shapes (march_block, min_group, shade_block, wave_paths)."""
+    cur = get_tuning()
+    for k, v in kw.items():
+        if k not in _TUNING_KEYS:
+            raise KeyError(k)
+        cur[k] = int(v)
+    check(load().mupsi_gpu_set_tuning(C.byref(_abi.Tuning(*[cur[k] for k in _TUNING_KEYS]))))
+    return cur
+
+
+def apply_tuning_file(path=TUNING_FILE):
+    """Apply the autotuner's choice (mupsi_b200/autotune.py) if its file exists."""
+    global _tuning_applied
+    _tuning_applied = True
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        chosen = json.load(f)["tuning"]
+    return set_tuning(**{k: chosen[k] for k in _TUNING_KEYS if k in chosen})
+
+
+def _ensure_tuning():
+    if not _tuning_applied:
+        apply_tuning_file()
+
+
 class GpuScene:
     """A scene on the device: the RenderContext plus GPMedium/MeanFunction batch probes."""
 
     def __init__(self, scene: Scene):
+        _ensure_tuning()
         self.scene = scene
         self._desc = scene.desc()
         h = C.c_void_p()
@@ -343,3 +385,62 @@ class GpuRenderer:
             return None
         check(code)
         return (out, mom) if moments else out
+
+
+class GpuBatch:
+    """Several scenes rendered together (mupsi_gpu_batch_*): one wave stream
+    whose paths carry their scene's index. No reference counterpart (the
+    reference renders one scene per Renderer)."""
+
+    SCHEDULES = {"shortest_first": _abi.SCHEDULE_SHORTEST_FIRST, "in_order": _abi.SCHEDULE_IN_ORDER}
+
+    def __init__(self, scenes):
+        _ensure_tuning()
+        self.scenes = [sc if isinstance(sc, GpuScene) else GpuScene(sc) for sc in scenes]
+        arr = (C.c_void_p * len(self.scenes))(*[sc.h.value for sc in self.scenes])
+        h = C.c_void_p()
+        check(load().mupsi_gpu_batch_create(len(self.scenes), arr, C.byref(h)))
+        self.h = h
+        self.cancel_flag = C.c_int32(0)
+
+    def close(self):
+        if self.h:
+            load().mupsi_gpu_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def cancel(self):
+        self.cancel_flag.value = 1
+
+    def render(self, spp, out=None, use_graphs=True, schedule="shortest_first", stream=None):
+        """Render scene i at spp[i] passes. `out`: None (host images are
+        returned), or a list of (h, w, 3) float32 buffers, all numpy or all CUDA
+        tensors (entries may be None). Returns (images, done_ms): done_ms[i] is
+        scene i's completion time in ms from the start of the first wave.
+        Returns None if cancelled."""
+        n = len(self.scenes)
+        if len(spp) != n:
+            raise ValueError("one spp per scene")
+        if out is None:
+            out = [np.empty((sc.scene.height, sc.scene.width, 3), np.float32) for sc in self.scenes]
+        dev = _mem(*out) == _abi.MEM_DEVICE
+        sp = (C.c_int32 * n)(*[int(v) for v in spp])
+        ptrs = (C.c_void_p * n)(*[_ptr(o) for o in out])
+        done = (C.c_float * n)()
+        args = _abi.BatchArgs(sp, ptrs, _abi.MEM_DEVICE if dev else _abi.MEM_HOST, C.pointer(self.cancel_flag), done,
+                              1 if use_graphs else 0, self.SCHEDULES[schedule], _stream(stream))
+        code = load().mupsi_gpu_batch_render(self.h, C.byref(args))
+        if code == _abi.ERR_CANCELLED:
+            return None
+        check(code)
+        return out, np.array(list(done), np.float64)
+
+    def info(self):
+        i = _abi.BatchInfo()
+        check(load().mupsi_gpu_batch_info(self.h, C.byref(i)))
+        return {f: getattr(i, f) for f, _ in _abi.BatchInfo._fields_}

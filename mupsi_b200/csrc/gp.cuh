@@ -65,10 +65,8 @@ MD void for_each_impulse(const KParams& k, int nx, int ny, int nz, uint32_t seed
 // the reference's (dx, dy, dz) order (cell c = 9(dx+1) + 3(dy+1) + (dz+1)).
 // GRAD = false computes the value only.
 template <bool GRAD>
-MD void psi_sums_range(const KParams& k, v3 p, uint32_t seed, int c0, int c1, float& sv, float& sx, float& sy,
-                       float& sz) {
-  int cx, cy, cz;
-  cell_of(k, p, cx, cy, cz);
+MD void psi_sums_cells(const KParams& k, v3 p, int cx, int cy, int cz, uint32_t seed, int c0, int c1, float& sv,
+                       float& sx, float& sy, float& sz) {
   float v = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f;
 #pragma unroll 1
   for (int c = c0; c < c1; ++c) {
@@ -92,126 +90,108 @@ MD void psi_sums_range(const KParams& k, v3 p, uint32_t seed, int c0, int c1, fl
   sz = gz;
 }
 template <bool GRAD>
+MD void psi_sums_range(const KParams& k, v3 p, uint32_t seed, int c0, int c1, float& sv, float& sx, float& sy,
+                       float& sz) {
+  int cx, cy, cz;
+  cell_of(k, p, cx, cy, cz);
+  psi_sums_cells<GRAD>(k, p, cx, cy, cz, seed, c0, c1, sv, sx, sy, sz);
+}
+template <bool GRAD>
 MD void psi_sums(const KParams& k, v3 p, uint32_t seed, float& sv, float& sx, float& sy, float& sz) {
   psi_sums_range<GRAD>(k, p, seed, 0, 27, sv, sx, sy, sz);
 }
 
 // A group of G lanes (G a power of two, lanes gbase..gbase+G-1 of the warp)
-// shares one evaluation: lane `sub` sums a contiguous block of the 27 cells and
-// the block sums are added with a butterfly over the group, so every lane of the
-// group ends with the same total. With G = 1 this is the sequential sum above.
+// shares one evaluation, and its sums are added in one fixed order whatever G
+// is, so a ray's psi (and with it every march decision and hit normal) does not
+// depend on the launch shape. The 27 cells are cut into 16 slots of one or two
+// consecutive cells (sizes 2,2,2,1 | 2,2,2,1 | 2,2,2,1 | 2,2,1,1); a slot sums
+// its cells' impulses from 0 in the reference's order, and the 16 slot sums are
+// added by a perfect pairwise tree (slots 2i and 2i+1 first, then pairs of
+// those, ...). Lane `sub` owns the V = max(1, 16/G) slots from sub V: it adds
+// their subtree itself and the shuffles (offsets 1, 2, ..., up to 8) add the
+// levels above; with G = 32, lanes 16-31 repeat lanes 0-15. Any 16/G
+// consecutive slots hold at most ceil(27/G) cells for G = 4, 8, 16, so lanes
+// are as evenly loaded as a plain split of the cells. Float addition commutes,
+// so both lanes of a shuffle pair get the same bits.
 struct Group {
   int G, sub;
   unsigned mask;
 };
-MD float group_sum(const Group& g, float v) {
-  for (int off = 1; off < g.G; off <<= 1) v += __shfl_xor_sync(g.mask, v, off, g.G);
-  return v;
-}
-MD void group_cells(const Group& g, int& c0, int& c1) {
-  const int per = (27 + g.G - 1) / g.G;
-  c0 = min(27, g.sub * per);
-  c1 = min(27, c0 + per);
-}
-MD float raw_noise_value_group(const KParams& k, v3 p, uint32_t seed, const Group& g) {
-  int c0, c1;
-  group_cells(g, c0, c1);
-  float v, x, y, z;
-  psi_sums_range<false>(k, p, seed, c0, c1, v, x, y, z);
-  v = group_sum(g, v);
-  return (k.sigma * v) / k.sqrt_var;
-}
-MD float4 raw_noise_group(const KParams& k, v3 p, uint32_t seed, const Group& g) {
-  int c0, c1;
-  group_cells(g, c0, c1);
-  float v, x, y, z;
-  psi_sums_range<true>(k, p, seed, c0, c1, v, x, y, z);
-  v = group_sum(g, v);
-  x = group_sum(g, x);
-  y = group_sum(g, y);
-  z = group_sum(g, z);
-  return make_float4((k.sigma * v) / k.sqrt_var, (k.sigma * x) / k.sqrt_var, (k.sigma * y) / k.sqrt_var,
-                     (k.sigma * z) / k.sqrt_var);
-}
-
-// ---- impulse cache for marches --------------------------------------------
-// Consecutive march steps of one ray share most of their 27 neighbour cells
-// (dt = 0.5 against cells of size kr). A lane group keeps the impulses of the
-// current 3x3x3 window in shared memory, one slot per cell of a mod-3 torus
-// (slot = (cx mod 3, cy mod 3, cz mod 3)): moving the window by one cell
-// replaces exactly the 9 slots of the layer it leaves. Lane `sub` owns the
-// slots s with s % G == sub, so no slot is shared between lanes. A slot holds
-// its cell's coordinates and ppc (s.x, s.y, s.z, w) records, computed exactly
-// as for_each_impulse computes them.
-#define CACHE_MAX_PPC 3
-struct ImpCache {
-  int* tag;      // [27 * 3]: cell coordinates held by each slot
-  float4* imp;   // [27 * CACHE_MAX_PPC]
-};
-// per lane group: the float4 records first, then the tags; a multiple of 16 so
-// every group's records start 16-byte aligned
-constexpr int kCacheBytes = ((27 * CACHE_MAX_PPC * 16 + 27 * 3 * 4) + 15) / 16 * 16;
-static_assert(kCacheBytes % 16 == 0, "lane-group cache stride must keep float4 alignment");
-
-MD int mod3(int x) { return ((x % 3) + 3) % 3; }
-MD void cache_clear(ImpCache c, const Group& g) {
-  for (int s = g.sub; s < 27; s += g.G) c.tag[3 * s] = INT_MIN;
+MD void slot_cells(int q, int& c0, int& c1) {
+  const int r = q & 3;
+  c0 = 7 * (q >> 2) + 2 * r - (q == 15 ? 1 : 0);
+  c1 = c0 + ((r == 3 || q == 14) ? 1 : 2);
 }
 template <bool GRAD>
-MD void psi_sums_cached(const KParams& k, v3 p, uint32_t seed, const Group& g, ImpCache c, float& sv, float& sx,
-                        float& sy, float& sz) {
+MD float4 slot_sums(const KParams& k, v3 p, int cx, int cy, int cz, uint32_t seed, int q) {
+  int c0, c1;
+  slot_cells(q, c0, c1);
+  float4 x;
+  psi_sums_cells<GRAD>(k, p, cx, cy, cz, seed, c0, c1, x.x, x.y, x.z, x.w);
+  return x;
+}
+template <bool GRAD>
+MD float4 add_s(float4 a, float4 b) {
+  if (!GRAD) return make_float4(a.x + b.x, 0.0f, 0.0f, 0.0f);
+  return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+// WIDE: the caller guarantees G >= 4 (V <= 4: the subtree is written out);
+// otherwise a stack of partial sums walks the lane's V <= 16 slots.
+template <bool GRAD, bool WIDE>
+MD float4 psi_sums_group(const KParams& k, v3 p, uint32_t seed, const Group& g) {
   int cx, cy, cz;
   cell_of(k, p, cx, cy, cz);
-  float v = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f;
-#pragma unroll 1
-  for (int s = g.sub; s < 27; s += g.G) {
-    // the cell of the window [c-1, c+1]^3 that maps to slot s
-    const int ax = cx - 1 + mod3(s / 9 - (cx - 1));
-    const int ay = cy - 1 + mod3((s / 3) % 3 - (cy - 1));
-    const int az = cz - 1 + mod3(s % 3 - (cz - 1));
-    int* t = c.tag + 3 * s;
-    float4* I = c.imp + CACHE_MAX_PPC * s;
-    if (t[0] != ax || t[1] != ay || t[2] != az) {
-      int i = 0;
-      for_each_impulse(k, ax, ay, az, seed, [&](v3 q, float w) { I[i++] = make_float4(q.x, q.y, q.z, w); });
-      t[0] = ax;
-      t[1] = ay;
-      t[2] = az;
+  const int V = g.G >= 16 ? 1 : 16 / g.G;
+  const int q0 = g.G >= 16 ? (g.sub & 15) : g.sub * V;
+  float4 r;
+  if (WIDE) {
+    r = slot_sums<GRAD>(k, p, cx, cy, cz, seed, q0);
+    if (V >= 2) r = add_s<GRAD>(r, slot_sums<GRAD>(k, p, cx, cy, cz, seed, q0 + 1));
+    if (V >= 4) {
+      const float4 a = slot_sums<GRAD>(k, p, cx, cy, cz, seed, q0 + 2);
+      r = add_s<GRAD>(r, add_s<GRAD>(a, slot_sums<GRAD>(k, p, cx, cy, cz, seed, q0 + 3)));
     }
-    for (int i = 0; i < k.ppc; ++i) {
-      const float4 q = I[i];
-      v3 d = p - mk3(q.x, q.y, q.z);
-      float r2 = d.x * d.x + (d.y * d.y + d.z * d.z);
-      float h = ex2_approx(r2 * k.k2);
-      v = fmaf(q.w, h, v);
-      if (GRAD) {
-        float gs = h * k.c2;
-        gx = fmaf(q.w, gs * d.x, gx);
-        gy = fmaf(q.w, gs * d.y, gy);
-        gz = fmaf(q.w, gs * d.z, gz);
+  } else {
+    float4 st[5];
+#pragma unroll 1
+    for (int j = 0; j < V; ++j) {
+      float4 x = slot_sums<GRAD>(k, p, cx, cy, cz, seed, q0 + j);
+      bool carry = true;
+#pragma unroll
+      for (int l = 0; l < 5; ++l) {
+        if (carry) {
+          if (l < 4 && ((j >> l) & 1)) {
+            x = add_s<GRAD>(st[l], x);
+          } else {
+            st[l] = x;
+            carry = false;
+          }
+        }
       }
     }
+    r = V == 1 ? st[0] : V == 2 ? st[1] : V == 4 ? st[2] : V == 8 ? st[3] : st[4];
   }
-  sv = v;
-  sx = gx;
-  sy = gy;
-  sz = gz;
+  const int top = min(g.G, 16);
+  for (int off = 1; off < top; off <<= 1) {
+    r.x += __shfl_xor_sync(g.mask, r.x, off, g.G);
+    if (GRAD) {
+      r.y += __shfl_xor_sync(g.mask, r.y, off, g.G);
+      r.z += __shfl_xor_sync(g.mask, r.z, off, g.G);
+      r.w += __shfl_xor_sync(g.mask, r.w, off, g.G);
+    }
+  }
+  return r;
 }
-MD float raw_noise_value_cached(const KParams& k, v3 p, uint32_t seed, const Group& g, ImpCache c) {
-  float v, x, y, z;
-  psi_sums_cached<false>(k, p, seed, g, c, v, x, y, z);
-  v = group_sum(g, v);
-  return (k.sigma * v) / k.sqrt_var;
+template <bool WIDE = false>
+MD float raw_noise_value_group(const KParams& k, v3 p, uint32_t seed, const Group& g) {
+  return (k.sigma * psi_sums_group<false, WIDE>(k, p, seed, g).x) / k.sqrt_var;
 }
-MD float4 raw_noise_cached(const KParams& k, v3 p, uint32_t seed, const Group& g, ImpCache c) {
-  float v, x, y, z;
-  psi_sums_cached<true>(k, p, seed, g, c, v, x, y, z);
-  v = group_sum(g, v);
-  x = group_sum(g, x);
-  y = group_sum(g, y);
-  z = group_sum(g, z);
-  return make_float4((k.sigma * v) / k.sqrt_var, (k.sigma * x) / k.sqrt_var, (k.sigma * y) / k.sqrt_var,
-                     (k.sigma * z) / k.sqrt_var);
+template <bool WIDE = false>
+MD float4 raw_noise_group(const KParams& k, v3 p, uint32_t seed, const Group& g) {
+  const float4 s = psi_sums_group<true, WIDE>(k, p, seed, g);
+  return make_float4((k.sigma * s.x) / k.sqrt_var, (k.sigma * s.y) / k.sqrt_var, (k.sigma * s.z) / k.sqrt_var,
+                     (k.sigma * s.w) / k.sqrt_var);
 }
 
 // RawNoise(p, seed) = sigma * InternalNoise / sqrt(Var) (gpnoise.h:44)

@@ -77,22 +77,93 @@ MD uint32_t medium_seed(const DScene* S, int x, int y, int k, int b) {
   return constant_sampler_i(s);
 }
 
+// meta.w packs the bounce count (11 bits; max_bounce <= 1024) and the path's
+// scene instance (a wave may hold paths of many scenes).
+MD int meta_bounce(int w) { return w & 2047; }
+MD int meta_inst(int w) { return w >> 11; }
+MD int pack_meta(int bounce, int inst) { return bounce | (inst << 11); }
+
+// A wave is a list of chunks: `passes` consecutive passes of one scene
+// instance, stored at path indices [path0, path0 + passes * width * height);
+// the chunk's pixels are [pix0, pix0 + wh) of the wave's accumulation range.
+struct WaveChunk {
+  int inst, pass0, passes, width;
+  int64_t path0, wh, pix0;
+};
+// One wave of a device-resident wave plan: its paths, accumulated pixels and
+// chunk range.
+struct WaveDesc {
+  int64_t n, npix;
+  int chunk0, nchunks;
+};
+// Where a wave's paths come from: explicit (x, y, k) arrays, a chunk table, or
+// (wave_idx != null) wave *wave_idx of a device wave plan, which lets one
+// captured graph replay every wave of a plan.
+struct WaveSrc {
+  int64_t n = 0;
+  const WaveChunk* chunks = nullptr;
+  int nchunks = 0;
+  const int32_t *xs = nullptr, *ys = nullptr, *ks = nullptr;
+  const WaveDesc* waves = nullptr;
+  const int* wave_idx = nullptr;
+};
+MD void resolve_wave(const WaveSrc& src, int64_t& n, int64_t& npix, const WaveChunk*& chunks, int& nchunks) {
+  n = src.n;
+  npix = 0;
+  chunks = src.chunks;
+  nchunks = src.nchunks;
+  if (src.wave_idx) {
+    const WaveDesc wd = src.waves[*src.wave_idx];
+    n = wd.n;
+    npix = wd.npix;
+    chunks = src.chunks + wd.chunk0;
+    nchunks = wd.nchunks;
+  }
+}
+// last chunk whose start (member `start`) is <= i
+template <typename F>
+MD int find_chunk(const WaveChunk* chunks, int nchunks, int64_t i, F start) {
+  int lo = 0, hi = nchunks - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (start(chunks[mid]) <= i)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
 // ------------------------------------------------------------ kernels
-__global__ void k_raygen(const DScene* __restrict__ S, Paths P, int64_t n, int pass0, const int32_t* xs,
-                         const int32_t* ys, const int32_t* ks) {
-  const int64_t wh = (int64_t)S->width * S->height;
+// Start of a wave: clear the queue counters and cursors of `iters` bounce
+// iterations and step the plan's wave index.
+__global__ void k_wave_begin(Paths P, int iters, int* wave_idx) {
+  for (int i = threadIdx.x; i < 2 * (iters + 1); i += blockDim.x) P.counts[i] = 0;
+  for (int i = threadIdx.x; i < iters + 1; i += blockDim.x) P.cursors[i] = 0;
+  if (wave_idx && threadIdx.x == 0) *wave_idx += 1;
+}
+
+__global__ void k_raygen(const DScene* const* __restrict__ scenes, Paths P, WaveSrc src) {
+  int64_t n, npix;
+  const WaveChunk* chunks;
+  int nchunks;
+  resolve_wave(src, n, npix, chunks, nchunks);
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    int x, y, k;
-    if (xs) {
-      x = xs[i];
-      y = ys[i];
-      k = ks[i];
+    int x, y, k, inst = 0;
+    if (src.xs) {
+      x = src.xs[i];
+      y = src.ys[i];
+      k = src.ks[i];
     } else {
-      int64_t pix = i % wh;
-      k = pass0 + (int)(i / wh);
-      x = (int)(pix % S->width);
-      y = (int)(pix / S->width);
+      const WaveChunk& c = chunks[find_chunk(chunks, nchunks, i, [](const WaveChunk& w) { return w.path0; })];
+      int64_t local = i - c.path0;
+      int64_t pix = local % c.wh;
+      inst = c.inst;
+      k = c.pass0 + (int)(local / c.wh);
+      x = (int)(pix % c.width);
+      y = (int)(pix / c.width);
     }
+    const DScene* S = scenes[inst];
     uint64_t rng = pcg_seeded(make_seed4((uint32_t)x, (uint32_t)y, (uint32_t)k, TRACE_SEED));
     Ray r = camera_ray(S, x, y);
     P.o[i] = make_float4(r.o.x, r.o.y, r.o.z, r.nt);
@@ -102,7 +173,7 @@ __global__ void k_raygen(const DScene* __restrict__ S, Paths P, int64_t n, int p
     P.rng[i] = st_rng(rng);
     P.ca[i] = make_float4(0, 0, 0, 0);
     P.cb[i] = make_float4(0, 0, 0, __uint_as_float(0u));
-    P.meta[i] = make_int4(x, y, k, 0);
+    P.meta[i] = make_int4(x, y, k, pack_meta(0, inst));
     P.q[2][i] = (uint32_t)i;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -111,31 +182,32 @@ __global__ void k_raygen(const DScene* __restrict__ S, Paths P, int64_t n, int p
   }
 }
 
+// Launch-wide settings of the march and shade kernels.
+struct WaveCfg {
+  int min_group;                 // smallest lane group per march
+  int* err;                      // device error word (ERR_* bits)
+  unsigned long long* counters;  // nullable work counters
+};
+
 // Persistent march over the medium queue of iteration `it`. Each ray is
 // marched by a group of G lanes that share its psi sums: G = 4 while the queue
 // fills the resident threads, larger (up to 32) as the queue shrinks, so the
 // late bounces' few long marches finish up to 8x sooner than on one lane.
-template <bool CACHE, int MK>
-__global__ void __launch_bounds__(128) k_march(const DScene* __restrict__ S, Paths P, int it) {
-  extern __shared__ __align__(16) unsigned char smem[];
+template <int MK>
+__global__ void __launch_bounds__(128) k_march(const DScene* const* __restrict__ scenes, Paths P, int it, WaveCfg cfg) {
   const uint32_t n = P.counts[2 * it];
   const uint32_t* q = P.q[it & 1];
   uint32_t* cursor = P.cursors + it;
   const unsigned lane = threadIdx.x & 31;
   const uint64_t resident = (uint64_t)gridDim.x * blockDim.x;
   Group grp;
-  grp.G = S->min_group;
+  grp.G = max(4, cfg.min_group);  // >= 4: march_result's WIDE gradient order
   while (grp.G < 32 && (uint64_t)n * (uint64_t)(2 * grp.G) <= resident) grp.G <<= 1;
   grp.sub = (int)(lane & (unsigned)(grp.G - 1));
   const unsigned gbase = lane & ~(unsigned)(grp.G - 1);
   grp.mask = grp.G == 32 ? 0xffffffffu : (((1u << grp.G) - 1u) << gbase);
-  ImpCache cache;
-  if (CACHE) {  // this group's slot table (G >= 4: at most 32 groups per block)
-    unsigned char* base = smem + (size_t)(threadIdx.x / grp.G) * kCacheBytes;
-    cache.tag = reinterpret_cast<int*>(base + 27 * CACHE_MAX_PPC * 16);
-    cache.imp = reinterpret_cast<float4*>(base);
-  }
   March m;
+  const DScene* S = scenes[0];
   uint32_t idx = 0;
   bool active = false;
   bool ovf = false;
@@ -156,9 +228,9 @@ __global__ void __launch_bounds__(128) k_march(const DScene* __restrict__ S, Pat
           float4 o = P.o[idx], d = P.d[idx];
           int4 meta = P.meta[idx];
           int med = __float_as_int(d.w);
+          S = scenes[meta_inst(meta.w)];
           march_begin(S, m, mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), o.w, 3.402823466e+38f, med,
-                      medium_seed(S, meta.x, meta.y, meta.z, meta.w), load_cond(P, idx));
-          if (CACHE) cache_clear(cache, grp);
+                      medium_seed(S, meta.x, meta.y, meta.z, meta_bounce(meta.w)), load_cond(P, idx));
           active = true;
           if (grp.sub == 0) marches++;
         }
@@ -167,10 +239,10 @@ __global__ void __launch_bounds__(128) k_march(const DScene* __restrict__ S, Pat
     if (!__any_sync(0xffffffffu, active)) break;
     if (active) {
       v3 p;
-      if (march_cheap<MK>(S, m, p, ovf)) march_psi<MK>(S, m, p, grp, ovf, CACHE ? &cache : nullptr);
+      if (march_cheap<MK>(S, m, p, ovf)) march_psi<MK, true>(S, m, p, grp, ovf);
       if (m.status != 0) {
         mupsi_medium_sample r;
-        march_result<MK>(S, m, r, ovf, grp, CACHE ? &cache : nullptr);
+        march_result<MK, true>(S, m, r, ovf, grp);
         if (grp.sub == 0) {
           P.ha[idx] = make_float4(r.t, r.p[0], r.p[1], r.p[2]);
           P.hb[idx] = make_float4(r.normal[0], r.normal[1], r.normal[2], __uint_as_float(r.exited));
@@ -184,8 +256,8 @@ __global__ void __launch_bounds__(128) k_march(const DScene* __restrict__ S, Pat
       }
     }
   }
-  if (ovf) atomicOr(S->err, ERR_BVH_STACK);
-  if (S->counters) {
+  if (ovf) atomicOr(cfg.err, ERR_BVH_STACK);
+  if (cfg.counters) {
     for (int o = 16; o > 0; o >>= 1) {
       steps += __shfl_down_sync(0xffffffffu, steps, o);
       psis += __shfl_down_sync(0xffffffffu, psis, o);
@@ -195,12 +267,12 @@ __global__ void __launch_bounds__(128) k_march(const DScene* __restrict__ S, Pat
       pars += __shfl_down_sync(0xffffffffu, pars, o);
     }
     if (lane == 0) {
-      atomicAdd(&S->counters[0], steps);
-      atomicAdd(&S->counters[1], psis);
-      atomicAdd(&S->counters[2], marches);
-      atomicAdd(&S->counters[3], imps);
-      atomicAdd(&S->counters[4], mus);
-      atomicAdd(&S->counters[5], pars);
+      atomicAdd(&cfg.counters[0], steps);
+      atomicAdd(&cfg.counters[1], psis);
+      atomicAdd(&cfg.counters[2], marches);
+      atomicAdd(&cfg.counters[3], imps);
+      atomicAdd(&cfg.counters[4], mus);
+      atomicAdd(&cfg.counters[5], pars);
     }
   }
 }
@@ -222,20 +294,22 @@ MD void push(uint32_t* q, uint32_t* count, uint32_t v) {
 }
 
 // One bounce of PathTracer::trace for every live path of iteration `it`.
-__global__ void __launch_bounds__(128) k_shade(const DScene* __restrict__ S, Paths P, int it) {
+__global__ void __launch_bounds__(128) k_shade(const DScene* const* __restrict__ scenes, Paths P, int it, WaveCfg cfg) {
   const uint32_t n = P.counts[2 * it + 1];
   const uint32_t* q = P.q[2 + (it & 1)];
   uint32_t* qm_next = P.q[(it + 1) & 1];
   uint32_t* qa_next = P.q[2 + ((it + 1) & 1)];
   uint32_t* cm_next = P.counts + 2 * (it + 1);
   uint32_t* ca_next = P.counts + 2 * (it + 1) + 1;
-  const bool single = S->gp_mode == MUPSI_GP_SINGLE_REALIZATION;
   const v3 med_albedo = mk3(0.8f, 0.8f, 0.8f);  // Medium::default_bsdf_: Lambertian, albedo 0.8
   bool ovf = false;
   for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
     const uint32_t i = q[j];
     float4 o4 = P.o[i], d4 = P.d[i], t4 = P.thr[i], e4 = P.em[i];
     int4 meta = P.meta[i];
+    const int inst = meta_inst(meta.w);
+    const DScene* S = scenes[inst];
+    const bool single = S->gp_mode == MUPSI_GP_SINGLE_REALIZATION;
     int medium = __float_as_int(d4.w);
     uint64_t rng = ld_rng(P.rng[i]);
     v3 thr = mk3(t4.x, t4.y, t4.z), em = mk3(e4.x, e4.y, e4.z);
@@ -244,7 +318,7 @@ __global__ void __launch_bounds__(128) k_shade(const DScene* __restrict__ S, Pat
     ray.d = mk3(d4.x, d4.y, d4.z);
     ray.nt = o4.w;
     ray.ft = 3.402823466e+38f;
-    int bounce = meta.w;
+    int bounce = meta_bounce(meta.w);
     bool has_hit = false, exited = true, dead = false;
     Cond cond = load_cond(P, i);
     if (medium >= 0) {
@@ -323,7 +397,7 @@ __global__ void __launch_bounds__(128) k_shade(const DScene* __restrict__ S, Pat
       P.em[i] = make_float4(em.x, em.y, em.z, 0.0f);
       P.rng[i] = st_rng(rng);
       store_cond(P, i, cond);
-      P.meta[i] = make_int4(meta.x, meta.y, meta.z, bounce);
+      P.meta[i] = make_int4(meta.x, meta.y, meta.z, pack_meta(bounce, inst));
       push(qa_next, ca_next, i);
       if (medium >= 0) push(qm_next, cm_next, i);
     } else {
@@ -332,7 +406,7 @@ __global__ void __launch_bounds__(128) k_shade(const DScene* __restrict__ S, Pat
       P.rad[3 * (int64_t)i + 2] = em.z;
     }
   }
-  if (ovf) atomicOr(S->err, ERR_BVH_STACK);
+  if (ovf) atomicOr(cfg.err, ERR_BVH_STACK);
 }
 
 // Per-pixel running sum over the wave's passes in pass order (framebuffer.cpp:28-35),
@@ -362,6 +436,30 @@ __global__ void k_accumulate(const float* __restrict__ rad, int passes, int64_t 
     sum[3 * p + 2] = s2;
     if (moments)
       for (int c = 0; c < 6; ++c) moments[6 * p + c] += m[c];
+  }
+}
+
+// k_accumulate over every chunk of a plan wave: chunk c adds its passes, in
+// pass order, to the running sum of instance c.inst.
+__global__ void k_accumulate_wave(const float* __restrict__ rad, WaveSrc src, float* const* __restrict__ sums) {
+  int64_t n, npix;
+  const WaveChunk* chunks;
+  int nchunks;
+  resolve_wave(src, n, npix, chunks, nchunks);
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < npix; q += (int64_t)gridDim.x * blockDim.x) {
+    const WaveChunk& c = chunks[find_chunk(chunks, nchunks, q, [](const WaveChunk& w) { return w.pix0; })];
+    const int64_t p = q - c.pix0;
+    float* sum = sums[c.inst];
+    float s0 = sum[3 * p], s1 = sum[3 * p + 1], s2 = sum[3 * p + 2];
+    for (int k = 0; k < c.passes; ++k) {
+      const float* r = rad + 3 * (c.path0 + (int64_t)k * c.wh + p);
+      s0 += r[0];
+      s1 += r[1];
+      s2 += r[2];
+    }
+    sum[3 * p] = s0;
+    sum[3 * p + 1] = s1;
+    sum[3 * p + 2] = s2;
   }
 }
 
@@ -446,21 +544,28 @@ __global__ void k_sample_condition(const DScene* S, int medium, int64_t n, const
 using namespace mupsi;
 
 // ------------------------------------------------------------ scene handle
+// Path state of one wave (SoA, grow-only) and the bounce iterations its queue
+// counters were sized for.
+struct PathBuf {
+  Paths paths{};
+  void* mem = nullptr;
+  size_t bytes = 0;
+  int64_t cap = 0;
+  int iters = 0;
+};
+
 struct mupsi_scene {
   DScene h;                 // host copy (pointers are device pointers)
   DScene* d = nullptr;      // device copy
+  DScene** d_list = nullptr;  // device array {d}: the wave kernels' scene table
+  WaveChunk* d_chunk = nullptr;  // device chunk table of one single-scene wave
   std::vector<void*> allocs;
   int width = 0, height = 0, max_bounce = 0;
   // progressive framebuffer: running sum and passes so far
   float* sum = nullptr;
   int passes_done = 0;
   int next_pass = -1;  // pass after the last one accumulated
-  // wave buffers (grow-only)
-  Paths paths{};
-  void* paths_mem = nullptr;
-  size_t paths_bytes = 0;
-  int64_t paths_cap = 0;
-  int max_iters = 0;
+  PathBuf pb;  // wave buffers (grow-only)
   int* err = nullptr;
   unsigned long long* counters = nullptr;
   // profiling: per-launch event pairs, recorded while `profile` is set
@@ -534,19 +639,15 @@ mupsi_scene::~mupsi_scene() {
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     for (void* p : allocs) cudaFree(p);
     if (d) cudaFree(d);
+    if (d_list) cudaFree(d_list);
+    if (d_chunk) cudaFree(d_chunk);
     if (sum) cudaFree(sum);
-    if (paths_mem) pool_give(paths_mem, paths_bytes);
+    if (pb.mem) pool_give(pb.mem, pb.bytes);
     if (err) cudaFree(err);
     if (counters) cudaFree(counters);
 }
 
 namespace {
-
-bool desc_cacheable(const mupsi_scene_desc* desc) {
-  for (int i = 0; i < desc->num_media; ++i)
-    if (desc->media[i].kernel.points_per_cell > CACHE_MAX_PPC) return false;
-  return true;
-}
 
 int build_scene(const mupsi_scene_desc* desc, mupsi_scene* s) {
   DScene& S = s->h;
@@ -578,18 +679,12 @@ int build_scene(const mupsi_scene_desc* desc, mupsi_scene* s) {
   for (int i = 0; i < desc->num_meshes; ++i)
     if (int e = make_device_mesh(desc->meshes[i], S.meshes[i], s->allocs)) return e;
   S.nmed = desc->num_media;
-  // lane groups share psi sums; a mesh mean's BVH queries would run on every
-  // lane of a group, so scenes with mesh means start from single-lane marches
-  // lane groups of >= 4 share psi sums and, when every medium has at most
-  // CACHE_MAX_PPC impulses per cell, keep the impulse window in shared memory
+  // lane groups of >= 4 share psi sums; scenes whose media all have sphere
+  // means run the march specialised for them
   S.min_group = 4;
   S.sphere_only = 1;
   for (int i = 0; i < desc->num_media; ++i)
     if (desc->media[i].mean_type != MUPSI_MEAN_SPHERE) S.sphere_only = 0;
-  // The shared-memory impulse cache measured slower than regenerating impulses
-  // (the march is latency- rather than issue-bound); it stays selectable.
-  S.cache = 0;
-  if (const char* e = std::getenv("MUPSI_MARCH_CACHE")) S.cache = (std::atoi(e) != 0) && desc_cacheable(desc);
   for (int i = 0; i < desc->num_media; ++i) {
     const mupsi_medium_desc& m = desc->media[i];
     if (int e = check_kernel(&m.kernel)) return e;
@@ -687,6 +782,9 @@ int build_scene(const mupsi_scene_desc* desc, mupsi_scene* s) {
   S.counters = nullptr;
   MUPSI_CUDA(cudaMalloc(&s->d, sizeof(DScene)));
   MUPSI_CUDA(cudaMemcpy(s->d, &S, sizeof(DScene), cudaMemcpyHostToDevice));
+  MUPSI_CUDA(cudaMalloc(&s->d_list, sizeof(DScene*)));
+  MUPSI_CUDA(cudaMemcpy(s->d_list, &s->d, sizeof(DScene*), cudaMemcpyHostToDevice));
+  MUPSI_CUDA(cudaMalloc(&s->d_chunk, sizeof(WaveChunk)));
   s->width = desc->width;
   s->height = desc->height;
   s->max_bounce = desc->max_bounce;
@@ -698,18 +796,18 @@ int build_scene(const mupsi_scene_desc* desc, mupsi_scene* s) {
 // PathTracer::trace's do-while runs at least one bounce iteration
 int wave_iters(const mupsi_scene* s) { return std::max(1, s->max_bounce); }
 
-int ensure_paths(mupsi_scene* s, int64_t cap) {
-  int iters = wave_iters(s) + 1;
-  if (cap <= s->paths_cap && iters <= s->max_iters) return MUPSI_OK;
-  if (s->paths_mem) {
-    pool_give(s->paths_mem, s->paths_bytes);
-    s->paths_mem = nullptr;
+int ensure_paths(PathBuf& b, int64_t cap, int iters) {
+  if (cap <= b.cap && iters <= b.iters) return MUPSI_OK;
+  if (b.mem) {
+    pool_give(b.mem, b.bytes);
+    b.mem = nullptr;
   }
-  cap = std::max(cap, s->paths_cap);
+  cap = std::max(cap, b.cap);
+  iters = std::max(iters, b.iters);
   size_t bytes = 0;
-  auto take = [&](size_t b) {
+  auto take = [&](size_t sz) {
     size_t off = bytes;
-    bytes += (b + 255) & ~(size_t)255;
+    bytes += (sz + 255) & ~(size_t)255;
     return off;
   };
   size_t o_o = take(cap * 16), o_d = take(cap * 16), o_t = take(cap * 16), o_e = take(cap * 16),
@@ -723,9 +821,9 @@ int ensure_paths(mupsi_scene* s, int64_t cap) {
     MUPSI_CUDA(cudaMalloc((void**)&base, bytes));
     got = bytes;
   }
-  s->paths_mem = base;
-  s->paths_bytes = got;
-  Paths& P = s->paths;
+  b.mem = base;
+  b.bytes = got;
+  Paths& P = b.paths;
   P.o = (float4*)(base + o_o);
   P.d = (float4*)(base + o_d);
   P.thr = (float4*)(base + o_t);
@@ -744,71 +842,110 @@ int ensure_paths(mupsi_scene* s, int64_t cap) {
   P.counts = (uint32_t*)(base + o_c);
   P.cursors = (uint32_t*)(base + o_cur);
   P.cap = cap;
-  s->paths_cap = cap;
-  s->max_iters = iters;
+  b.cap = cap;
+  b.iters = iters;
   return MUPSI_OK;
 }
+int ensure_paths(mupsi_scene* s, int64_t cap) { return ensure_paths(s->pb, cap, wave_iters(s) + 1); }
 
-// Persistent march grid: resident blocks per SM x SMs, for the cached (dynamic
-// shared memory: one slot table per lane group of 4) or uncached kernel.
+// Launch shapes of the wave kernels (mupsi_gpu_set_tuning; chosen by the
+// project's autotuner, mupsi_b200/autotune.py).
+mupsi_tuning g_tuning = {128, 4, 128, 0};
+
+// Persistent march grid: resident blocks per SM x SMs.
 struct MarchLaunch {
-  void (*fn)(const DScene*, Paths, int);
-  int blocks;
-  size_t smem;
+  void (*fn)(const DScene* const*, Paths, int, WaveCfg);
+  int blocks, block;
 };
-// variant: bit 0 = impulse cache, bit 1 = sphere means only
-MarchLaunch march_launch(bool cache, bool sphere_only) {
-  static MarchLaunch ml[4] = {};
-  const int v = (cache ? 1 : 0) | (sphere_only ? 2 : 0);
-  MarchLaunch& m = ml[v];
-  if (!m.blocks) {
-    switch (v) {
-      case 0: m.fn = k_march<false, MEAN_ANY>; break;
-      case 1: m.fn = k_march<true, MEAN_ANY>; break;
-      case 2: m.fn = k_march<false, MEAN_SPHERE_ONLY>; break;
-      default: m.fn = k_march<true, MEAN_SPHERE_ONLY>; break;
-    }
-    m.smem = cache ? (size_t)(128 / 4) * kCacheBytes : 0;
-    if (cache) cudaFuncSetAttribute(m.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m.smem);
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, m.fn, 128, m.smem);
-    m.blocks = std::max(1, per_sm) * num_sms();
-  }
+MarchLaunch march_launch(bool sphere_only) {
+  static std::mutex mu;
+  static std::vector<std::pair<int, MarchLaunch>> memo;  // key: variant | block << 1
+  const int block = g_tuning.march_block;
+  const int key = (sphere_only ? 1 : 0) | (block << 1);
+  std::lock_guard<std::mutex> lock(mu);
+  for (auto& e : memo)
+    if (e.first == key) return e.second;
+  MarchLaunch m;
+  m.fn = sphere_only ? k_march<MEAN_SPHERE_ONLY> : k_march<MEAN_ANY>;
+  m.block = block;
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, m.fn, block, 0);
+  m.blocks = std::max(1, per_sm) * num_sms();
+  memo.push_back({key, m});
   return m;
 }
-void launch_march(const MarchLaunch& ml, const DScene* d, const Paths& P, int it, cudaStream_t st) {
-  ml.fn<<<ml.blocks, 128, ml.smem, st>>>(d, P, it);
+
+// Everything one wave's kernels need besides where its paths come from.
+struct WaveExec {
+  const DScene* const* scenes;  // device scene table
+  Paths P;
+  int iters;                    // bounce iterations: max over the wave's scenes of max(1, max_bounce)
+  bool sphere_only;
+  WaveCfg cfg;
+};
+
+// Launch one wave: clear the queue counters, generate the paths, then `iters`
+// bounce iterations of march + shade. Grids do not depend on the wave's size
+// (raygen and shade are grid-stride loops, the march is persistent), so the
+// same launches serve every wave of a plan. `prof` (nullable) records CUDA
+// events around each march and shade.
+void launch_wave(const WaveExec& w, const WaveSrc& src, cudaStream_t st, mupsi_scene* prof) {
+  k_wave_begin<<<1, 256, 0, st>>>(w.P, w.iters, const_cast<int*>(src.wave_idx));
+  int64_t gb = (int64_t)num_sms() * 16;
+  if (!src.wave_idx) gb = std::max<int64_t>(1, std::min<int64_t>(gb, (src.n + 255) / 256));
+  k_raygen<<<(int)gb, 256, 0, st>>>(w.scenes, w.P, src);
+  const MarchLaunch ml = march_launch(w.sphere_only);
+  const int sblock = g_tuning.shade_block;
+  const int sb = num_sms() * (2048 / sblock);
+  for (int it = 0; it < w.iters; ++it) {
+    if (prof && prof->profile) {
+      cudaEvent_t a = prof->next_event(), b = prof->next_event(), c = prof->next_event();
+      cudaEventRecord(a, st);
+      ml.fn<<<ml.blocks, ml.block, 0, st>>>(w.scenes, w.P, it, w.cfg);
+      cudaEventRecord(b, st);
+      k_shade<<<sb, sblock, 0, st>>>(w.scenes, w.P, it, w.cfg);
+      cudaEventRecord(c, st);
+      prof->ev_march.push_back({a, b});
+      prof->ev_shade.push_back({b, c});
+    } else {
+      ml.fn<<<ml.blocks, ml.block, 0, st>>>(w.scenes, w.P, it, w.cfg);
+      k_shade<<<sb, sblock, 0, st>>>(w.scenes, w.P, it, w.cfg);
+    }
+  }
+}
+int wave_launches(int iters) { return 2 + 2 * iters; }
+
+WaveExec scene_exec(mupsi_scene* s) {
+  WaveExec w;
+  w.scenes = s->d_list;
+  w.P = s->pb.paths;
+  w.iters = wave_iters(s);
+  w.sphere_only = s->h.sphere_only != 0;
+  w.cfg.min_group = g_tuning.min_group;
+  w.cfg.err = s->err;
+  w.cfg.counters = s->profile ? s->counters : nullptr;
+  return w;
 }
 
-// One wave: n paths, from pass0 (or explicit x/y/k arrays). Leaves radiance in P.rad.
+// One single-scene wave: n paths from pass0 (or explicit x/y/k arrays).
 int run_wave(mupsi_scene* s, int64_t n, int pass0, const int32_t* xs, const int32_t* ys, const int32_t* ks,
              cudaStream_t st) {
-  Paths& P = s->paths;
-  const int iters = wave_iters(s);
-  MUPSI_CUDA(cudaMemsetAsync(P.counts, 0, (size_t)(s->max_iters + 1) * 8, st));
-  MUPSI_CUDA(cudaMemsetAsync(P.cursors, 0, (size_t)(s->max_iters + 1) * 4, st));
-  count_launch(2);
-  int gb = (int)std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 16);
-  k_raygen<<<gb, 256, 0, st>>>(s->d, P, n, pass0, xs, ys, ks);
-  count_launch();
-  const MarchLaunch ml = march_launch(s->h.cache != 0, s->h.sphere_only != 0);
-  int sb = (int)std::min<int64_t>((n + 127) / 128, (int64_t)num_sms() * 16);
-  for (int it = 0; it < iters; ++it) {
-    if (s->profile) {
-      cudaEvent_t a = s->next_event(), b = s->next_event(), c = s->next_event();
-      cudaEventRecord(a, st);
-      launch_march(ml, s->d, P, it, st);
-      cudaEventRecord(b, st);
-      k_shade<<<sb, 128, 0, st>>>(s->d, P, it);
-      cudaEventRecord(c, st);
-      s->ev_march.push_back({a, b});
-      s->ev_shade.push_back({b, c});
-    } else {
-      launch_march(ml, s->d, P, it, st);
-      k_shade<<<sb, 128, 0, st>>>(s->d, P, it);
-    }
-    count_launch(2);
+  WaveExec w = scene_exec(s);
+  WaveSrc src;
+  src.n = n;
+  if (xs) {
+    src.xs = xs;
+    src.ys = ys;
+    src.ks = ks;
+  } else {
+    const int64_t wh = (int64_t)s->width * s->height;
+    WaveChunk c{0, pass0, (int)(n / wh), s->width, 0, wh, 0};
+    MUPSI_CUDA(cudaMemcpyAsync(s->d_chunk, &c, sizeof c, cudaMemcpyHostToDevice, st));
+    src.chunks = s->d_chunk;
+    src.nchunks = 1;
   }
+  launch_wave(w, src, st, s);
+  count_launch(wave_launches(w.iters));
   MUPSI_CUDA(cudaGetLastError());
   return MUPSI_OK;
 }
@@ -820,11 +957,11 @@ void collect_events(mupsi_scene* s) {
     cudaEventElapsedTime(&ms, pr.first, pr.second);
     s->march_ms += ms;
     s->march_launches++;
-    if (first && (int)s->iter_march_ms.size() < s->max_iters) s->iter_march_ms.push_back(ms);
+    if (first && (int)s->iter_march_ms.size() < s->pb.iters) s->iter_march_ms.push_back(ms);
   }
   if (first && !s->ev_march.empty()) {
-    s->iter_counts.resize(2 * (size_t)(s->max_iters + 1));
-    cudaMemcpy(s->iter_counts.data(), s->paths.counts, s->iter_counts.size() * 4, cudaMemcpyDeviceToHost);
+    s->iter_counts.resize(2 * (size_t)(s->pb.iters + 1));
+    cudaMemcpy(s->iter_counts.data(), s->pb.paths.counts, s->iter_counts.size() * 4, cudaMemcpyDeviceToHost);
     s->iter_done = true;
   }
   for (auto& pr : s->ev_shade) {
@@ -854,6 +991,7 @@ int check_err(mupsi_scene* s, cudaStream_t st) {
 int grid_n(int64_t n) { return (int)std::min<int64_t>((n + 127) / 128, (int64_t)num_sms() * 32); }
 
 const int64_t kDefaultWavePaths = 8ll << 20;
+int64_t wave_paths() { return g_tuning.wave_paths > 0 ? g_tuning.wave_paths : kDefaultWavePaths; }
 
 // ---------------------------------------------------------------------------
 // Allocation-free trace (mupsi_gpu_trace_samples_noalloc). Some hosts cannot
@@ -922,6 +1060,133 @@ Paths noalloc_paths(void* base_ptr) {
   P.cursors = (uint32_t*)take((size_t)(kNoAllocMaxIters + 1) * 4);
   P.cap = cap;
   return P;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ batch
+// Several scene instances rendered through one stream of waves. Each wave packs
+// pass chunks of many instances into one path array with one shared queue per
+// bounce iteration; every path carries its instance id (meta.w), so the
+// persistent march balances rays of all instances over the whole GPU. The
+// wave plan (chunks and per-wave ranges) is uploaded once per render and a
+// device wave index steps through it, so one captured graph per bounce count
+// replays every wave.
+namespace {
+struct BatchGraph {
+  int iters;
+  cudaGraphExec_t exec;
+};
+}  // namespace
+
+struct mupsi_batch {
+  std::vector<mupsi_scene*> inst;
+  DScene** d_list = nullptr;
+  float** d_sums = nullptr;
+  int* d_wave_idx = nullptr;
+  int* err = nullptr;
+  WaveChunk* d_chunks = nullptr;
+  size_t chunk_cap = 0;
+  WaveDesc* d_waves = nullptr;
+  size_t wave_cap = 0;
+  PathBuf pb;
+  bool sphere_only = true;
+  cudaStream_t bs = nullptr;  // graphs are captured and replayed on this stream
+  std::vector<BatchGraph> graphs;
+  mupsi_tuning graph_tuning{};  // launch shapes the graphs were captured with
+  std::vector<cudaEvent_t> events;
+  mupsi_batch_info info{};
+  void drop_graphs() {
+    for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
+    graphs.clear();
+  }
+  ~mupsi_batch() {
+    drop_graphs();
+    for (cudaEvent_t e : events) cudaEventDestroy(e);
+    if (bs) cudaStreamDestroy(bs);
+    if (d_list) cudaFree(d_list);
+    if (d_sums) cudaFree(d_sums);
+    if (d_wave_idx) cudaFree(d_wave_idx);
+    if (err) cudaFree(err);
+    if (d_chunks) cudaFree(d_chunks);
+    if (d_waves) cudaFree(d_waves);
+    if (pb.mem) pool_give(pb.mem, pb.bytes);
+  }
+};
+
+namespace {
+
+template <typename T>
+int grow_device(T*& ptr, size_t& cap, size_t need, bool& moved) {
+  if (need <= cap) return MUPSI_OK;
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  cap = std::max(need, 2 * cap);
+  MUPSI_CUDA(cudaMalloc((void**)&ptr, cap * sizeof(T)));
+  moved = true;
+  return MUPSI_OK;
+}
+
+// One wave of the plan on stream bs: paths, bounces, accumulation.
+void batch_wave_launches(mupsi_batch* b, int iters) {
+  WaveExec w;
+  w.scenes = b->d_list;
+  w.P = b->pb.paths;
+  w.iters = iters;
+  w.sphere_only = b->sphere_only;
+  w.cfg.min_group = g_tuning.min_group;
+  w.cfg.err = b->err;
+  w.cfg.counters = nullptr;
+  WaveSrc src;
+  src.chunks = b->d_chunks;
+  src.waves = b->d_waves;
+  src.wave_idx = b->d_wave_idx;
+  launch_wave(w, src, b->bs, nullptr);
+  k_accumulate_wave<<<num_sms() * 16, 128, 0, b->bs>>>(b->pb.paths.rad, src, b->d_sums);
+}
+
+bool same_tuning(const mupsi_tuning& a, const mupsi_tuning& c) {
+  return a.march_block == c.march_block && a.min_group == c.min_group && a.shade_block == c.shade_block;
+}
+
+// The graph of a wave with `iters` bounce iterations, captured on first use.
+int batch_graph(mupsi_batch* b, int iters, cudaGraphExec_t* out) {
+  if (!same_tuning(b->graph_tuning, g_tuning)) {
+    b->drop_graphs();
+    b->graph_tuning = g_tuning;
+  }
+  for (auto& g : b->graphs)
+    if (g.iters == iters) {
+      *out = g.exec;
+      return MUPSI_OK;
+    }
+  march_launch(b->sphere_only);  // occupancy query outside the capture
+  cudaGraph_t graph = nullptr;
+  MUPSI_CUDA(cudaStreamBeginCapture(b->bs, cudaStreamCaptureModeThreadLocal));
+  batch_wave_launches(b, iters);
+  cudaError_t e = cudaStreamEndCapture(b->bs, &graph);
+  if (e != cudaSuccess) return fail(MUPSI_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  cudaGraphExec_t exec = nullptr;
+  e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return fail(MUPSI_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  b->graphs.push_back({iters, exec});
+  b->info.graphs_captured++;
+  *out = exec;
+  return MUPSI_OK;
+}
+
+int check_batch_err(mupsi_batch* b) {
+  int h = 0;
+  MUPSI_CUDA(cudaMemcpy(&h, b->err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) {
+    cudaMemset(b->err, 0, sizeof(int));
+    if (h & ERR_BVH_STACK) return fail(MUPSI_ERR_DEVICE_LIMIT, "BVH traversal exceeded the 64-entry stack");
+    return fail(MUPSI_ERR_DEVICE_LIMIT, "march iteration cap reached");
+  }
+  for (mupsi_scene* s : b->inst)
+    if (int e = check_err(s, b->bs)) return e;
+  return MUPSI_OK;
 }
 
 }  // namespace
@@ -1044,9 +1309,9 @@ int mupsi_gpu_trace_samples(mupsi_scene* scene, int64_t n, const int32_t* x, con
   MUPSI_CUDA(dk.in(k, n, mem));
   if (int e = run_wave(scene, n, 0, dx.ptr, dy.ptr, dk.ptr, st)) return e;
   if (mem == MUPSI_MEM_DEVICE) {
-    MUPSI_CUDA(cudaMemcpyAsync(out_rgb, scene->paths.rad, n * 12, cudaMemcpyDeviceToDevice, st));
+    MUPSI_CUDA(cudaMemcpyAsync(out_rgb, scene->pb.paths.rad, n * 12, cudaMemcpyDeviceToDevice, st));
   } else {
-    MUPSI_CUDA(cudaMemcpyAsync(out_rgb, scene->paths.rad, n * 12, cudaMemcpyDeviceToHost, st));
+    MUPSI_CUDA(cudaMemcpyAsync(out_rgb, scene->pb.paths.rad, n * 12, cudaMemcpyDeviceToHost, st));
   }
   return check_err(scene, st);
 }
@@ -1068,7 +1333,7 @@ int mupsi_gpu_render(mupsi_scene* scene, const mupsi_render_args* a) {
     MUPSI_CUDA(cudaMemsetAsync(dmom, 0, wh * 6 * sizeof(double), st));
   }
   int total = a->spp_end - a->spp_begin;
-  int per_wave = (int)std::max<int64_t>(1, std::min<int64_t>(total, kDefaultWavePaths / wh));
+  int per_wave = (int)std::max<int64_t>(1, std::min<int64_t>(total, wave_paths() / wh));
   if (total > 0) {
     if (int e = ensure_paths(scene, (int64_t)per_wave * wh)) return e;
   }
@@ -1080,7 +1345,7 @@ int mupsi_gpu_render(mupsi_scene* scene, const mupsi_render_args* a) {
     }
     int passes = std::min(per_wave, a->spp_end - k0);
     if ((rc = run_wave(scene, (int64_t)passes * wh, k0, nullptr, nullptr, nullptr, st))) break;
-    k_accumulate<<<grid_n(wh), 128, 0, st>>>(scene->paths.rad, passes, wh, scene->sum, dmom);
+    k_accumulate<<<grid_n(wh), 128, 0, st>>>(scene->pb.paths.rad, passes, wh, scene->sum, dmom);
     count_launch();
     scene->passes_done += passes;
     scene->next_pass = k0 + passes;
@@ -1137,21 +1402,17 @@ int mupsi_gpu_trace_samples_noalloc(mupsi_scene* scene, int64_t n, const int32_t
   void* scratch = nullptr;
   if (int e = noalloc_scratch(&scratch)) return e;
   cudaStream_t st = (cudaStream_t)stream;  // NULL: the default stream (no stream is created here)
-  Paths P = noalloc_paths(scratch);
-  const int iters = std::max(1, scene->max_bounce);
-  // the array keeps the previous call's contents: clear the queue counters and cursors
-  MUPSI_CUDA(cudaMemsetAsync(P.counts, 0, (size_t)(iters + 1) * 8, st));
-  MUPSI_CUDA(cudaMemsetAsync(P.cursors, 0, (size_t)(iters + 1) * 4, st));
-  int gb = (int)std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 16);
-  k_raygen<<<gb, 256, 0, st>>>(scene->d, P, n, 0, x, y, k);
-  const MarchLaunch ml = march_launch(scene->h.cache != 0, scene->h.sphere_only != 0);
-  int sb = (int)std::min<int64_t>((n + 127) / 128, (int64_t)num_sms() * 16);
-  for (int it = 0; it < iters; ++it) {
-    launch_march(ml, scene->d, P, it, st);
-    k_shade<<<sb, 128, 0, st>>>(scene->d, P, it);
-  }
-  count_launch(1 + 2 * iters);
+  WaveExec w = scene_exec(scene);
+  w.P = noalloc_paths(scratch);  // launch_wave clears its queue counters and cursors
+  WaveSrc src;
+  src.n = n;
+  src.xs = x;
+  src.ys = y;
+  src.ks = k;
+  launch_wave(w, src, st, nullptr);
+  count_launch(wave_launches(w.iters));
   MUPSI_CUDA(cudaGetLastError());
+  const Paths& P = w.P;
   MUPSI_CUDA(cudaMemcpyAsync(out_rgb, P.rad, n * 12, cudaMemcpyDeviceToDevice, st));
   return check_err(scene, st);
 }
@@ -1199,6 +1460,219 @@ int mupsi_gpu_scene_stats(mupsi_scene* scene, mupsi_render_stats* out, int32_t r
     scene->march_launches = scene->shade_launches = 0;
   }
   return MUPSI_OK;
+}
+
+int mupsi_gpu_set_tuning(const mupsi_tuning* t) {
+  clear_error();
+  if (!t) return fail(MUPSI_ERR_INVALID, "null tuning");
+  if (t->march_block < 32 || t->march_block > 128 || t->march_block % 32)
+    return fail(MUPSI_ERR_INVALID, "march_block must be 32, 64, 96 or 128");
+  if (t->min_group < 4 || t->min_group > 32 || (t->min_group & (t->min_group - 1)))
+    return fail(MUPSI_ERR_INVALID, "min_group must be 4, 8, 16 or 32");
+  if (t->shade_block < 32 || t->shade_block > 128 || t->shade_block % 32)
+    return fail(MUPSI_ERR_INVALID, "shade_block must be a multiple of 32 in [32, 128]");
+  if (t->wave_paths < 0 || t->wave_paths > (1 << 28)) return fail(MUPSI_ERR_INVALID, "wave_paths out of range");
+  g_tuning = *t;
+  return MUPSI_OK;
+}
+
+int mupsi_gpu_get_tuning(mupsi_tuning* out) {
+  clear_error();
+  if (!out) return fail(MUPSI_ERR_INVALID, "null argument");
+  *out = g_tuning;
+  return MUPSI_OK;
+}
+
+int mupsi_gpu_batch_create(int32_t num_scenes, mupsi_scene* const* scenes, mupsi_batch** out) {
+  clear_error();
+  if (!out) return fail(MUPSI_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (num_scenes <= 0 || !scenes) return fail(MUPSI_ERR_INVALID, "a batch needs at least one scene");
+  if (num_scenes > (1 << 20)) return fail(MUPSI_ERR_INVALID, "at most 2^20 scenes per batch");
+  std::unique_ptr<mupsi_batch> b(new mupsi_batch);
+  std::vector<DScene*> list;
+  std::vector<float*> sums;
+  for (int i = 0; i < num_scenes; ++i) {
+    if (!scenes[i]) return fail(MUPSI_ERR_INVALID, "null scene in batch");
+    b->inst.push_back(scenes[i]);
+    list.push_back(scenes[i]->d);
+    sums.push_back(scenes[i]->sum);
+    if (!scenes[i]->h.sphere_only) b->sphere_only = false;
+  }
+  MUPSI_CUDA(cudaMalloc((void**)&b->d_list, list.size() * sizeof(DScene*)));
+  MUPSI_CUDA(cudaMemcpy(b->d_list, list.data(), list.size() * sizeof(DScene*), cudaMemcpyHostToDevice));
+  MUPSI_CUDA(cudaMalloc((void**)&b->d_sums, sums.size() * sizeof(float*)));
+  MUPSI_CUDA(cudaMemcpy(b->d_sums, sums.data(), sums.size() * sizeof(float*), cudaMemcpyHostToDevice));
+  MUPSI_CUDA(cudaMalloc((void**)&b->d_wave_idx, sizeof(int)));
+  MUPSI_CUDA(cudaMalloc((void**)&b->err, sizeof(int)));
+  MUPSI_CUDA(cudaMemset(b->err, 0, sizeof(int)));
+  MUPSI_CUDA(cudaStreamCreateWithFlags(&b->bs, cudaStreamNonBlocking));
+  *out = b.release();
+  return MUPSI_OK;
+}
+
+int mupsi_gpu_batch_destroy(mupsi_batch* batch) {
+  clear_error();
+  if (!batch) return MUPSI_OK;
+  cudaStreamSynchronize(batch->bs);
+  delete batch;
+  return MUPSI_OK;
+}
+
+int mupsi_gpu_batch_info(const mupsi_batch* batch, mupsi_batch_info* out) {
+  clear_error();
+  if (!batch || !out) return fail(MUPSI_ERR_INVALID, "null argument");
+  *out = batch->info;
+  return MUPSI_OK;
+}
+
+int mupsi_gpu_batch_render(mupsi_batch* b, const mupsi_batch_args* a) {
+  clear_error();
+  if (!b || !a || !a->spp) return fail(MUPSI_ERR_INVALID, "null argument");
+  const int n = (int)b->inst.size();
+  for (int i = 0; i < n; ++i)
+    if (a->spp[i] < 0) return fail(MUPSI_ERR_INVALID, "negative spp");
+  if (a->schedule != MUPSI_SCHEDULE_SHORTEST_FIRST && a->schedule != MUPSI_SCHEDULE_IN_ORDER)
+    return fail(MUPSI_ERR_INVALID, "unknown schedule");
+  b->info.waves = b->info.graph_launches = b->info.max_iters = 0;
+  b->info.paths = 0;
+  // ---- plan: instances in schedule order, their passes packed into waves of
+  // at most wave_paths() paths (a pass is never split across waves)
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  auto work = [&](int i) { return (int64_t)a->spp[i] * b->inst[i]->width * b->inst[i]->height; };
+  if (a->schedule == MUPSI_SCHEDULE_SHORTEST_FIRST)
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return work(x) < work(y); });
+  const int64_t W = wave_paths();
+  std::vector<WaveChunk> chunks;
+  std::vector<WaveDesc> waves;
+  std::vector<int> wave_iters_v, last_wave(n, -1);
+  WaveDesc cur{0, 0, 0, 0};
+  int cur_iters = 0;
+  auto close_wave = [&]() {
+    if (cur.nchunks == 0) return;
+    waves.push_back(cur);
+    wave_iters_v.push_back(cur_iters);
+    cur = WaveDesc{0, 0, (int)chunks.size(), 0};
+    cur_iters = 0;
+  };
+  for (int i : order) {
+    mupsi_scene* s = b->inst[i];
+    const int64_t wh = (int64_t)s->width * s->height;
+    int pass = 0;
+    while (pass < a->spp[i]) {
+      int64_t fit = (W - cur.n) / wh;
+      if (fit <= 0) {
+        if (cur.n > 0) {
+          close_wave();
+          continue;
+        }
+        fit = 1;
+      }
+      const int take = (int)std::min<int64_t>(fit, a->spp[i] - pass);
+      chunks.push_back(WaveChunk{i, pass, take, s->width, cur.n, wh, cur.npix});
+      cur.n += (int64_t)take * wh;
+      cur.npix += wh;
+      cur.nchunks++;
+      cur_iters = std::max(cur_iters, wave_iters(s));
+      pass += take;
+      last_wave[i] = (int)waves.size();
+    }
+  }
+  close_wave();
+  // ---- buffers
+  int64_t max_n = 0;
+  int max_it = 0;
+  for (size_t w = 0; w < waves.size(); ++w) {
+    max_n = std::max(max_n, waves[w].n);
+    max_it = std::max(max_it, wave_iters_v[w]);
+  }
+  bool moved = false;
+  if (!waves.empty()) {
+    if (max_n > b->pb.cap || max_it + 1 > b->pb.iters) moved = true;
+    if (int e = ensure_paths(b->pb, max_n, max_it + 1)) return e;
+    if (int e = grow_device(b->d_chunks, b->chunk_cap, chunks.size(), moved)) return e;
+    if (int e = grow_device(b->d_waves, b->wave_cap, waves.size(), moved)) return e;
+  }
+  if (moved) b->drop_graphs();
+  // events[0]: start of the first wave; events[1 + w]: end of wave w
+  while (b->events.size() < waves.size() + 1) {
+    cudaEvent_t e;
+    MUPSI_CUDA(cudaEventCreate(&e));
+    b->events.push_back(e);
+  }
+  cudaStream_t st = resolve_stream(a->stream);
+  // the batch stream starts after the caller's stream's earlier work
+  MUPSI_CUDA(cudaEventRecord(b->events[0], st));
+  MUPSI_CUDA(cudaStreamWaitEvent(b->bs, b->events[0], 0));
+  cudaStream_t bs = b->bs;
+  if (!waves.empty()) {
+    MUPSI_CUDA(cudaMemcpyAsync(b->d_chunks, chunks.data(), chunks.size() * sizeof(WaveChunk), cudaMemcpyHostToDevice, bs));
+    MUPSI_CUDA(cudaMemcpyAsync(b->d_waves, waves.data(), waves.size() * sizeof(WaveDesc), cudaMemcpyHostToDevice, bs));
+  }
+  for (int i = 0; i < n; ++i) {
+    mupsi_scene* s = b->inst[i];
+    if (a->spp[i] > 0) MUPSI_CUDA(cudaMemsetAsync(s->sum, 0, (size_t)s->width * s->height * 12, bs));
+    s->passes_done = a->spp[i];
+    s->next_pass = a->spp[i];
+  }
+  MUPSI_CUDA(cudaMemsetAsync(b->d_wave_idx, 0xff, sizeof(int), bs));  // -1: k_wave_begin steps to 0
+  MUPSI_CUDA(cudaEventRecord(b->events[0], bs));
+  int rc = MUPSI_OK;
+  for (size_t w = 0; w < waves.size(); ++w) {
+    if (a->cancel && *a->cancel) {
+      rc = fail(MUPSI_ERR_CANCELLED, "render cancelled");
+      break;
+    }
+    const int iters = wave_iters_v[w];
+    if (a->use_graphs) {
+      cudaGraphExec_t exec = nullptr;
+      if ((rc = batch_graph(b, iters, &exec))) break;
+      cudaError_t e = cudaGraphLaunch(exec, bs);
+      if (e != cudaSuccess) {
+        rc = fail(MUPSI_ERR_CUDA, std::string("graph launch: ") + cudaGetErrorString(e));
+        break;
+      }
+      b->info.graph_launches++;
+    } else {
+      batch_wave_launches(b, iters);
+    }
+    count_launch(wave_launches(iters) + 1);
+    b->info.waves++;
+    b->info.max_iters = std::max(b->info.max_iters, iters);
+    b->info.paths += waves[w].n;
+    MUPSI_CUDA(cudaEventRecord(b->events[1 + w], bs));
+  }
+  if (rc == MUPSI_OK) {
+    MUPSI_CUDA(cudaGetLastError());
+    for (int i = 0; i < n; ++i) {
+      mupsi_scene* s = b->inst[i];
+      if (!a->rgb_out || !a->rgb_out[i] || a->spp[i] == 0) continue;
+      const int64_t wh = (int64_t)s->width * s->height;
+      const float inv = 1.0f / (float)a->spp[i];
+      if (a->out_mem == MUPSI_MEM_DEVICE) {
+        k_average<<<grid_n(wh * 3), 128, 0, bs>>>(s->sum, wh * 3, inv, a->rgb_out[i]);
+        count_launch();
+      } else {
+        float* tmp = nullptr;
+        MUPSI_CUDA(cudaMallocAsync((void**)&tmp, wh * 12, bs));
+        k_average<<<grid_n(wh * 3), 128, 0, bs>>>(s->sum, wh * 3, inv, tmp);
+        count_launch();
+        MUPSI_CUDA(cudaMemcpyAsync(a->rgb_out[i], tmp, wh * 12, cudaMemcpyDeviceToHost, bs));
+        MUPSI_CUDA(cudaFreeAsync(tmp, bs));
+      }
+    }
+  }
+  MUPSI_CUDA(cudaStreamSynchronize(bs));
+  if (rc == MUPSI_OK && a->done_ms) {
+    for (int i = 0; i < n; ++i) {
+      float ms = 0.0f;
+      if (last_wave[i] >= 0) MUPSI_CUDA(cudaEventElapsedTime(&ms, b->events[0], b->events[1 + last_wave[i]]));
+      a->done_ms[i] = ms;
+    }
+  }
+  int e = check_batch_err(b);
+  return rc ? rc : e;
 }
 
 }  // extern "C"

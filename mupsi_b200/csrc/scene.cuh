@@ -51,7 +51,6 @@ struct DScene {
   int* err;
   unsigned long long* counters;  // nullable: [0] march steps visited, [1] psi evaluations, [2] marches
   int min_group;                 // smallest lane group per march
-  int cache;                     // marches keep impulses in shared memory (every medium has ppc <= 3)
   int sphere_only;               // every mean is a sphere: the march kernel without BVH code
 };
 
@@ -348,11 +347,12 @@ MD bool march_cheap(const DScene* S, March& m, v3& p, bool& ovf) {
 
 // Phase B: f at the pending point (value only); decides hit or next step. The
 // psi sum is shared by the lanes of group g (all of which hold the same march).
-template <int MK = MEAN_ANY>
-MD void march_psi(const DScene* S, March& m, v3 p, const Group& g, bool& ovf, const ImpCache* cache = nullptr) {
+// WIDE: the group has G >= 4 lanes.
+template <int MK = MEAN_ANY, bool WIDE = false>
+MD void march_psi(const DScene* S, March& m, v3 p, const Group& g, bool& ovf) {
   const DMedium& md = S->media[m.medium];
   m.n_psi++;
-  float q = cache ? raw_noise_value_cached(md.k, p, m.seed, g, *cache) : raw_noise_value_group(md.k, p, m.seed, g);
+  float q = raw_noise_value_group<WIDE>(md.k, p, m.seed, g);
   float c = m.c.active ? cond_value(md.k, m.c, p) : 0.0f;
   float f;
   if (m.pend_exact) {
@@ -389,26 +389,25 @@ MD void march_psi(const DScene* S, March& m, v3 p, const Group& g, bool& ovf, co
   march_advance(S, m, -INFINITY);
 }
 
-// GPMedium::evalWithGradient with the psi sum shared by group g
-template <int MK = MEAN_ANY>
+// GPMedium::evalWithGradient with the psi sum shared by group g (WIDE: g.G >= 4)
+template <int MK = MEAN_ANY, bool WIDE = false>
 MD float4 medium_eval_group(const DScene* S, const DMedium& md, v3 p, uint32_t seed, const Cond& c, bool& ovf,
-                            const Group& g, const ImpCache* cache = nullptr) {
+                            const Group& g) {
   float4 mu = mean_value_grad<MK>(S, md, p, ovf);
-  float4 nz = cache ? raw_noise_cached(md.k, p, seed, g, *cache) : raw_noise_group(md.k, p, seed, g);
+  float4 nz = raw_noise_group<WIDE>(md.k, p, seed, g);
   float4 f = make_float4(mu.x + nz.x, mu.y + nz.y, mu.z + nz.z, mu.w + nz.w);
   return add_cond(md.k, c, p, f);
 }
 
 // hit point and normal of a finished march
 // (an exited march leaves t, p and normal zero: sampleDistance does not write them)
-template <int MK = MEAN_ANY>
-MD void march_result(const DScene* S, const March& m, mupsi_medium_sample& out, bool& ovf, const Group& g,
-                     const ImpCache* cache = nullptr) {
+template <int MK = MEAN_ANY, bool WIDE = false>
+MD void march_result(const DScene* S, const March& m, mupsi_medium_sample& out, bool& ovf, const Group& g) {
   out.exited = m.status == 1 ? 0u : 1u;
   out.t = m.status == 1 ? m.t : 0.0f;
   if (m.status == 1) {
     v3 p = m.o + m.d * m.t;
-    float4 f = medium_eval_group<MK>(S, S->media[m.medium], p, m.seed, m.c, ovf, g, cache);
+    float4 f = medium_eval_group<MK, WIDE>(S, S->media[m.medium], p, m.seed, m.c, ovf, g);
     v3 n = normalized(mk3(f.y, f.z, f.w));
     st3(out.p, p);
     st3(out.normal, n);

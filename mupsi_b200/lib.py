@@ -46,6 +46,12 @@ def _setup(L):
     L.mupsi_gpu_trace_samples_noalloc.argtypes = [vp, i64, vp, vp, vp, vp, vp]
     L.mupsi_gpu_scene_profile.argtypes = [vp, i32]
     L.mupsi_gpu_scene_stats.argtypes = [vp, C.POINTER(_abi.RenderStats), i32]
+    L.mupsi_gpu_set_tuning.argtypes = [C.POINTER(_abi.Tuning)]
+    L.mupsi_gpu_get_tuning.argtypes = [C.POINTER(_abi.Tuning)]
+    L.mupsi_gpu_batch_create.argtypes = [i32, C.POINTER(vp), C.POINTER(vp)]
+    L.mupsi_gpu_batch_destroy.argtypes = [vp]
+    L.mupsi_gpu_batch_render.argtypes = [vp, C.POINTER(_abi.BatchArgs)]
+    L.mupsi_gpu_batch_info.argtypes = [vp, C.POINTER(_abi.BatchInfo)]
     return L
 
 

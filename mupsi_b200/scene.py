@@ -393,3 +393,36 @@ def config_mesh_scene(level=6, width=512, height=512, spp=64, seed=0):
     fm = s.add_mesh(Mesh(fv, ff))
     s.add_mesh_primitive(fm, bsdf=_abi.BSDF_LAMBERTIAN, albedo=0.7)
     return s
+
+
+def batch_scenes(n=64, seed=4):
+    """Uneven scene instances for one batched render, seeded: resolution from
+    {64^2, 128^2, 256^2, 512^2}, spp in [4, 64], max_bounce in [2, 10],
+    length_scale ~ U(0.25, 4), points_per_cell from {1, 3, 8}, a sphere mean of
+    radius r ~ U(20, 100) inside a null bounding sphere of radius 1.8 r, and half
+    of the instances single_realization, half renewal_plus. Each instance is the
+    plain-method scene (camera at the origin along -z, fov 45, constant sky 1)
+    with the bounding sphere framed as config0_scene frames its r = 130 sphere."""
+    rng = np.random.default_rng(seed)
+    modes = rng.permutation([_abi.GP_SINGLE_REALIZATION] * (n // 2) + [_abi.GP_RENEWAL_PLUS] * (n - n // 2))
+    out = []
+    for i in range(n):
+        res = int(rng.choice([64, 128, 256, 512]))
+        spp = int(rng.integers(4, 65))
+        mb = int(rng.integers(2, 11))
+        ls = float(rng.uniform(0.25, 4.0))
+        ppc = int(rng.choice([1, 3, 8]))
+        r = float(rng.uniform(20.0, 100.0))
+        big = 1.8 * r
+        z = -500.0 * big / 130.0
+        s = Scene()
+        s.width = s.height = res
+        s.spp = spp
+        s.max_bounce = s.max_medium_bounce = mb
+        s.gp_mode = int(modes[i])
+        s.sky = (1.0, 1.0, 1.0)
+        m = s.add_medium("sphere", center=(0, 0, z), radius=r, sigma=1.0, length_scale=ls, aniso=(1, 1, 1),
+                         points_per_cell=ppc)
+        s.add_sphere((0, 0, z), big, bsdf=_abi.BSDF_NULL, int_medium=m)
+        out.append(s)
+    return out

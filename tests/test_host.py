@@ -106,3 +106,42 @@ def test_icosphere_sizes():
         assert 20 * 4**level == nf and 10 * 4**level + 2 == nv
     v, f = S.icosphere(3)
     assert len(f) == 1280 and len(v) == 642
+
+
+def test_batch_scenes_parameters():
+    from mupsi_b200 import _abi
+    sc = S.batch_scenes()
+    assert len(sc) == 64
+    assert {s.width for s in sc} <= {64, 128, 256, 512} and all(s.width == s.height for s in sc)
+    assert all(4 <= s.spp <= 64 and 2 <= s.max_bounce <= 10 for s in sc)
+    assert sum(s.gp_mode == _abi.GP_SINGLE_REALIZATION for s in sc) == 32
+    for s in sc:
+        m = s.media[0]
+        assert 0.25 <= m["length"] <= 4.0 and m["ppc"] in (1, 3, 8) and 20.0 <= m["radius"] <= 100.0
+        assert abs(s.primitives[0]["radius"] - 1.8 * m["radius"]) < 1e-3
+    again = S.batch_scenes()
+    assert [(s.width, s.spp, s.media[0]["length"]) for s in sc] == [(s.width, s.spp, s.media[0]["length"])
+                                                                    for s in again]
+
+
+def test_autotune_coordinate_descent():
+    from mupsi_b200.autotune import CANDIDATES, DEFAULT, coordinate_descent
+    target = {"march_block": 96, "min_group": 16, "shade_block": 64, "wave_paths": 1 << 22}
+
+    def cost(cfg):
+        return sum(abs(np.log2(cfg[k]) - np.log2(target[k])) for k in target) + 1.0
+
+    best, t, trials = coordinate_descent(cost, CANDIDATES, DEFAULT, passes=3)
+    assert best == target and t == 1.0
+    assert len({tuple(sorted(x["config"].items())) for x in trials}) == len(trials)
+
+
+def test_tuning_file_is_valid():
+    import json
+    from mupsi_b200.api import TUNING_FILE
+    from mupsi_b200.autotune import CANDIDATES
+    if not os.path.exists(TUNING_FILE):
+        pytest.skip("no tuning file committed")
+    t = json.load(open(TUNING_FILE))["tuning"]
+    for k, v in t.items():
+        assert v in CANDIDATES[k]
