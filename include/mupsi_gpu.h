@@ -297,6 +297,49 @@ int mupsi_gpu_scene_profile(mupsi_scene* scene, int32_t enable);
 /* Copy the accumulated statistics; reset != 0 clears them afterwards. */
 int mupsi_gpu_scene_stats(mupsi_scene* scene, mupsi_render_stats* out, int32_t reset);
 
+/* ------------------------------------------------------- surrogate mean --
+ * A learned stand-in for a mesh mean's signed distance (no reference
+ * counterpart; the march uses it only to skip steps far from the surface):
+ *   x = p - center;  u_f = B_f . x, f < 48;  gamma = (sin u, cos u)  (96)
+ *   h1 = relu(W1 gamma + b1);  h_l = relu(W_l h_{l-1} + b_l), l = 2..4  (64 wide)
+ *   mu_hat(p) = y_scale * (w5 . h4 + b5)
+ * B holds angular frequencies (radians per scene unit). gamma, the weights and
+ * h1..h4 are BF16 (round to nearest even); products accumulate in FP32 on the
+ * tcgen05 tensor cores, the output layer on CUDA cores. The parameters are
+ * one FP32 vector of MUPSI_MLP_PARAMS values: W1[64][96], b1[64], W2[64][64],
+ * b2[64], W3, b3, W4, b4, w5[64], b5. Training minimises
+ * L = mean over points of (mu_hat - mu)^2 / y_scale^2 with Adam on FP32 master
+ * weights (BF16 copies feed the tensor cores). */
+#define MUPSI_MLP_PARAMS 18753
+#define MUPSI_MLP_FREQS 48
+typedef struct mupsi_mlp mupsi_mlp;
+typedef struct {
+  float center[3];
+  float y_scale;
+  float fourier[MUPSI_MLP_FREQS * 3]; /* B: row f = (B_f.x, B_f.y, B_f.z) */
+  const float* params;                /* host, MUPSI_MLP_PARAMS initial values */
+} mupsi_mlp_desc;
+int mupsi_gpu_mlp_create(const mupsi_mlp_desc* desc, mupsi_mlp** out);
+int mupsi_gpu_mlp_destroy(mupsi_mlp* mlp);
+/* Current FP32 parameters (host out[MUPSI_MLP_PARAMS]). */
+int mupsi_gpu_mlp_get_params(mupsi_mlp* mlp, float* out);
+/* mu_hat at n points p[n*3]; out[n]. */
+int mupsi_gpu_mlp_infer(mupsi_mlp* mlp, int64_t n, const float* p, float* out, mupsi_mem mem, void* stream);
+/* dL/dparams over the n points (host grad_out[MUPSI_MLP_PARAMS], FP32) and L (host). */
+int mupsi_gpu_mlp_grad(mupsi_mlp* mlp, int64_t n, const float* p, const float* target, float* grad_out,
+                       float* loss_out, mupsi_mem mem, void* stream);
+typedef struct {
+  int32_t steps;       /* Adam steps */
+  int32_t batch;       /* points per step, drawn with replacement (seeded) from the n */
+  float lr, lr_final;  /* learning rate, cosine-decayed from lr to lr_final */
+  float beta1, beta2, eps;
+  uint64_t seed;
+} mupsi_mlp_train_args;
+/* Train on n points p[n*3] with exact targets[n]; loss_out (nullable, host,
+ * `steps` entries) receives each step's minibatch loss. */
+int mupsi_gpu_mlp_train(mupsi_mlp* mlp, int64_t n, const float* p, const float* target,
+                        const mupsi_mlp_train_args* args, float* loss_out, mupsi_mem mem, void* stream);
+
 /* ------------------------------------------------------------------ tuning
  * Launch shapes of the wave kernels, process-wide. No reference counterpart
  * (the reference's OpenMP loop has no launch shapes); the values come from the

@@ -10,8 +10,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmupsi_gpu.so")
-SOURCES = ["core.cu", "render.cu", "host_bvh.cpp"]
-HEADERS = ["core.cuh", "dmath.cuh", "geom.cuh", "gp.cuh", "host.h", "scene.cuh"]
+SOURCES = ["core.cu", "render.cu", "mlp.cu", "host_bvh.cpp"]
+HEADERS = ["core.cuh", "dmath.cuh", "geom.cuh", "gp.cuh", "host.h", "scene.cuh", "tc.cuh"]
 ROOT_HEADER = os.path.join(HERE, "..", "include", "mupsi_gpu.h")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -52,6 +52,12 @@ def _setup(L):
     L.mupsi_gpu_batch_destroy.argtypes = [vp]
     L.mupsi_gpu_batch_render.argtypes = [vp, C.POINTER(_abi.BatchArgs)]
     L.mupsi_gpu_batch_info.argtypes = [vp, C.POINTER(_abi.BatchInfo)]
+    L.mupsi_gpu_mlp_create.argtypes = [vp, C.POINTER(vp)]
+    L.mupsi_gpu_mlp_destroy.argtypes = [vp]
+    L.mupsi_gpu_mlp_get_params.argtypes = [vp, vp]
+    L.mupsi_gpu_mlp_infer.argtypes = [vp, i64, vp, vp, C.c_int, vp]
+    L.mupsi_gpu_mlp_grad.argtypes = [vp, i64, vp, vp, vp, vp, C.c_int, vp]
+    L.mupsi_gpu_mlp_train.argtypes = [vp, i64, vp, vp, vp, vp, C.c_int, vp]
     return L
 
 

@@ -80,6 +80,9 @@ class _Port:
         L.mo_sample_condition.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.c_void_p, _u32, C.c_void_p]
         L.mo_trace.argtypes = [C.c_void_p, C.c_int64, _i32, _i32, _i32, _f32]
         L.mo_trace_work.argtypes = [C.c_void_p, C.c_int64, _i32, _i32, _i32, _i64]
+        L.mo_mlp_forward.argtypes = [_f32, _f32, _f32, C.c_float, C.c_int64, _f32, _f32]
+        L.mo_mlp_grad.argtypes = [_f32, _f32, _f32, C.c_float, C.c_int64, _f32, _f32, _f64,
+                                  C.POINTER(C.c_double)]
 
 
 def kernel_struct(sigma, kernel_radius, aniso, ppc):
@@ -127,6 +130,22 @@ class PortOracle:
         x, y, i = C.c_float(), C.c_float(), C.c_uint32()
         self.L.mo_constant_sampler(seed, C.byref(x), C.byref(y), C.byref(i))
         return x.value, y.value, i.value
+
+    def mlp_forward(self, params, fourier, center, y_scale, p):
+        """Surrogate MLP mu_hat at points p (n, 3) -> (n,) float32."""
+        p = _f(p)
+        out = np.zeros(len(p), np.float32)
+        self.L.mo_mlp_forward(_f(params), _f(fourier), _f(center), float(y_scale), len(p), p, out)
+        return out
+
+    def mlp_grad(self, params, fourier, center, y_scale, p, target):
+        """(dL/dparams (float64), L) for L = mean((mu_hat - target)^2) / y_scale^2."""
+        p = _f(p)
+        g = np.zeros(18753, np.float64)
+        loss = C.c_double()
+        self.L.mo_mlp_grad(_f(params), _f(fourier), _f(center), float(y_scale), len(p), p, _f(target), g,
+                           C.byref(loss))
+        return g, loss.value
 
     def psi(self, kernel, p, seed, cond=None):
         p = _f(p)

@@ -77,6 +77,13 @@ void mo_trace(const mo_scene* s, int64_t n, const int32_t* x, const int32_t* y, 
 void mo_trace_work(const mo_scene* s, int64_t n, const int32_t* x, const int32_t* y, const int32_t* k,
                    int64_t* out);
 
+/* Surrogate-mean MLP (mupsi_mlp_desc in include/mupsi_gpu.h; no reference
+ * counterpart), FP64 with BF16 rounding where the GPU stores BF16 operands. */
+void mo_mlp_forward(const float* params, const float* fourier, const float* center, float y_scale, int64_t n,
+                    const float* p, float* out);
+void mo_mlp_grad(const float* params, const float* fourier, const float* center, float y_scale, int64_t n,
+                 const float* p, const float* target, double* grad, double* loss);
+
 #ifdef __cplusplus
 }
 #endif

@@ -17,8 +17,8 @@ def pytest_configure(config):
 
 def _ensure_oracle():
     lib = os.path.join(ROOT, "oracle", "libmupsi_oracle.so")
-    src = os.path.join(ROOT, "oracle", "mupsi_oracle.c")
-    if not os.path.exists(lib) or os.path.getmtime(lib) < os.path.getmtime(src):
+    srcs = [os.path.join(ROOT, "oracle", f) for f in ("mupsi_oracle.c", "mupsi_mlp_oracle.c", "mupsi_oracle.h")]
+    if not os.path.exists(lib) or os.path.getmtime(lib) < max(os.path.getmtime(f) for f in srcs):
         env = dict(os.environ)
         env.pop("CC", None)
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "libmupsi_oracle.so"], check=True, env=env,
