@@ -291,6 +291,8 @@ typedef struct {
   float iter_march_ms[16];
   uint64_t mean_evals;    /* exact mesh-mean evaluations inside marches */
   uint64_t parity_casts;  /* of which needed the Mesh::inside parity cast */
+  uint64_t surr_requests; /* surrogate predictions the marches asked for */
+  uint64_t surr_accepted; /* of which outside the band (used as the lazy mean's bound) */
 } mupsi_render_stats;
 /* enable != 0 starts counting work and timing kernels on later renders. */
 int mupsi_gpu_scene_profile(mupsi_scene* scene, int32_t enable);
@@ -339,6 +341,20 @@ typedef struct {
  * `steps` entries) receives each step's minibatch loss. */
 int mupsi_gpu_mlp_train(mupsi_mlp* mlp, int64_t n, const float* p, const float* target,
                         const mupsi_mlp_train_args* args, float* loss_out, mupsi_mem mem, void* stream);
+/* Let scene's renders use mlp for medium `medium`'s mesh mean. Where a march
+ * would re-evaluate its lazy exact mean far from the last exact value, it
+ * suspends and asks the network instead (all suspended marches of a bounce
+ * are answered by one tensor-core inference launch, then resume). A
+ * prediction m with |m| > band is taken as
+ *   |m| / scale - margin <= |mu| <= |m| * scale + margin,  sign(mu) = sign(m)
+ * (scale: the Lipschitz safety factor; margin from the held-out error); inside
+ * the band, at every conditioning point and for every hit the exact BVH mean
+ * is used. At most max_requests (1..32) predictions per march. One surrogate
+ * per scene; mlp = NULL detaches. Single-scene renders and traces use it
+ * (batches and the allocation-free trace do not). The scene refers to mlp:
+ * detach or destroy the scene before destroying mlp. */
+int mupsi_gpu_scene_set_surrogate(mupsi_scene* scene, int32_t medium, mupsi_mlp* mlp, float band, float scale,
+                                  float margin, int32_t max_requests);
 
 /* ------------------------------------------------------------------ tuning
  * Launch shapes of the wave kernels, process-wide. No reference counterpart

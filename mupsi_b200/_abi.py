@@ -146,6 +146,8 @@ class RenderStats(C.Structure):
         ("iter_march_ms", C.c_float * 16),
         ("mean_evals", C.c_uint64),
         ("parity_casts", C.c_uint64),
+        ("surr_requests", C.c_uint64),
+        ("surr_accepted", C.c_uint64),
     ]
 
 

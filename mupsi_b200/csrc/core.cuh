@@ -62,4 +62,9 @@ struct Staged {
   }
 };
 
+// Surrogate inference (mlp.cu): mu_hat of the points P + i * pstride, i < n,
+// or i < *n_dev when n_dev is set (a count written on the device, at most n).
+int mlp_infer_device(mupsi_mlp* m, int64_t n, const float* p, int pstride, const uint32_t* n_dev, float* out,
+                     cudaStream_t st);
+
 }  // namespace mupsi

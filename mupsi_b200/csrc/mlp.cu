@@ -348,11 +348,16 @@ __global__ void __launch_bounds__(128, 1) k_mlp_grad(const float* __restrict__ p
 }
 
 // ---------------------------------------------------------------- inference
+// Points p_i at P + i * pstride; n points, or *n_dev points when n_dev is set
+// (a count another kernel wrote, at most n).
 __global__ void __launch_bounds__(128) k_mlp_infer(const float* __restrict__ params, MlpConst mc,
-                                                   const float* __restrict__ P, int64_t n, float* __restrict__ out,
+                                                   const float* __restrict__ P, int pstride, int64_t n,
+                                                   const uint32_t* __restrict__ n_dev, float* __restrict__ out,
                                                    int* err) {
   extern __shared__ __align__(1024) unsigned char sm[];
   const int tid = threadIdx.x, warp = tid >> 5;
+  if (n_dev) n = min(n, (int64_t)*n_dev);
+  if ((int64_t)blockIdx.x * kRows >= n) return;  // no tile for this CTA
   float* bias = reinterpret_cast<float*>(sm + kIF);
   float* w5f = bias + 256;
   float* misc = w5f + 64;
@@ -380,9 +385,9 @@ __global__ void __launch_bounds__(128) k_mlp_infer(const float* __restrict__ par
     const bool valid = row < n;
     float x0 = 0.0f, x1 = 0.0f, x2 = 0.0f;
     if (valid) {
-      x0 = P[3 * row] - mc.c[0];
-      x1 = P[3 * row + 1] - mc.c[1];
-      x2 = P[3 * row + 2] - mc.c[2];
+      x0 = P[pstride * row] - mc.c[0];
+      x1 = P[pstride * row + 1] - mc.c[1];
+      x2 = P[pstride * row + 2] - mc.c[2];
     }
     store_features(sm, kIX, tid, kFeat, mc, x0, x1, x2);
     float y = 0.0f;
@@ -531,13 +536,13 @@ int mlp_launch_grad(mupsi_mlp* m, int64_t n, const float* p, const float* t, flo
 
 }  // namespace
 
-// mu_hat at n device points (device out), on stream st; used by the march.
-int mlp_infer_device(mupsi_mlp* m, int64_t n, const float* p, float* out, cudaStream_t st) {
+int mlp_infer_device(mupsi_mlp* m, int64_t n, const float* p, int pstride, const uint32_t* n_dev, float* out,
+                     cudaStream_t st) {
   if (n <= 0) return MUPSI_OK;
   if (int e = mlp_kernel_attrs()) return e;
   const int64_t tiles = (n + kRows - 1) / kRows;
   const int grid = (int)std::min<int64_t>(tiles, (int64_t)num_sms() * 3);
-  k_mlp_infer<<<grid, 128, kInferSmem, st>>>(m->params, m->mc, p, n, out, m->err);
+  k_mlp_infer<<<grid, 128, kInferSmem, st>>>(m->params, m->mc, p, pstride, n, n_dev, out, m->err);
   count_launch();
   MUPSI_CUDA(cudaGetLastError());
   return MUPSI_OK;
@@ -597,7 +602,7 @@ int mupsi_gpu_mlp_infer(mupsi_mlp* m, int64_t n, const float* p, float* out, mup
   Staged<float> dp(st), dout(st);
   MUPSI_CUDA(dp.in(p, n * 3, mem));
   MUPSI_CUDA(dout.out(out, n, mem));
-  if (int e = mlp_infer_device(m, n, dp.ptr, dout.ptr, st)) return e;
+  if (int e = mlp_infer_device(m, n, dp.ptr, 3, nullptr, dout.ptr, st)) return e;
   MUPSI_CUDA(dout.finish());
   return mlp_check_err(m, st);
 }

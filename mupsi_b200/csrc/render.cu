@@ -50,6 +50,16 @@ struct Paths {
   uint32_t* counts;     // per iteration: [it*2+0] medium count, [it*2+1] live count
   uint32_t* cursors;    // per iteration: march work cursor
   int64_t cap;
+  // surrogate rounds (rounds > 1): a march suspended for a prediction keeps its
+  // state here, its request goes to req[round & 1] and the network's answer to
+  // pred[round & 1]; the next round resumes it
+  int rounds;
+  float4* ms0;          // t, step index (int bits), f at the origin, flags | requests << 8
+  float4* ms1;          // mu_j, mu_hi, t_j, -
+  float4* req[2];       // point xyz, path index (uint bits)
+  float* pred[2];
+  uint32_t* rcounts;    // [it * rounds + r]: requests made in round r
+  uint32_t* rcursors;   // [it * rounds + r]: work cursor of round r >= 1
 };
 
 MD uint64_t ld_rng(const uint2 v) { return ((uint64_t)v.y << 32) | v.x; }
@@ -140,6 +150,11 @@ MD int find_chunk(const WaveChunk* chunks, int nchunks, int64_t i, F start) {
 __global__ void k_wave_begin(Paths P, int iters, int* wave_idx) {
   for (int i = threadIdx.x; i < 2 * (iters + 1); i += blockDim.x) P.counts[i] = 0;
   for (int i = threadIdx.x; i < iters + 1; i += blockDim.x) P.cursors[i] = 0;
+  if (P.rounds > 1)
+    for (int i = threadIdx.x; i < iters * P.rounds; i += blockDim.x) {
+      P.rcounts[i] = 0;
+      P.rcursors[i] = 0;
+    }
   if (wave_idx && threadIdx.x == 0) *wave_idx += 1;
 }
 
@@ -194,10 +209,17 @@ struct WaveCfg {
 // fills the resident threads, larger (up to 32) as the queue shrinks, so the
 // late bounces' few long marches finish up to 8x sooner than on one lane.
 template <int MK>
-__global__ void __launch_bounds__(128) k_march(const DScene* const* __restrict__ scenes, Paths P, int it, WaveCfg cfg) {
-  const uint32_t n = P.counts[2 * it];
+__global__ void __launch_bounds__(128) k_march(const DScene* const* __restrict__ scenes, Paths P, int it, int round,
+                                               WaveCfg cfg) {
+  // round 0 marches the iteration's medium queue; round r >= 1 resumes the
+  // marches suspended in round r - 1 with their surrogate predictions
+  // (a scene with sphere means only has no surrogate: one round, no resumes)
+  const bool resume = MK != MEAN_SPHERE_ONLY && round > 0;
+  const int R = P.rounds;
+  const uint32_t n = resume ? P.rcounts[it * R + round - 1] : P.counts[2 * it];
   const uint32_t* q = P.q[it & 1];
-  uint32_t* cursor = P.cursors + it;
+  uint32_t* cursor = resume ? P.rcursors + it * R + round : P.cursors + it;
+  const bool can_suspend = round + 1 < R;
   const unsigned lane = threadIdx.x & 31;
   const uint64_t resident = (uint64_t)gridDim.x * blockDim.x;
   Group grp;
@@ -211,7 +233,7 @@ __global__ void __launch_bounds__(128) k_march(const DScene* const* __restrict__
   uint32_t idx = 0;
   bool active = false;
   bool ovf = false;
-  unsigned long long steps = 0, psis = 0, marches = 0, imps = 0, mus = 0, pars = 0;
+  unsigned long long steps = 0, psis = 0, marches = 0, imps = 0, mus = 0, pars = 0, reqs = 0, accs = 0;
   while (true) {
     // refill idle groups from the queue (warp-aggregated over group leaders)
     unsigned need = __ballot_sync(0xffffffffu, !active && grp.sub == 0);
@@ -224,15 +246,33 @@ __global__ void __launch_bounds__(128) k_march(const DScene* const* __restrict__
       j = __shfl_sync(0xffffffffu, j, (int)gbase);
       if (!active) {
         if (j < n) {
-          idx = q[j];
+          idx = resume ? __float_as_uint(P.req[(round - 1) & 1][j].w) : q[j];
           float4 o = P.o[idx], d = P.d[idx];
           int4 meta = P.meta[idx];
           int med = __float_as_int(d.w);
           S = scenes[meta_inst(meta.w)];
           march_begin(S, m, mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), o.w, 3.402823466e+38f, med,
                       medium_seed(S, meta.x, meta.y, meta.z, meta_bounce(meta.w)), load_cond(P, idx));
+          m.may_request = MK != MEAN_SPHERE_ONLY && can_suspend && m.lazy && S->media[med].surr;
+          if (MK != MEAN_SPHERE_ONLY && resume) {
+            const float4 a = P.ms0[idx], b = P.ms1[idx];
+            const int fl = __float_as_int(a.w);
+            m.t = a.x;
+            m.k = __float_as_int(a.y);
+            m.fprev = a.z;
+            m.fprev_pos = (fl & 1) != 0;
+            m.fprev_big = (fl & 2) != 0;
+            m.n_req = fl >> 8;
+            m.init = false;
+            m.mu_j = b.x;
+            m.mu_hi = b.y;
+            m.t_j = b.z;
+            const bool used = march_apply_prediction(S->media[med], m, P.pred[(round - 1) & 1][j]);
+            if (grp.sub == 0 && used) accs++;
+          } else if (grp.sub == 0) {
+            marches++;
+          }
           active = true;
-          if (grp.sub == 0) marches++;
         }
       }
     }
@@ -240,7 +280,22 @@ __global__ void __launch_bounds__(128) k_march(const DScene* const* __restrict__
     if (active) {
       v3 p;
       if (march_cheap<MK>(S, m, p, ovf)) march_psi<MK, true>(S, m, p, grp, ovf);
-      if (m.status != 0) {
+      if (MK != MEAN_SPHERE_ONLY && m.status == 3) {  // suspended: save the march, request a prediction at p
+        if (grp.sub == 0) {
+          const int fl = (m.fprev_pos ? 1 : 0) | (m.fprev_big ? 2 : 0) | (m.n_req << 8);
+          P.ms0[idx] = make_float4(m.t, __int_as_float(m.k), m.fprev, __int_as_float(fl));
+          P.ms1[idx] = make_float4(m.mu_j, m.mu_hi, m.t_j, 0.0f);
+          const uint32_t slot = atomicAdd(&P.rcounts[it * R + round], 1u);
+          P.req[round & 1][slot] = make_float4(p.x, p.y, p.z, __uint_as_float(idx));
+          reqs++;
+          steps += m.n_steps;
+          psis += m.n_psi;
+          imps += (unsigned long long)m.n_psi * 27ull * (unsigned long long)S->media[m.medium].k.ppc;
+          mus += m.n_mu;
+          pars += m.n_par;
+        }
+        active = false;
+      } else if (m.status != 0) {
         mupsi_medium_sample r;
         march_result<MK, true>(S, m, r, ovf, grp);
         if (grp.sub == 0) {
@@ -265,6 +320,8 @@ __global__ void __launch_bounds__(128) k_march(const DScene* const* __restrict__
       imps += __shfl_down_sync(0xffffffffu, imps, o);
       mus += __shfl_down_sync(0xffffffffu, mus, o);
       pars += __shfl_down_sync(0xffffffffu, pars, o);
+      reqs += __shfl_down_sync(0xffffffffu, reqs, o);
+      accs += __shfl_down_sync(0xffffffffu, accs, o);
     }
     if (lane == 0) {
       atomicAdd(&cfg.counters[0], steps);
@@ -273,6 +330,8 @@ __global__ void __launch_bounds__(128) k_march(const DScene* const* __restrict__
       atomicAdd(&cfg.counters[3], imps);
       atomicAdd(&cfg.counters[4], mus);
       atomicAdd(&cfg.counters[5], pars);
+      atomicAdd(&cfg.counters[6], reqs);
+      atomicAdd(&cfg.counters[7], accs);
     }
   }
 }
@@ -552,6 +611,7 @@ struct PathBuf {
   size_t bytes = 0;
   int64_t cap = 0;
   int iters = 0;
+  int rounds = 1;  // surrogate rounds the round buffers were sized for
 };
 
 struct mupsi_scene {
@@ -566,6 +626,8 @@ struct mupsi_scene {
   int passes_done = 0;
   int next_pass = -1;  // pass after the last one accumulated
   PathBuf pb;  // wave buffers (grow-only)
+  mupsi_mlp* surr_mlp = nullptr;  // surrogate of a mesh mean (not owned)
+  int surr_rounds = 1;            // march rounds per bounce iteration with it: predictions + 1
   int* err = nullptr;
   unsigned long long* counters = nullptr;
   // profiling: per-launch event pairs, recorded while `profile` is set
@@ -796,14 +858,15 @@ int build_scene(const mupsi_scene_desc* desc, mupsi_scene* s) {
 // PathTracer::trace's do-while runs at least one bounce iteration
 int wave_iters(const mupsi_scene* s) { return std::max(1, s->max_bounce); }
 
-int ensure_paths(PathBuf& b, int64_t cap, int iters) {
-  if (cap <= b.cap && iters <= b.iters) return MUPSI_OK;
+int ensure_paths(PathBuf& b, int64_t cap, int iters, int rounds) {
+  if (cap <= b.cap && iters <= b.iters && rounds <= b.rounds && b.mem) return MUPSI_OK;
   if (b.mem) {
     pool_give(b.mem, b.bytes);
     b.mem = nullptr;
   }
   cap = std::max(cap, b.cap);
   iters = std::max(iters, b.iters);
+  rounds = std::max(rounds, b.rounds);
   size_t bytes = 0;
   auto take = [&](size_t sz) {
     size_t off = bytes;
@@ -815,6 +878,10 @@ int ensure_paths(PathBuf& b, int64_t cap, int iters) {
          o_ha = take(cap * 16), o_hb = take(cap * 16), o_rad = take(cap * 12), o_q0 = take(cap * 4),
          o_q1 = take(cap * 4), o_q2 = take(cap * 4), o_q3 = take(cap * 4), o_c = take((size_t)(iters + 1) * 8),
          o_cur = take((size_t)(iters + 1) * 4);
+  const bool sr = rounds > 1;
+  size_t o_s0 = sr ? take(cap * 16) : 0, o_s1 = sr ? take(cap * 16) : 0, o_rq0 = sr ? take(cap * 16) : 0,
+         o_rq1 = sr ? take(cap * 16) : 0, o_pr0 = sr ? take(cap * 4) : 0, o_pr1 = sr ? take(cap * 4) : 0,
+         o_rc = sr ? take((size_t)iters * rounds * 4) : 0, o_rr = sr ? take((size_t)iters * rounds * 4) : 0;
   size_t got = 0;
   char* base = static_cast<char*>(pool_take(bytes, &got));
   if (!base) {
@@ -842,11 +909,23 @@ int ensure_paths(PathBuf& b, int64_t cap, int iters) {
   P.counts = (uint32_t*)(base + o_c);
   P.cursors = (uint32_t*)(base + o_cur);
   P.cap = cap;
+  P.rounds = 1;
+  P.ms0 = sr ? (float4*)(base + o_s0) : nullptr;
+  P.ms1 = sr ? (float4*)(base + o_s1) : nullptr;
+  P.req[0] = sr ? (float4*)(base + o_rq0) : nullptr;
+  P.req[1] = sr ? (float4*)(base + o_rq1) : nullptr;
+  P.pred[0] = sr ? (float*)(base + o_pr0) : nullptr;
+  P.pred[1] = sr ? (float*)(base + o_pr1) : nullptr;
+  P.rcounts = sr ? (uint32_t*)(base + o_rc) : nullptr;
+  P.rcursors = sr ? (uint32_t*)(base + o_rr) : nullptr;
   b.cap = cap;
   b.iters = iters;
+  b.rounds = rounds;
   return MUPSI_OK;
 }
-int ensure_paths(mupsi_scene* s, int64_t cap) { return ensure_paths(s->pb, cap, wave_iters(s) + 1); }
+int ensure_paths(mupsi_scene* s, int64_t cap) {
+  return ensure_paths(s->pb, cap, wave_iters(s) + 1, s->surr_mlp ? s->surr_rounds : 1);
+}
 
 // Launch shapes of the wave kernels (mupsi_gpu_set_tuning; chosen by the
 // project's autotuner, mupsi_b200/autotune.py).
@@ -854,7 +933,7 @@ mupsi_tuning g_tuning = {128, 4, 128, 0};
 
 // Persistent march grid: resident blocks per SM x SMs.
 struct MarchLaunch {
-  void (*fn)(const DScene* const*, Paths, int, WaveCfg);
+  void (*fn)(const DScene* const*, Paths, int, int, WaveCfg);
   int blocks, block;
 };
 MarchLaunch march_launch(bool sphere_only) {
@@ -882,7 +961,20 @@ struct WaveExec {
   int iters;                    // bounce iterations: max over the wave's scenes of max(1, max_bounce)
   bool sphere_only;
   WaveCfg cfg;
+  mupsi_mlp* mlp = nullptr;     // surrogate answering suspended marches (rounds > 1)
 };
+
+// The march of bounce iteration `it`: round 0, then, with a surrogate, the
+// inference of the round's requests and the round that resumes them.
+void launch_march_rounds(const WaveExec& w, const MarchLaunch& ml, int it, cudaStream_t st) {
+  const int R = w.P.rounds;
+  for (int r = 0; r < R; ++r) {
+    ml.fn<<<ml.blocks, ml.block, 0, st>>>(w.scenes, w.P, it, r, w.cfg);
+    if (r + 1 < R)
+      mlp_infer_device(w.mlp, w.P.cap, reinterpret_cast<const float*>(w.P.req[r & 1]), 4, w.P.rcounts + it * R + r,
+                       w.P.pred[r & 1], st);
+  }
+}
 
 // Launch one wave: clear the queue counters, generate the paths, then `iters`
 // bounce iterations of march + shade. Grids do not depend on the wave's size
@@ -901,19 +993,19 @@ void launch_wave(const WaveExec& w, const WaveSrc& src, cudaStream_t st, mupsi_s
     if (prof && prof->profile) {
       cudaEvent_t a = prof->next_event(), b = prof->next_event(), c = prof->next_event();
       cudaEventRecord(a, st);
-      ml.fn<<<ml.blocks, ml.block, 0, st>>>(w.scenes, w.P, it, w.cfg);
+      launch_march_rounds(w, ml, it, st);
       cudaEventRecord(b, st);
       k_shade<<<sb, sblock, 0, st>>>(w.scenes, w.P, it, w.cfg);
       cudaEventRecord(c, st);
       prof->ev_march.push_back({a, b});
       prof->ev_shade.push_back({b, c});
     } else {
-      ml.fn<<<ml.blocks, ml.block, 0, st>>>(w.scenes, w.P, it, w.cfg);
+      launch_march_rounds(w, ml, it, st);
       k_shade<<<sb, sblock, 0, st>>>(w.scenes, w.P, it, w.cfg);
     }
   }
 }
-int wave_launches(int iters) { return 2 + 2 * iters; }
+int wave_launches(int iters, int rounds = 1) { return 2 + (2 * rounds) * iters; }
 
 WaveExec scene_exec(mupsi_scene* s) {
   WaveExec w;
@@ -924,6 +1016,8 @@ WaveExec scene_exec(mupsi_scene* s) {
   w.cfg.min_group = g_tuning.min_group;
   w.cfg.err = s->err;
   w.cfg.counters = s->profile ? s->counters : nullptr;
+  w.mlp = s->surr_mlp;
+  w.P.rounds = s->surr_mlp ? s->surr_rounds : 1;  // ensure_paths sized the round buffers
   return w;
 }
 
@@ -945,7 +1039,7 @@ int run_wave(mupsi_scene* s, int64_t n, int pass0, const int32_t* xs, const int3
     src.nchunks = 1;
   }
   launch_wave(w, src, st, s);
-  count_launch(wave_launches(w.iters));
+  count_launch(wave_launches(w.iters, w.P.rounds));
   MUPSI_CUDA(cudaGetLastError());
   return MUPSI_OK;
 }
@@ -1059,6 +1153,11 @@ Paths noalloc_paths(void* base_ptr) {
   P.counts = (uint32_t*)take((size_t)(kNoAllocMaxIters + 1) * 8);
   P.cursors = (uint32_t*)take((size_t)(kNoAllocMaxIters + 1) * 4);
   P.cap = cap;
+  P.rounds = 1;  // no surrogate rounds in the allocation-free path
+  P.ms0 = P.ms1 = nullptr;
+  P.req[0] = P.req[1] = nullptr;
+  P.pred[0] = P.pred[1] = nullptr;
+  P.rcounts = P.rcursors = nullptr;
   return P;
 }
 
@@ -1445,6 +1544,8 @@ int mupsi_gpu_scene_stats(mupsi_scene* scene, mupsi_render_stats* out, int32_t r
   out->impulse_evals = c[3];
   out->mean_evals = c[4];
   out->parity_casts = c[5];
+  out->surr_requests = c[6];
+  out->surr_accepted = c[7];
   out->march_ms = scene->march_ms;
   out->shade_ms = scene->shade_ms;
   out->march_launches = scene->march_launches;
@@ -1590,7 +1691,7 @@ int mupsi_gpu_batch_render(mupsi_batch* b, const mupsi_batch_args* a) {
   bool moved = false;
   if (!waves.empty()) {
     if (max_n > b->pb.cap || max_it + 1 > b->pb.iters) moved = true;
-    if (int e = ensure_paths(b->pb, max_n, max_it + 1)) return e;
+    if (int e = ensure_paths(b->pb, max_n, max_it + 1, 1)) return e;
     if (int e = grow_device(b->d_chunks, b->chunk_cap, chunks.size(), moved)) return e;
     if (int e = grow_device(b->d_waves, b->wave_cap, waves.size(), moved)) return e;
   }
@@ -1673,6 +1774,41 @@ int mupsi_gpu_batch_render(mupsi_batch* b, const mupsi_batch_args* a) {
   }
   int e = check_batch_err(b);
   return rc ? rc : e;
+}
+
+int mupsi_gpu_scene_set_surrogate(mupsi_scene* scene, int32_t medium, mupsi_mlp* mlp, float band, float scale,
+                                  float margin, int32_t max_requests) {
+  clear_error();
+  if (!scene) return fail(MUPSI_ERR_INVALID, "null scene");
+  if (medium < 0 || medium >= scene->h.nmed) return fail(MUPSI_ERR_INVALID, "medium out of range");
+  DMedium& md = scene->h.media[medium];
+  if (mlp) {
+    if (md.mean_type != MUPSI_MEAN_MESH) return fail(MUPSI_ERR_INVALID, "the surrogate stands in for a mesh mean");
+    if (!(band >= 0.0f) || !(scale >= 1.0f) || !(margin >= 0.0f) || !std::isfinite(band) || !std::isfinite(scale) ||
+        !std::isfinite(margin))
+      return fail(MUPSI_ERR_INVALID, "need band >= 0, scale >= 1, margin >= 0");
+    if (max_requests < 1 || max_requests > 32) return fail(MUPSI_ERR_INVALID, "max_requests must be in [1, 32]");
+    for (int i = 0; i < scene->h.nmed; ++i)
+      if (i != medium) scene->h.media[i].surr = 0;  // one surrogate per scene
+    md.surr = 1;
+    md.surr_max = max_requests;
+    md.surr_band = band;
+    md.surr_scale = scale;
+    md.surr_add = margin;
+    scene->surr_mlp = mlp;
+    scene->surr_rounds = max_requests + 1;
+  } else {
+    md.surr = 0;
+    bool any = false;
+    for (int i = 0; i < scene->h.nmed; ++i) any = any || scene->h.media[i].surr;
+    if (!any) {
+      scene->surr_mlp = nullptr;
+      scene->surr_rounds = 1;
+    }
+  }
+  MUPSI_CUDA(cudaDeviceSynchronize());
+  MUPSI_CUDA(cudaMemcpy(scene->d, &scene->h, sizeof(DScene), cudaMemcpyHostToDevice));
+  return MUPSI_OK;
 }
 
 }  // extern "C"

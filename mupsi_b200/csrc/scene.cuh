@@ -26,6 +26,12 @@ struct DMedium {
   v3 bs_c;     // mesh mean: bounding sphere of the world-space mesh (with slack)
   float bs_r;
   KParams k;
+  // learned surrogate of a mesh mean (set by mupsi_gpu_scene_set_surrogate):
+  // a prediction m with |m| > surr_band bounds the mean by
+  // |m| / surr_scale - surr_add <= |mu| <= |m| * surr_scale + surr_add, same sign
+  int surr;
+  int surr_max;  // predictions per march
+  float surr_band, surr_scale, surr_add;
 };
 
 // error bits raised by device code
@@ -132,7 +138,7 @@ struct March {
   bool fprev_pos;
   bool fprev_big; // |f_origin| > B: its value never decides the 1e-6 test
   float fprev;
-  int status;     // 0 running, 1 hit, 2 exited
+  int status;     // 0 running, 1 hit, 2 exited, 3 suspended for a surrogate prediction
   int medium;
   uint32_t n_steps, n_psi;  // work counters: steps visited, psi evaluations
   uint32_t n_mu, n_par;     // mesh means: exact evaluations, parity casts among them
@@ -141,6 +147,12 @@ struct March {
   // that bound cannot decide the sign of f.
   bool lazy;
   float mu_j, t_j;
+  float mu_hi;      // upper bound on |mu| at t_j (|mu_j| when mu_j is exact)
+  // surrogate predictions: allowed (this launch can suspend the march), made
+  // so far, and the step at which the last one arrived (no second request there)
+  bool may_request;
+  int n_req;
+  float t_resumed;
   // pending step between the two phases
   bool pend_exact;  // pend_mu holds the exact mean at the pending point
   float pend_mu, pend_lb, pend_sgn;
@@ -174,6 +186,10 @@ MD void march_begin(const DScene* S, March& m, v3 o, v3 d, float near_t, float f
   m.lazy = S->media[medium].mean_type == MUPSI_MEAN_MESH;
   m.mu_j = 0.0f;
   m.t_j = 0.0f;
+  m.mu_hi = 0.0f;
+  m.may_request = false;
+  m.n_req = 0;
+  m.t_resumed = -1.0f;
   m.pend_exact = false;
   m.pend_mu = 0.0f;
   m.pend_lb = 0.0f;
@@ -205,7 +221,7 @@ MD float mean_exact(const DScene* S, March& m, v3 p, float t, bool& ovf) {
   }
   float sign = m.mu_j > 0.0f ? 1.0f : -1.0f;
   if (mu_lower(m, t) <= 0.0f && (segment_crossings(mesh, m.o, m.d, m.t_j, t, ovf) & 1)) sign = -sign;
-  float ub = fabsf(m.mu_j) + fabsf(t - m.t_j) * 1.0001f + 1e-2f;
+  float ub = m.mu_hi + fabsf(t - m.t_j) * 1.0001f + 1e-2f;
   uint32_t tri;
   v3 q = mk3(0, 0, 0);
   bool found = false;
@@ -266,6 +282,7 @@ MD bool march_cheap(const DScene* S, March& m, v3& p, bool& ovf) {
     p = m.o;
     float mu = mean_value<MK>(S, md, p, ovf);
     m.mu_j = mu;
+    m.mu_hi = fabsf(mu);
     m.t_j = 0.0f;  // p(0) = o exactly
     if (fabsf(mu) * 0.999999f > noise_bound_at(md.k, m.c, p)) {
       m.fprev_pos = mu > 0.0f;
@@ -291,6 +308,7 @@ MD bool march_cheap(const DScene* S, March& m, v3& p, bool& ovf) {
     if (exact) {
       mu = mean_value<MK>(S, md, p, ovf);
       m.mu_j = mu;
+      m.mu_hi = fabsf(mu);
       m.t_j = m.t;
       lb = fabsf(mu);
       sgn = mu;
@@ -307,8 +325,15 @@ MD bool march_cheap(const DScene* S, March& m, v3& p, bool& ovf) {
       // a stale bound far from the last exact value: re-evaluate mu (BVH) so
       // a long jump can follow; near the surface the psi comparison decides
       if (lb * 0.999999f <= m.B && m.t - m.t_j >= fmaxf(16.0f, fabsf(m.mu_j))) {
+        if (m.may_request && m.t != m.t_resumed && m.n_req < md.surr_max) {
+          // ask the surrogate first: the march is suspended here and resumes
+          // at this step with the prediction (march_apply_prediction)
+          m.status = 3;
+          return false;
+        }
         mu = mean_exact<MK>(S, m, p, m.t, ovf);
         m.mu_j = mu;
+        m.mu_hi = fabsf(mu);
         m.t_j = m.t;
         lb = fabsf(mu);
         sgn = mu;
@@ -345,6 +370,25 @@ MD bool march_cheap(const DScene* S, March& m, v3& p, bool& ovf) {
   return false;
 }
 
+// A surrogate prediction `pred` for the step where the march was suspended:
+// outside the band it becomes the anchor of the lazy mean (a lower bound on
+// |mu| with the prediction's sign, and an upper bound for the next exact
+// query); inside the band, or too weak to bound anything, the march takes the
+// exact mean at this step instead (t_resumed blocks a second request).
+MD bool march_apply_prediction(const DMedium& md, March& m, float pred) {
+  m.n_req++;
+  m.t_resumed = m.t;
+  const float a = fabsf(pred);
+  const float lo = a / md.surr_scale - md.surr_add;
+  if (a > md.surr_band && lo > 0.0f && isfinite(pred)) {
+    m.mu_j = pred > 0.0f ? lo : -lo;
+    m.mu_hi = a * md.surr_scale + md.surr_add;
+    m.t_j = m.t;
+    return true;
+  }
+  return false;
+}
+
 // Phase B: f at the pending point (value only); decides hit or next step. The
 // psi sum is shared by the lanes of group g (all of which hold the same march).
 // WIDE: the group has G >= 4 lanes.
@@ -372,6 +416,7 @@ MD void march_psi(const DScene* S, March& m, v3 p, const Group& g, bool& ovf) {
     }
     float mu = mean_exact<MK>(S, m, p, m.t, ovf);
     m.mu_j = mu;
+    m.mu_hi = fabsf(mu);
     m.t_j = m.t;
     f = mu + q;
     if (m.c.active) f += c;

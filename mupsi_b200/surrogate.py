@@ -179,3 +179,24 @@ def training_points(vertices, faces, n, box_lo, box_hi, seed=0, normal_sigma=2.0
     pts += nrm * rng.normal(0.0, normal_sigma, n_surf)[:, None]
     out = np.concatenate([box, pts]).astype(np.float32)
     return out[rng.permutation(n)]
+
+
+def attach(gpu_scene, medium, surrogate, band=3.0, scale=1.5, margin=1.0, max_requests=8):
+    """Let gpu_scene's marches use `surrogate` for medium `medium` (None
+    detaches): a prediction m with |m| > band gives |m|/scale - margin <= |mu|."""
+    check(load().mupsi_gpu_scene_set_surrogate(gpu_scene.h, medium, surrogate.h if surrogate else None, band, scale,
+                                               margin, max_requests))
+    gpu_scene._surrogate = surrogate
+
+
+def bound_margin(pred, exact, band=3.0, scale=1.5, safety=2.0):
+    """Margin for attach(): `safety` x the largest violation of |mu| >= |m|/scale
+    over held-out points with |m| > band (or a wrong sign there), at least 0.5."""
+    pred = np.asarray(pred, np.float64)
+    exact = np.asarray(exact, np.float64)
+    far = np.abs(pred) > band
+    if not far.any():
+        return 0.5
+    viol = np.abs(pred[far]) / scale - np.abs(exact[far])
+    viol = np.where(np.sign(pred[far]) != np.sign(exact[far]), np.abs(pred[far]) / scale, viol)
+    return float(max(0.5, safety * max(0.0, viol.max())))
