@@ -42,7 +42,7 @@ def _args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=8.0, help="CPU work per reference/baseline step")
-    ap.add_argument("--extras", type=int, default=1, help="also time configurations 1 and 2 (single GPU)")
+    ap.add_argument("--extras", type=int, default=1, help="also time configurations 1-4 (single GPU)")
     return ap.parse_args()
 
 
@@ -396,6 +396,91 @@ def run_extras(args):
                            "samples_per_s": 512 * 512 * 64 / (ms / 1000.0)}
     gs.close()
     out["config4_batch"] = run_batch()
+    out["config3_surrogate"] = run_surrogate()
+    return out
+
+
+def run_surrogate(spp=2, train_steps=6000):
+    """Configuration 3: the displaced icosphere at level 8 (1,310,720 triangles) as
+    the mesh mean, 1024x1024, renewal_plus. The surrogate MLP is trained on the
+    GPU on 2^22 points (half uniform in the medium's bounding box, half surface
+    samples moved by N(0, 2^2) along the normal) labelled with the GPU's exact
+    BVH mean, checked on 2^18 held-out points, then attached (band 3, scale 1.5,
+    margin from the held-out bound violations x 2). Both forms render the same
+    `spp` passes (a bounded sample of the 64-spp workload), device-timed."""
+    import torch
+    from mupsi_b200 import scene as S
+    from mupsi_b200 import surrogate as SG
+    from mupsi_b200.api import GpuRenderer, GpuScene
+
+    res = 1024
+    center = np.array([0.0, 0.0, -300.0], np.float32)
+    sc = S.config_mesh_scene(level=8, width=res, height=res, spp=64)
+    gs = GpuScene(sc)
+    mesh = sc.meshes[0]
+    lo, hi = center - 100.0, center + 100.0
+    t0 = time.perf_counter()
+    P = SG.training_points(mesh.vertices, mesh.faces, 1 << 22, lo, hi, seed=0)
+    Pd = torch.tensor(P, device="cuda")
+    Td = gs.mean(0, Pd)[:, 0].contiguous()
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t0
+    Q = SG.training_points(mesh.vertices, mesh.faces, 1 << 18, lo, hi, seed=1)
+    TQ = gs.mean(0, Q)[:, 0].copy()
+    sm = SG.SurrogateMean(center, 32.0, seed=0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    losses = sm.train(Pd, Td, steps=train_steps, batch=16384, lr=3e-3, lr_final=1e-5, seed=0)
+    e1.record()
+    e1.synchronize()
+    train_ms = e0.elapsed_time(e1)
+    pred = sm.infer(Q)
+    err = np.abs(pred - TQ)
+    far = np.abs(pred) > 3.0
+    margin = SG.bound_margin(pred, TQ, band=3.0, scale=1.5, safety=2.0)
+
+    def render(g):
+        r = GpuRenderer()
+        r.prepare_render(g)
+        fb = torch.empty((res, res, 3), device="cuda")
+        r.start_render_progressive(1, out=fb)  # warm-up
+        g.profile(True)
+        g.stats(reset=True)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        r.start_render_progressive(spp, out=fb)
+        b.record()
+        b.synchronize()
+        st = g.stats(reset=True)
+        g.profile(False)
+        return fb.cpu().numpy(), a.elapsed_time(b), st
+
+    img_e, ms_e, st_e = render(gs)
+    gs2 = GpuScene(sc)
+    SG.attach(gs2, 0, sm, band=3.0, scale=1.5, margin=margin, max_requests=8)
+    img_s, ms_s, st_s = render(gs2)
+    n = res * res * spp
+    rmse = float(np.sqrt(np.mean((img_s - img_e) ** 2)))
+    out = {"workload": f"displaced icosphere level 8 (1,310,720 triangles) mesh mean, 1024x1024, {spp} of 64 spp, "
+                       "renewal_plus, length_scale 2, floor quad",
+           "training": {"points": 1 << 22, "steps": train_steps, "batch": 16384, "train_ms": round(train_ms, 1),
+                        "data_s": round(t_data, 2), "final_loss": float(losses[-50:].mean())},
+           "held_out": {"points": 1 << 18, "mean_abs_err": float(err.mean()), "p99_abs_err": float(np.quantile(err, .99)),
+                        "max_abs_err": float(err.max()), "max_abs_err_outside_band": float(err[far].max()),
+                        "bound": f"|mu| >= |m|/1.5 - {margin:.3f} outside |m| > 3"},
+           "exact": {"ms": round(ms_e, 1), "samples_per_s": n / (ms_e / 1e3),
+                     "exact_mean_evals_per_sample": st_e["mean_evals"] / n},
+           "surrogate": {"ms": round(ms_s, 1), "samples_per_s": n / (ms_s / 1e3),
+                         "exact_mean_evals_per_sample": st_s["mean_evals"] / n,
+                         "predictions_per_sample": st_s["surr_requests"] / n,
+                         "accepted_per_sample": st_s["surr_accepted"] / n},
+           "speedup": ms_e / ms_s,
+           "image_rmse_vs_exact": rmse, "image_rmse_rel": rmse / max(1e-12, float(np.mean(img_e))),
+           "identical_pixels": float(np.all(img_s.view(np.uint32) == img_e.view(np.uint32), axis=2).mean())}
+    gs2.close()
+    sm.close()
+    gs.close()
     return out
 
 

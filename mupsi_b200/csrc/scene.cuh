@@ -280,6 +280,24 @@ MD bool march_cheap(const DScene* S, March& m, v3& p, bool& ovf) {
   const DMedium& md = S->media[m.medium];
   if (m.init) {
     p = m.o;
+    if (MK != MEAN_SPHERE_ONLY && m.lazy) {
+      // an origin outside the mesh's bounding sphere: mu > 0 (the parity test
+      // reports outside) and |p - c| - r <= mu <= |p - c| + r; when that lower
+      // bound exceeds the noise bound, sign(f) at the origin is settled
+      // without a BVH query
+      const float dc = norm3(p - md.bs_c);
+      const float lbs = dc - md.bs_r;
+      if (lbs * 0.999999f > noise_bound_at(md.k, m.c, p)) {
+        m.mu_j = lbs;
+        m.mu_hi = dc + md.bs_r;
+        m.t_j = 0.0f;
+        m.fprev_pos = true;
+        m.fprev_big = true;
+        m.init = false;
+      }
+    }
+  }
+  if (m.init) {
     float mu = mean_value<MK>(S, md, p, ovf);
     m.mu_j = mu;
     m.mu_hi = fabsf(mu);
