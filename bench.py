@@ -293,6 +293,7 @@ def run_gpu(args):
     # render, framebuffer read back, release, every step
     host_fb = torch.empty((H, W, 3), dtype=torch.float32, pin_memory=True).numpy()
     e2e_times = []
+    e2e_parts = []
     desc_bytes = 0
     for i in range(args.warmup + args.steps):
         torch.cuda.synchronize()
@@ -300,10 +301,13 @@ def run_gpu(args):
         g2 = GpuScene(sc)
         r2 = GpuRenderer()
         r2.prepare_render(g2)
+        t1 = time.perf_counter()
         r2.start_render_progressive(pass1, spp_begin=pass0, out=host_fb)
+        t2 = time.perf_counter()
         g2.close()
         if i >= args.warmup:
             e2e_times.append(time.perf_counter() - t0)
+            e2e_parts.append((t1 - t0, t2 - t1, time.perf_counter() - t2))
     # bytes the scene create copies host->device: descriptor + march table (4001 floats)
     desc_bytes = 4 * 4001 + 8192
     e2e_t = torch.tensor([sum(e2e_times)], dtype=torch.float64, device="cuda")
@@ -324,7 +328,10 @@ def run_gpu(args):
                 "config": _config({"parallelism": f"spp-sharded x{world}" if world > 1 else "single GPU",
                                    "global_batch": SAMPLES_PER_STEP * world}),
                 "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": desc_bytes,
-                        "d2h_bytes_per_step": W * H * 3 * 4},
+                        "d2h_bytes_per_step": W * H * 3 * 4,
+                        "step_ms": [round(1e3 * t, 3) for t in e2e_times],
+                        "median_create_render_destroy_ms": [round(1e3 * float(np.median([p[k] for p in e2e_parts])), 3)
+                                                            for k in range(3)]},
                 "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clk}
         if extras:
             line["extras"] = extras
