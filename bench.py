@@ -43,6 +43,8 @@ def _args():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=8.0, help="CPU work per reference/baseline step")
     ap.add_argument("--extras", type=int, default=1, help="also time configurations 1-4 (single GPU)")
+    ap.add_argument("--only", choices=EXTRAS, default=None,
+                    help="time only this configuration (its JSON object, no bench line)")
     return ap.parse_args()
 
 
@@ -341,15 +343,29 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
-def run_extras(args):
-    """Configuration 1 (psi microbench: 2^24 points, 18 sweep points, psi + grad psi +
-    Renewal+ conditioning) and configuration 2 (displaced-icosphere mesh mean, 81,920
-    triangles, 512x512x64) on the same GPU, device-timed with CUDA events."""
-    import torch
-    from mupsi_b200 import scene as S
-    from mupsi_b200.api import GpuRenderer, GpuScene, SparseGPNoiseGenerator, SparseSEKernel
+EXTRAS = ("config1", "config2", "config4", "config3")
 
+
+def run_extras(args, only=None):
+    """The other configurations on the same GPU, device-timed with CUDA events:
+    1 (psi microbench), 2 (level-6 mesh mean render), 4 (batched instances) and
+    3 (level-8 mesh, exact mean against the surrogate). `only` runs one of them."""
     out = {}
+    legs = {"config1": ("config1_psi", run_psi_sweep), "config2": ("config2_mesh", run_mesh),
+            "config4": ("config4_batch", run_batch), "config3": ("config3_surrogate", run_surrogate)}
+    for name in EXTRAS:
+        if only is None or only == name:
+            key, fn = legs[name]
+            out[key] = fn()
+    return out
+
+
+def run_psi_sweep():
+    """Configuration 1: psi + grad psi + Renewal+ conditioning at 2^24 points per
+    sweep point (length scale x aniso x points per cell, 18 points)."""
+    import torch
+    from mupsi_b200.api import SparseGPNoiseGenerator, SparseSEKernel
+
     n = 1 << 24
     g = torch.Generator(device="cuda").manual_seed(0)
     p = (torch.rand((n, 3), device="cuda", generator=g) * 300 - 150).contiguous()
@@ -382,9 +398,16 @@ def run_extras(args):
                 total_ms += ms
                 imps += n * 27 * ppc
                 sweep[f"L{L}_aniso{az:g}_ppc{ppc}"] = {"ms": round(ms, 3), "Gqueries_s": round(n / ms / 1e6, 3)}
-    out["config1_psi"] = {"queries_per_point": n, "points": 18, "total_ms": round(total_ms, 2),
-                          "Gimpulse_evals_s": round(imps / total_ms / 1e6, 1), "sweep": sweep}
-    del p, seed, d, cond, res
+    return {"queries_per_point": n, "points": 18, "total_ms": round(total_ms, 2),
+            "Gimpulse_evals_s": round(imps / total_ms / 1e6, 1), "sweep": sweep}
+
+
+def run_mesh():
+    """Configuration 2: displaced icosphere level 6 (81,920 triangles) mesh mean, 512x512x64."""
+    import torch
+    from mupsi_b200 import scene as S
+    from mupsi_b200.api import GpuRenderer, GpuScene
+
     sc = S.config_mesh_scene(level=6, width=512, height=512, spp=64)
     gs = GpuScene(sc)
     r = GpuRenderer()
@@ -398,13 +421,9 @@ def run_extras(args):
     e1.record()
     e1.synchronize()
     ms = e0.elapsed_time(e1)
-    out["config2_mesh"] = {"workload": "displaced icosphere level 6 (81,920 triangles) mesh mean, 512x512x64, "
-                                       "length_scale 2, floor quad", "ms": round(ms, 1),
-                           "samples_per_s": 512 * 512 * 64 / (ms / 1000.0)}
     gs.close()
-    out["config4_batch"] = run_batch()
-    out["config3_surrogate"] = run_surrogate()
-    return out
+    return {"workload": "displaced icosphere level 6 (81,920 triangles) mesh mean, 512x512x64, "
+                        "length_scale 2, floor quad", "ms": round(ms, 1), "samples_per_s": 512 * 512 * 64 / (ms / 1000.0)}
 
 
 def run_surrogate(spp=2, train_steps=6000):
@@ -534,6 +553,10 @@ def main():
     args = _args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.only:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        print(json.dumps(run_extras(args, only=args.only)), flush=True)
     else:
         run_gpu(args)
 
