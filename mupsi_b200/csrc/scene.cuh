@@ -432,6 +432,21 @@ MD void march_psi(const DScene* S, March& m, v3 p, const Group& g, bool& ovf) {
       march_advance(S, m, -INFINITY);
       return;
     }
+    if (m.lazy) {
+      // mu is a signed distance, 1-Lipschitz along the ray: from the anchor it
+      // lies in [mu_lo, mu_hi] here. When that interval plus psi + cond keeps
+      // the sign f had at the origin, this step is not a hit and needs no BVH
+      // query (a sign change still takes the exact value below).
+      const float d = fabsf(m.t - m.t_j) * 1.0001f + 1e-2f;
+      const float lo = (m.mu_j > 0.0f ? m.mu_j : -m.mu_hi) - d;
+      const float hi = (m.mu_j > 0.0f ? m.mu_hi : m.mu_j) + d;
+      const float qc = q + c;
+      const float slack = (fabsf(q) + fabsf(c) + fmaxf(fabsf(lo), fabsf(hi))) * 1e-5f + 1e-5f;
+      if ((m.fprev_pos && lo + qc > slack) || (!m.fprev_pos && hi + qc < -slack)) {
+        march_advance(S, m, -INFINITY);
+        return;
+      }
+    }
     float mu = mean_exact<MK>(S, m, p, m.t, ovf);
     m.mu_j = mu;
     m.mu_hi = fabsf(mu);
