@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(128) k_march(const DScene* const* __restrict__
     if (!__any_sync(0xffffffffu, active)) break;
     if (active) {
       v3 p;
-      if (march_cheap<MK>(S, m, p, ovf)) march_psi<MK, true>(S, m, p, grp, ovf);
+      if (march_cheap<MK>(S, m, p, ovf, &grp)) march_psi<MK, true>(S, m, p, grp, ovf);
       if (MK != MEAN_SPHERE_ONLY && m.status == 3) {  // suspended: save the march, request a prediction at p
         if (grp.sub == 0) {
           const int fl = (m.fprev_pos ? 1 : 0) | (m.fprev_big ? 2 : 0) | (m.n_req << 8);

@@ -65,8 +65,11 @@ def test_batch_equals_single_renders(gpu, tuning_restored, graphs, schedule):
     b.close()
 
 
-def test_results_do_not_depend_on_launch_shape(gpu, tuning_restored):
-    sc = S.config0_scene(20, 20, 3)
+@pytest.mark.parametrize("scene", ["sphere", "mesh"])
+def test_results_do_not_depend_on_launch_shape(gpu, tuning_restored, scene):
+    # sphere: the fixed psi order; mesh: also the group-parallel closest-point
+    # query (lowest triangle index among ties)
+    sc = S.config0_scene(20, 20, 3) if scene == "sphere" else S.config_mesh_scene(level=4, width=20, height=20, spp=3)
     gs = GpuScene(sc)
     xs, ys, ks = (a.ravel().astype(np.int32) for a in np.meshgrid(np.arange(20), np.arange(20), np.arange(3),
                                                                  indexing="ij"))
