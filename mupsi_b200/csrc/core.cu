@@ -85,6 +85,12 @@ KParams make_kparams(const mupsi_kernel& k) {
   KParams p;
   p.sigma = k.sigma;
   p.kr = k.kernel_radius;
+  {
+    int e = 0;
+    const float m = std::frexp(p.kr, &e);  // kr = m * 2^e, m in [0.5, 1)
+    p.kr_pow2 = (m == 0.5f && e > -125 && e < 126) ? 1 : 0;
+    p.inv_kr = p.kr_pow2 ? std::ldexp(1.0f, 1 - e) : 0.0f;
+  }
   p.L2 = k.aniso[0] * k.aniso[0] + (k.aniso[1] * k.aniso[1] + k.aniso[2] * k.aniso[2]);
   p.ppc = k.points_per_cell;
   // Var() (gpnoise.h:31): int / std::pow(float, int) -> double, * pow(pi, 1.5), returned as float

@@ -27,6 +27,8 @@ struct KParams {
   float gradh_max;   // max over r of |grad h| = sqrt(2/L2) * exp(-1/2)
   float psi_scale;   // sigma * ppc / sqrt_var
   int ppc;           // impulses per cell
+  int kr_pow2;       // kr is a power of two: p / kr == p * inv_kr, bit for bit
+  float inv_kr;
 };
 
 MD float ex2_approx(float x) {
@@ -37,9 +39,15 @@ MD float ex2_approx(float x) {
 
 // Grid cell of p: (p / kr).cast<int>() (gpnoise.cpp:54), truncation toward zero.
 MD void cell_of(const KParams& k, v3 p, int& cx, int& cy, int& cz) {
-  cx = (int)(p.x / k.kr);
-  cy = (int)(p.y / k.kr);
-  cz = (int)(p.z / k.kr);
+  if (k.kr_pow2) {  // division by 2^e is the exact scaling by 2^-e, as the multiply is
+    cx = (int)(p.x * k.inv_kr);
+    cy = (int)(p.y * k.inv_kr);
+    cz = (int)(p.z * k.inv_kr);
+  } else {
+    cx = (int)(p.x / k.kr);
+    cy = (int)(p.y / k.kr);
+    cz = (int)(p.z / k.kr);
+  }
 }
 
 // Impulses of one cell, visited in the reference's order. F(s, w) is called per
