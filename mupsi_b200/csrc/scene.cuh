@@ -156,6 +156,10 @@ struct March {
   // pending step between the two phases
   bool pend_exact;  // pend_mu holds the exact mean at the pending point
   float pend_mu, pend_lb, pend_sgn;
+  // psi of the next step, computed ahead by an otherwise idle half of a 32-lane
+  // group (march_psi): valid for the step at spec_t
+  bool spec_valid;
+  float spec_t, spec_q;
 };
 
 // o, d: the Ray's origin and (already normalised) direction
@@ -191,6 +195,9 @@ MD void march_begin(const DScene* S, March& m, v3 o, v3 d, float near_t, float f
   m.n_req = 0;
   m.t_resumed = -1.0f;
   m.pend_exact = false;
+  m.spec_valid = false;
+  m.spec_t = 0.0f;
+  m.spec_q = 0.0f;
   m.pend_mu = 0.0f;
   m.pend_lb = 0.0f;
 }
@@ -514,7 +521,39 @@ template <int MK = MEAN_ANY, bool WIDE = false>
 MD void march_psi(const DScene* S, March& m, v3 p, const Group& g, bool& ovf) {
   const DMedium& md = S->media[m.medium];
   m.n_psi++;
-  float q = raw_noise_value_group<WIDE>(md.k, p, m.seed, g);
+  float q;
+  if (m.spec_valid && m.spec_t == m.t) {
+    q = m.spec_q;  // computed with the previous step (same point, same order)
+    m.spec_valid = false;
+  } else if (MK == MEAN_SPHERE_ONLY && WIDE && g.G == 32) {
+    // The psi order keeps 16 lanes busy; the upper half evaluates the next step
+    // (sphere-mean marches: in mesh marches the BVH queries set the pace)
+    // (t as march_advance will produce it, the same point march_cheap will form)
+    // for use if the march gets there next.
+    float tn = m.t;
+    bool ok;
+    if (m.use_tab) {
+      ok = m.k + 1 <= S->tab_steps;
+      if (ok) tn = __ldg(S->tab + m.k + 1);
+    } else {
+      tn = m.t + m.dt;
+      ok = tn < m.ft && tn != m.t;
+    }
+    const bool upper = g.sub >= 16;
+    Group h;
+    h.G = 16;
+    h.sub = g.sub & 15;
+    h.mask = upper ? 0xffff0000u : 0x0000ffffu;
+    const v3 pe = upper && ok ? m.o + m.d * tn : p;
+    const float v = (md.k.sigma * psi_sums_group<false, true>(md.k, pe, m.seed, h).x) / md.k.sqrt_var;
+    const float vo = __shfl_xor_sync(0xffffffffu, v, 16);
+    q = upper ? vo : v;
+    m.spec_q = upper ? v : vo;
+    m.spec_t = tn;
+    m.spec_valid = ok;
+  } else {
+    q = raw_noise_value_group<WIDE>(md.k, p, m.seed, g);
+  }
   float c = m.c.active ? cond_value(md.k, m.c, p) : 0.0f;
   float f;
   if (m.pend_exact) {
