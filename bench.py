@@ -433,7 +433,8 @@ def run_surrogate(spp=2, train_steps=6000):
     samples moved by N(0, 2^2) along the normal) labelled with the GPU's exact
     BVH mean, checked on 2^18 held-out points, then attached (band 3, scale 1.5,
     margin from the held-out bound violations x 2). Both forms render the same
-    `spp` passes (a bounded sample of the 64-spp workload), device-timed."""
+    `spp` passes (a bounded sample of the 64-spp workload), device-timed, best of
+    two renders."""
     import torch
     from mupsi_b200 import scene as S
     from mupsi_b200 import surrogate as SG
@@ -472,15 +473,19 @@ def run_surrogate(spp=2, train_steps=6000):
         r.start_render_progressive(1, out=fb)  # warm-up
         g.profile(True)
         g.stats(reset=True)
-        torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
-        r.start_render_progressive(spp, out=fb)
-        b.record()
-        b.synchronize()
+        times = []
+        for _ in range(2):  # best of two renders of the same passes
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            r.start_render_progressive(spp, out=fb)
+            b.record()
+            b.synchronize()
+            times.append(a.elapsed_time(b))
         st = g.stats(reset=True)
         g.profile(False)
-        return fb.cpu().numpy(), a.elapsed_time(b), st
+        st = {k: (v / 2 if isinstance(v, (int, float)) else v) for k, v in st.items()}  # per render
+        return fb.cpu().numpy(), min(times), st
 
     img_e, ms_e, st_e = render(gs)
     gs2 = GpuScene(sc)
