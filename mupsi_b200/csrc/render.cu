@@ -209,7 +209,7 @@ struct WaveCfg {
 // fills the resident threads, larger (up to 32) as the queue shrinks, so the
 // late bounces' few long marches finish up to 8x sooner than on one lane.
 template <int MK>
-__global__ void __launch_bounds__(128) k_march(const DScene* const* __restrict__ scenes, Paths P, int it, int round,
+__global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? 6 : 1) k_march(const DScene* const* __restrict__ scenes, Paths P, int it, int round,
                                                WaveCfg cfg) {
   // round 0 marches the iteration's medium queue; round r >= 1 resumes the
   // marches suspended in round r - 1 with their surrogate predictions
