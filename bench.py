@@ -488,6 +488,24 @@ def run_surrogate(spp=2, train_steps=6000):
         return fb.cpu().numpy(), min(times), st
 
     img_e, ms_e, st_e = render(gs)
+    # the plain exact form (BVH parity cast + closest point at every visited
+    # step) on a 256x256 view of the same scene: same rays per pixel sample,
+    # 16x fewer samples to keep the run short
+    scp = S.config_mesh_scene(level=8, width=256, height=256, spp=2)
+    gp = GpuScene(scp)
+    gp.set_mean_eval(0, every_step=True)
+    rp = GpuRenderer()
+    rp.prepare_render(gp)
+    fbp = torch.empty((256, 256, 3), device="cuda")
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    rp.start_render_progressive(2, out=fbp)
+    b.record()
+    b.synchronize()
+    plain_ms = a.elapsed_time(b)
+    plain_rate = 256 * 256 * 2 / (plain_ms / 1e3)
+    gp.close()
     gs2 = GpuScene(sc)
     SG.attach(gs2, 0, sm, band=3.0, scale=1.5, margin=margin, max_requests=8)
     img_s, ms_s, st_s = render(gs2)
@@ -506,7 +524,10 @@ def run_surrogate(spp=2, train_steps=6000):
                          "exact_mean_evals_per_sample": st_s["mean_evals"] / n,
                          "predictions_per_sample": st_s["surr_requests"] / n,
                          "accepted_per_sample": st_s["surr_accepted"] / n},
+           "plain_every_step": {"workload": "same scene and camera at 256x256, 2 spp", "ms": round(plain_ms, 1),
+                                "samples_per_s": plain_rate},
            "speedup": ms_e / ms_s,
+           "speedup_vs_plain": (n / (ms_s / 1e3)) / plain_rate,
            "image_rmse_vs_exact": rmse, "image_rmse_rel": rmse / max(1e-12, float(np.mean(img_e))),
            "identical_pixels": float(np.all(img_s.view(np.uint32) == img_e.view(np.uint32), axis=2).mean())}
     gs2.close()

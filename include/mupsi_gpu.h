@@ -356,6 +356,15 @@ int mupsi_gpu_mlp_train(mupsi_mlp* mlp, int64_t n, const float* p, const float* 
 int mupsi_gpu_scene_set_surrogate(mupsi_scene* scene, int32_t medium, mupsi_mlp* mlp, float band, float scale,
                                   float margin, int32_t max_requests);
 
+/* How a march evaluates a mesh mean (no reference counterpart: the reference
+ * evaluates mu at every step, GPMedium::evalWithGradient per step,
+ * medium/gpmedium.cpp:46-103). LAZY (the default) keeps the last exact value
+ * and its Lipschitz bounds and queries the BVH only where they cannot settle a
+ * step; EVERY_STEP queries the BVH (parity cast + closest point) at every
+ * visited step, the plain exact form. Both give the same march results. */
+enum { MUPSI_MEAN_EVAL_LAZY = 0, MUPSI_MEAN_EVAL_EVERY_STEP = 1 };
+int mupsi_gpu_scene_set_mean_eval(mupsi_scene* scene, int32_t medium, int32_t mode);
+
 /* ------------------------------------------------------------------ tuning
  * Launch shapes of the wave kernels, process-wide. No reference counterpart
  * (the reference's OpenMP loop has no launch shapes); the values come from the

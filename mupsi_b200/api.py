@@ -326,6 +326,10 @@ class GpuScene:
                                                      _stream(stream)))
         return out
 
+    def set_mean_eval(self, medium, every_step):
+        """Mesh mean at every visited step (the plain exact form) or lazily (default)."""
+        check(load().mupsi_gpu_scene_set_mean_eval(self.h, medium, 1 if every_step else 0))
+
     def profile(self, enable=True):
         """Count march work and time the wavefront kernels with CUDA events."""
         check(load().mupsi_gpu_scene_profile(self.h, 1 if enable else 0))

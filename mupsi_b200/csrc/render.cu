@@ -1811,4 +1811,16 @@ int mupsi_gpu_scene_set_surrogate(mupsi_scene* scene, int32_t medium, mupsi_mlp*
   return MUPSI_OK;
 }
 
+int mupsi_gpu_scene_set_mean_eval(mupsi_scene* scene, int32_t medium, int32_t mode) {
+  clear_error();
+  if (!scene) return fail(MUPSI_ERR_INVALID, "null scene");
+  if (medium < 0 || medium >= scene->h.nmed) return fail(MUPSI_ERR_INVALID, "medium out of range");
+  if (mode != MUPSI_MEAN_EVAL_LAZY && mode != MUPSI_MEAN_EVAL_EVERY_STEP)
+    return fail(MUPSI_ERR_INVALID, "unknown mean evaluation mode");
+  scene->h.media[medium].every_step = mode == MUPSI_MEAN_EVAL_EVERY_STEP;
+  MUPSI_CUDA(cudaDeviceSynchronize());
+  MUPSI_CUDA(cudaMemcpy(scene->d, &scene->h, sizeof(DScene), cudaMemcpyHostToDevice));
+  return MUPSI_OK;
+}
+
 }  // extern "C"

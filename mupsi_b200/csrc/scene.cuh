@@ -31,6 +31,7 @@ struct DMedium {
   // |m| / surr_scale - surr_add <= |mu| <= |m| * surr_scale + surr_add, same sign
   int surr;
   int surr_max;  // predictions per march
+  int every_step;  // mesh mean queried exactly at every visited step (the plain form; no lazy mean)
   float surr_band, surr_scale, surr_add;
 };
 
@@ -187,7 +188,7 @@ MD void march_begin(const DScene* S, March& m, v3 o, v3 d, float near_t, float f
   m.n_psi = 0;
   m.n_mu = 0;
   m.n_par = 0;
-  m.lazy = S->media[medium].mean_type == MUPSI_MEAN_MESH;
+  m.lazy = S->media[medium].mean_type == MUPSI_MEAN_MESH && !S->media[medium].every_step;
   m.mu_j = 0.0f;
   m.t_j = 0.0f;
   m.mu_hi = 0.0f;

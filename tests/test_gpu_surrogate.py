@@ -92,3 +92,24 @@ def test_surrogate_rejects_bad_settings(gpu, trained):
     with pytest.raises(MupsiError):
         SG.attach(GpuScene(s0), 0, sm)
     g.close()
+
+
+def test_plain_every_step_mean_matches_lazy(gpu):
+    """The plain exact form (BVH parity cast + closest point at every visited
+    step) and the lazy exact form give the same samples: the lazy mean's bounds,
+    crossings and intervals only skip queries whose answer they already know."""
+    sc = S.config_mesh_scene(level=3, width=24, height=24, spp=2, seed=3)
+    lazy, plain = GpuScene(sc), GpuScene(sc)
+    plain.set_mean_eval(0, every_step=True)
+    xs, ys, ks = (a.ravel().astype(np.int32) for a in np.meshgrid(np.arange(24), np.arange(24), np.arange(2),
+                                                                 indexing="ij"))
+    a, b = lazy.trace(xs, ys, ks), plain.trace(xs, ys, ks)
+    assert np.all(bits(a) == bits(b), axis=1).mean() >= 0.99
+    plain.profile(True)
+    plain.stats(reset=True)
+    plain.trace(xs, ys, ks)
+    st = plain.stats()
+    assert st["mean_evals"] == 0  # no lazy evaluations: every step went through the full mean
+    from mupsi_b200.lib import MupsiError
+    with pytest.raises(MupsiError):
+        plain.set_mean_eval(3, every_step=True)
