@@ -191,6 +191,14 @@ int mupsi_gpu_bvh_intersect(const mupsi_mesh* mesh, int64_t n, const mupsi_ray* 
 /* BVH::occluded (bvh.cpp:254-300), including its traversal start at node 0. */
 int mupsi_gpu_bvh_occluded(const mupsi_mesh* mesh, int64_t n, const mupsi_ray* rays, uint8_t* out,
                            mupsi_mem mem, void* stream);
+/* Where BVH::occluded starts: REFERENCE (the default) at node 0 as the
+ * reference does (bvh/bvh.cpp:259; node 0 is the post-order array's first leaf,
+ * so most occluders are missed), ROOT at the root (a full traversal, the same
+ * answer as an intersect within [near_t, far_t]). For a mesh handle, or for all
+ * meshes of a scene (its shadow rays). */
+enum { MUPSI_OCCLUSION_REFERENCE = 0, MUPSI_OCCLUSION_ROOT = 1 };
+int mupsi_gpu_mesh_set_occlusion(mupsi_mesh* mesh, int32_t mode);
+int mupsi_gpu_scene_set_occlusion(mupsi_scene* scene, int32_t mode);
 /* BVH::closest (bvh.cpp:302-353): out_tri[n], out_dq[n*4] = (dist, q xyz). */
 int mupsi_gpu_bvh_closest(const mupsi_mesh* mesh, int64_t n, const float* p, uint32_t* out_tri, float* out_dq,
                           mupsi_mem mem, void* stream);

@@ -162,6 +162,10 @@ class DeviceMesh:
         except Exception:
             pass
 
+    def set_occlusion(self, from_root):
+        """occluded(): from node 0 as the reference (default) or from the root."""
+        check(load().mupsi_gpu_mesh_set_occlusion(self.h, 1 if from_root else 0))
+
     def intersect(self, rays, stream=None):
         """BVH::intersect: rays (n, 8) [o, d, nearT, farT] -> (tri u32 (0xFFFFFFFF miss), (t, u, v))."""
         rays = _host(rays, np.float32)
@@ -325,6 +329,10 @@ class GpuScene:
         check(load().mupsi_gpu_trace_samples_noalloc(self.h, x.shape[0], _ptr(x), _ptr(y), _ptr(k), _ptr(out),
                                                      _stream(stream)))
         return out
+
+    def set_occlusion(self, from_root):
+        """Shadow rays: BVH::occluded from node 0 as the reference (default) or from the root."""
+        check(load().mupsi_gpu_scene_set_occlusion(self.h, 1 if from_root else 0))
 
     def set_mean_eval(self, medium, every_step):
         """Mesh mean at every visited step (the plain exact form) or lazily (default)."""

@@ -267,6 +267,7 @@ int make_device_mesh(const mupsi_mesh_desc& md, DMesh& d, std::vector<void*>& al
   d.num_nodes = (int64_t)nodes.size();
   d.num_faces = md.num_faces;
   d.root = root;
+  d.occl_start = 0;
   d.total_area = total;
   HostM4 T = translate_scale(md.position, md.scale), Ti = inverse4(T);
   std::memcpy(d.T.m, T.m, sizeof T.m);
@@ -434,6 +435,15 @@ int mupsi_gpu_bvh_intersect(const mupsi_mesh* mesh, int64_t n, const mupsi_ray* 
   MUPSI_CUDA(dt.finish());
   MUPSI_CUDA(duv.finish());
   if (err.read()) return fail(MUPSI_ERR_DEVICE_LIMIT, "BVH traversal exceeded the 64-entry stack");
+  return MUPSI_OK;
+}
+
+int mupsi_gpu_mesh_set_occlusion(mupsi_mesh* mesh, int32_t mode) {
+  clear_error();
+  if (!mesh) return fail(MUPSI_ERR_INVALID, "null mesh");
+  if (mode != MUPSI_OCCLUSION_REFERENCE && mode != MUPSI_OCCLUSION_ROOT)
+    return fail(MUPSI_ERR_INVALID, "unknown occlusion mode");
+  mesh->store.d.occl_start = mode == MUPSI_OCCLUSION_ROOT ? mesh->store.d.root : 0u;
   return MUPSI_OK;
 }
 

@@ -40,6 +40,7 @@ struct DMesh {
   const float* cdf;       // area CDF [F]
   int64_t num_nodes, num_faces;
   uint32_t root;
+  uint32_t occl_start;    // first node of BVH::occluded: 0 as the reference, or root
   float total_area;
   m4 T, Tinv;
   int identity;           // Tinv.isIdentity()
@@ -147,12 +148,13 @@ MD bool bvh_intersect(const DMesh& m, Ray& r, uint32_t& tri, float& uu, float& v
 
 // BVH::occluded (bvh.cpp:254-300). The reference starts this traversal at node 0,
 // which is the first leaf of the post-order array, not the root (bvh.cpp:259);
-// that behaviour is kept so shadow rays agree with the reference.
+// that behaviour is the default so shadow rays agree with the reference, and
+// MUPSI_OCCLUSION_ROOT (occl_start = root) switches to the full traversal.
 MD bool bvh_occluded(const DMesh& m, const Ray& r, bool& overflow) {
   if (m.num_nodes == 0) return false;
   uint32_t st[BVH_STACK];
   int sp = 0;
-  st[sp++] = 0;
+  st[sp++] = m.occl_start;
   while (sp > 0) {
     BNode nd = load_node(m.nodes, st[--sp]);
     if (!aabb_hit(nd, r)) continue;

@@ -60,6 +60,8 @@ def _setup(L):
     L.mupsi_gpu_mlp_train.argtypes = [vp, i64, vp, vp, vp, vp, C.c_int, vp]
     L.mupsi_gpu_scene_set_surrogate.argtypes = [vp, i32, vp, C.c_float, C.c_float, C.c_float, i32]
     L.mupsi_gpu_scene_set_mean_eval.argtypes = [vp, i32, i32]
+    L.mupsi_gpu_mesh_set_occlusion.argtypes = [vp, i32]
+    L.mupsi_gpu_scene_set_occlusion.argtypes = [vp, i32]
     return L
 
 

@@ -87,3 +87,22 @@ def test_bvh_edge_cases(gpu, port):
     finally:
         port.scene_free(h)
 
+
+
+def test_occlusion_from_root_matches_intersect(gpu):
+    """MUPSI_OCCLUSION_ROOT: occluded() answers exactly as an intersect within
+    [near_t, far_t]; the reference's start at node 0 (the default) misses
+    occluders outside the first leaf."""
+    rng = np.random.default_rng(9)
+    v, f = S.displaced_icosphere(4, seed=4)
+    m = DeviceMesh(v, f)
+    rays = _rays(rng, 20000)
+    tri, _ = m.intersect(rays)
+    hit = tri != 0xFFFFFFFF
+    reference = m.occluded(rays).astype(bool)
+    m.set_occlusion(True)
+    root = m.occluded(rays).astype(bool)
+    assert np.array_equal(root, hit)
+    assert (reference != root).sum() > 100
+    m.set_occlusion(False)
+    assert np.array_equal(m.occluded(rays).astype(bool), reference)

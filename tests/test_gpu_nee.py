@@ -92,3 +92,26 @@ def test_bvh_stack_overflow_reports_device_limit(gpu):
     assert e.value.code == _abi.ERR_DEVICE_LIMIT
     tri, _ = m.intersect(np.array([[-1, 0.2, 0.2, -1, 0, 0, 0, 10]], np.float32))  # still usable
     assert tri[0] == 0xFFFFFFFF
+
+
+def test_scene_occlusion_from_root(gpu):
+    """Scene shadow rays with BVH::occluded from the root: an icosphere hanging
+    between a sphere light and a floor shadows it, while the reference's start
+    at node 0 (the default) lets most shadow rays through."""
+    sc = S.Scene()
+    sc.width = sc.height = 32
+    sc.max_bounce = 3
+    fv, ff = S.floor_quad()
+    sc.add_mesh_primitive(sc.add_mesh(S.Mesh(fv, ff)), bsdf=_abi.BSDF_LAMBERTIAN, albedo=0.7)
+    ov, of = S.displaced_icosphere(3, radius=50.0, center=(0.0, 40.0, -400.0), seed=1)
+    sc.add_mesh_primitive(sc.add_mesh(S.Mesh(ov, of)), bsdf=_abi.BSDF_LAMBERTIAN, albedo=0.5)
+    sc.add_sphere((0.0, 220.0, -400.0), 30.0, bsdf=_abi.BSDF_LAMBERTIAN, emission=(20.0, 20.0, 20.0))
+    xs, ys, ks = (a.ravel().astype(np.int32) for a in np.meshgrid(np.arange(32), np.arange(32), np.arange(2),
+                                                                 indexing="ij"))
+    ref_mode = GpuScene(sc).trace(xs, ys, ks)
+    g = GpuScene(sc)
+    g.set_occlusion(True)
+    root_mode = g.trace(xs, ys, ks)
+    darker = np.all(root_mode <= ref_mode * (1 + 1e-5) + 1e-6, axis=1)
+    assert darker.all()  # the same paths; only NEE contributions can disappear
+    assert (root_mode.sum(axis=1) < ref_mode.sum(axis=1) - 1e-3).sum() > 10
