@@ -364,6 +364,13 @@ int mupsi_gpu_mlp_train(mupsi_mlp* mlp, int64_t n, const float* p, const float* 
 int mupsi_gpu_scene_set_surrogate(mupsi_scene* scene, int32_t medium, mupsi_mlp* mlp, float band, float scale,
                                   float margin, int32_t max_requests);
 
+/* Skydrome with a BitmapTexture (controller.cpp:191-195, skydrome.cpp:8-17,
+ * texture.cpp:52-69): rays that leave the scene take the nearest texel of the
+ * equirectangular image at their direction. rgb: width x height texels of 3
+ * floats, row 0 at the top, host memory (copied); it replaces the constant sky
+ * of the descriptor. width = height = 0 removes it. */
+int mupsi_gpu_scene_set_sky_texture(mupsi_scene* scene, int32_t width, int32_t height, const float* rgb);
+
 /* How a march evaluates a mesh mean (no reference counterpart: the reference
  * evaluates mu at every step, GPMedium::evalWithGradient per step,
  * medium/gpmedium.cpp:46-103). LAZY (the default) keeps the last exact value

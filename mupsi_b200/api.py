@@ -255,6 +255,8 @@ class GpuScene:
         h = C.c_void_p()
         check(load().mupsi_gpu_scene_create(C.byref(self._desc), C.byref(h)))
         self.h = h
+        if getattr(scene, "sky_texture", None) is not None:
+            self.set_sky_texture(scene.sky_texture)
 
     def close(self):
         if self.h:
@@ -329,6 +331,14 @@ class GpuScene:
         check(load().mupsi_gpu_trace_samples_noalloc(self.h, x.shape[0], _ptr(x), _ptr(y), _ptr(k), _ptr(out),
                                                      _stream(stream)))
         return out
+
+    def set_sky_texture(self, img):
+        """Skydrome BitmapTexture: (h, w, 3) float RGB, row 0 at the top; None removes it."""
+        if img is None:
+            check(load().mupsi_gpu_scene_set_sky_texture(self.h, 0, 0, None))
+            return
+        img = np.ascontiguousarray(img, np.float32)
+        check(load().mupsi_gpu_scene_set_sky_texture(self.h, img.shape[1], img.shape[0], img.ctypes.data))
 
     def set_occlusion(self, from_root):
         """Shadow rays: BVH::occluded from node 0 as the reference (default) or from the root."""

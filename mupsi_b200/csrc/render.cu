@@ -445,6 +445,8 @@ __global__ void __launch_bounds__(128) k_shade(const DScene* const* __restrict__
           bounce++;
           has_hit = true;
         }
+      } else if (S->sky_tex) {
+        em = em + cmul(thr, sky_lookup(S, ray.d));
       } else if (S->has_sky) {
         em = em + cmul(thr, S->sky);
       }
@@ -627,6 +629,7 @@ struct mupsi_scene {
   int next_pass = -1;  // pass after the last one accumulated
   PathBuf pb;  // wave buffers (grow-only)
   mupsi_mlp* surr_mlp = nullptr;  // surrogate of a mesh mean (not owned)
+  void* sky_mem = nullptr;        // sky texture texels (owned)
   int surr_rounds = 1;            // march rounds per bounce iteration with it: predictions + 1
   int* err = nullptr;
   unsigned long long* counters = nullptr;
@@ -703,6 +706,7 @@ mupsi_scene::~mupsi_scene() {
     if (d) cudaFree(d);
     if (d_list) cudaFree(d_list);
     if (d_chunk) cudaFree(d_chunk);
+    if (sky_mem) cudaFree(sky_mem);
     if (sum) cudaFree(sum);
     if (pb.mem) pool_give(pb.mem, pb.bytes);
     if (err) cudaFree(err);
@@ -1831,6 +1835,32 @@ int mupsi_gpu_scene_set_occlusion(mupsi_scene* scene, int32_t mode) {
   for (int i = 0; i < scene->h.nmesh; ++i)
     scene->h.meshes[i].occl_start = mode == MUPSI_OCCLUSION_ROOT ? scene->h.meshes[i].root : 0u;
   MUPSI_CUDA(cudaDeviceSynchronize());
+  MUPSI_CUDA(cudaMemcpy(scene->d, &scene->h, sizeof(DScene), cudaMemcpyHostToDevice));
+  return MUPSI_OK;
+}
+
+int mupsi_gpu_scene_set_sky_texture(mupsi_scene* scene, int32_t width, int32_t height, const float* rgb) {
+  clear_error();
+  if (!scene) return fail(MUPSI_ERR_INVALID, "null scene");
+  if (width < 0 || height < 0 || width > (1 << 15) || height > (1 << 15))
+    return fail(MUPSI_ERR_INVALID, "sky texture size out of range");
+  if ((width == 0) != (height == 0)) return fail(MUPSI_ERR_INVALID, "sky texture needs width and height");
+  if (width > 0 && !rgb) return fail(MUPSI_ERR_INVALID, "null sky texels");
+  MUPSI_CUDA(cudaDeviceSynchronize());
+  if (scene->sky_mem) {
+    cudaFree(scene->sky_mem);
+    scene->sky_mem = nullptr;
+  }
+  scene->h.sky_tex = nullptr;
+  scene->h.sky_w = scene->h.sky_h = 0;
+  if (width > 0) {
+    const size_t bytes = (size_t)width * height * 3 * sizeof(float);
+    MUPSI_CUDA(cudaMalloc(&scene->sky_mem, bytes));
+    MUPSI_CUDA(cudaMemcpy(scene->sky_mem, rgb, bytes, cudaMemcpyHostToDevice));
+    scene->h.sky_tex = static_cast<const float*>(scene->sky_mem);
+    scene->h.sky_w = width;
+    scene->h.sky_h = height;
+  }
   MUPSI_CUDA(cudaMemcpy(scene->d, &scene->h, sizeof(DScene), cudaMemcpyHostToDevice));
   return MUPSI_OK;
 }

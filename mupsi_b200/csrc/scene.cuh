@@ -46,6 +46,10 @@ struct DScene {
   float eps, nearteps;
   int has_sky;
   v3 sky;
+  // Skydrome with a BitmapTexture: RGB texels, row 0 at the top (nullable;
+  // replaces the constant sky)
+  const float* sky_tex;
+  int sky_w, sky_h;
   int nprim, nmed, nmesh, nlights;
   int lights[MAX_PRIMS];
   DPrim prims[MAX_PRIMS];
@@ -757,6 +761,26 @@ MD Hit scene_intersect(const DScene* S, Ray& r, bool& ovf) {
     }
   }
   return hi;
+}
+
+// Skydrome::intersect (skydrome.cpp:8-17) + BitmapTexture::operator[]
+// (texture.cpp:52-69): equirectangular (u, v) of the direction in the
+// reference's float/double mix, nearest texel, v flipped (row 0 at the top).
+MD v3 sky_lookup(const DScene* S, v3 dir) {
+  const double pi = 3.14159265358979323846;
+  float u = (float)(((double)atan2f(dir.z, dir.x) + pi) / (2.0f * pi));
+  float cy = -dir.y;
+  cy = cy < -1.0f ? -1.0f : (cy > 1.0f ? 1.0f : cy);
+  float v = (float)((double)acosf(cy) / pi);
+  u = u - floorf(u);
+  v = v - floorf(v);
+  v = 1.0f - v;
+  int x = (int)(u * (float)S->sky_w) % S->sky_w;
+  int y = (int)(v * (float)S->sky_h) % S->sky_h;
+  if (x < 0) x += S->sky_w;
+  if (y < 0) y += S->sky_h;
+  const float* t = S->sky_tex + 3 * ((int64_t)y * S->sky_w + x);
+  return mk3(__ldg(t), __ldg(t + 1), __ldg(t + 2));
 }
 
 // Scene::occluded (scene.cpp:41-48)

@@ -62,6 +62,7 @@ def _setup(L):
     L.mupsi_gpu_scene_set_mean_eval.argtypes = [vp, i32, i32]
     L.mupsi_gpu_mesh_set_occlusion.argtypes = [vp, i32]
     L.mupsi_gpu_scene_set_occlusion.argtypes = [vp, i32]
+    L.mupsi_gpu_scene_set_sky_texture.argtypes = [vp, i32, i32, vp]
     return L
 
 

@@ -91,6 +91,7 @@ class Scene:
         self.eps = float(np.float32(1e-4))
         self.nearteps = float(np.float32(1e-4) * np.float32(15))
         self.sky = None              # None = no skydrome; else constant RGB radiance
+        self.sky_texture = None      # (h, w, 3) float32 skydrome image, row 0 at the top (replaces `sky`)
         self.media = []              # dicts: mean_type, center, radius, mesh, sigma, length, aniso, ppc
         self.meshes = []             # Mesh
         self.primitives = []         # dicts
@@ -168,7 +169,7 @@ class Scene:
             if key in j:
                 raise NotImplementedError(f"{key} is not part of the GPIS GPU path")
         if "skydrome" in j:
-            raise NotImplementedError("image skydromes are not supported yet; pass sky=<constant radiance>")
+            s.sky_texture = load_sky_image(_resolve(base_dir, j["skydrome"]))
         if sky is not None:
             s.sky = _rgb(sky)
         if "primitives" not in j or not isinstance(j["primitives"], list):
@@ -220,9 +221,10 @@ class Scene:
         self._keep = [media, meshes, prims]
         return d
 
-    def to_json(self, obj_paths=None):
+    def to_json(self, obj_paths=None, sky_path=None):
         """scene.json dict the reference's Controller::load accepts for this scene
-        (meshes must have been written to `obj_paths`). Returns (dict, extra_meshes):
+        (meshes must have been written to `obj_paths`, a sky texture to `sky_path`
+        with save_sky_raw). Returns (dict, extra_meshes):
         primitives the schema cannot express (non-default albedo) are returned as
         (obj_path, albedo) pairs for a harness to add."""
         j = {"width": self.width, "height": self.height, "spp": self.spp, "max_bounce": self.max_bounce,
@@ -231,6 +233,10 @@ class Scene:
              "camera": {"pos": list(self.cam_pos), "dir": list(self.cam_dir), "up": list(self.cam_up),
                         "fov": self.cam_fov}, "primitives": []}
         extra = []
+        if self.sky_texture is not None:
+            if sky_path is None:
+                raise ValueError("a sky texture needs sky_path")
+            j["skydrome"] = sky_path
         if self.media:
             if len(self.media) > 1:
                 raise ValueError("scene.json holds one gp_medium")
@@ -259,6 +265,43 @@ class Scene:
                 else:
                     j["primitives"].append({"type": "mesh", "file": obj_paths[p["mesh"]], "bsdf": names[p["bsdf"]]})
         return j, extra
+
+
+def load_sky_image(path):
+    """A skydrome image as BitmapTexture::load reads it (texture.cpp:12-50):
+    .hdr/.exr as float, other formats as 8-bit / 255, RGB, row 0 at the top.
+    Files written by save_sky_raw are read directly; everything else needs
+    OpenCV (cv2)."""
+    with open(path, "rb") as fh:
+        head = fh.read(10)
+    if head == b"MUPSI_RGBF":
+        return load_sky_raw(path)
+    import cv2
+    is_hdr = os.path.splitext(path)[1].lower() in (".hdr", ".exr")
+    img = cv2.imread(path, (cv2.IMREAD_ANYDEPTH | cv2.IMREAD_COLOR) if is_hdr else cv2.IMREAD_COLOR)
+    if img is None:
+        raise OSError(f"cannot load {path}")
+    img = cv2.cvtColor(img, cv2.COLOR_BGR2RGB)
+    return (img.astype(np.float32) if is_hdr else img.astype(np.float32) / np.float32(255.0)).copy()
+
+
+def save_sky_raw(path, img):
+    """Write a float RGB image (h, w, 3) as "MUPSI_RGBF w h\n" + float32 texels
+    (rows from the top): the format the CPU oracle's image reader takes."""
+    img = np.ascontiguousarray(img, np.float32)
+    with open(path, "wb") as fh:
+        fh.write(f"MUPSI_RGBF {img.shape[1]} {img.shape[0]}\n".encode())
+        fh.write(img.tobytes())
+
+
+def load_sky_raw(path):
+    with open(path, "rb") as fh:
+        magic, w, h = fh.readline().split()
+        if magic != b"MUPSI_RGBF":
+            raise OSError(f"{path} is not a MUPSI_RGBF image")
+        w, h = int(w), int(h)
+        data = np.frombuffer(fh.read(w * h * 12), np.float32)
+    return data.reshape(h, w, 3).copy()
 
 
 def _rgb(v):

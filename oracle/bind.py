@@ -80,6 +80,7 @@ class _Port:
         L.mo_sample_condition.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.c_void_p, _u32, C.c_void_p]
         L.mo_trace.argtypes = [C.c_void_p, C.c_int64, _i32, _i32, _i32, _f32]
         L.mo_trace_work.argtypes = [C.c_void_p, C.c_int64, _i32, _i32, _i32, _i64]
+        L.mo_scene_set_sky_texture.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
         L.mo_mlp_forward.argtypes = [_f32, _f32, _f32, C.c_float, C.c_int64, _f32, _f32]
         L.mo_mlp_grad.argtypes = [_f32, _f32, _f32, C.c_float, C.c_int64, _f32, _f32, _f64,
                                   C.POINTER(C.c_double)]
@@ -185,6 +186,14 @@ class PortOracle:
     def scene_create(self, desc):
         h = self.L.mo_scene_create(C.byref(desc))
         return h
+
+    def scene_set_sky(self, h, img):
+        """Skydrome BitmapTexture (h, w, 3) float RGB, row 0 at the top; None removes it."""
+        if img is None:
+            self.L.mo_scene_set_sky_texture(h, 0, 0, None)
+            return
+        img = np.ascontiguousarray(img, np.float32)
+        self.L.mo_scene_set_sky_texture(h, img.shape[1], img.shape[0], img.ctypes.data)
 
     def scene_free(self, h):
         self.L.mo_scene_free(h)

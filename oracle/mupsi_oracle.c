@@ -545,6 +545,9 @@ struct mo_scene {
   /* camera (camera.h:13-19) */
   v3 cpos, cdir, cup, cright, ctrue_up;
   float fov, aspect;
+  /* Skydrome(BitmapTexture) (skydrome.cpp, texture.cpp): RGB, row 0 at the top */
+  float* sky_tex;
+  int sky_w, sky_h;
 };
 
 /* Mesh::computeFaceNormals (mesh.cpp:140-154) */
@@ -647,7 +650,39 @@ void mo_scene_free(mo_scene* s) {
   free(s->prims);
   free(s->lights);
   free(s->media);
+  free(s->sky_tex);
   free(s);
+}
+
+void mo_scene_set_sky_texture(mo_scene* s, int w, int h, const float* rgb) {
+  free(s->sky_tex);
+  s->sky_tex = NULL;
+  s->sky_w = s->sky_h = 0;
+  if (w <= 0 || h <= 0 || !rgb) return;
+  s->sky_tex = (float*)malloc(sizeof(float) * 3 * (size_t)w * h);
+  memcpy(s->sky_tex, rgb, sizeof(float) * 3 * (size_t)w * h);
+  s->sky_w = w;
+  s->sky_h = h;
+}
+
+/* Skydrome::intersect (skydrome.cpp:8-17) and BitmapTexture::operator[]
+ * (texture.cpp:52-69): equirectangular (u, v) of the direction, nearest texel
+ * with v flipped (row 0 is the top). */
+static v3 sky_lookup(const mo_scene* s, v3 dir) {
+  const double pi = 3.14159265358979323846;
+  float u = (float)(((double)atan2f(dir.z, dir.x) + pi) / (2.0f * pi));
+  float cy = -dir.y;
+  cy = cy < -1.0f ? -1.0f : (cy > 1.0f ? 1.0f : cy);
+  float v = (float)((double)acosf(cy) / pi);
+  u = u - floorf(u);
+  v = v - floorf(v);
+  v = 1.0f - v;
+  int x = (int)(u * (float)s->sky_w) % s->sky_w;
+  int y = (int)(v * (float)s->sky_h) % s->sky_h;
+  if (x < 0) x += s->sky_w;
+  if (y < 0) y += s->sky_h;
+  const float* t = s->sky_tex + 3 * ((size_t)y * s->sky_w + x);
+  return (v3){t[0], t[1], t[2]};
 }
 
 /* --------------------------------------------------------- rays / BVH -- */
@@ -1460,6 +1495,8 @@ static v3 trace_sample(const mo_scene* s, int x, int y, int k, int64_t* work) {
         ray.nt = neart;
         bounce++;
         has_hit = 1;
+      } else if (s->sky_tex) {
+        emission = vadd(emission, cmul(thr, sky_lookup(s, ray.d)));
       } else if (s->d.has_sky) {
         emission = vadd(emission, cmul(thr, vload(s->d.sky)));
       }

@@ -51,6 +51,9 @@ int64_t mo_bvh_build(int64_t nv, const float* verts, int64_t nf, const int32_t* 
 typedef struct mo_scene mo_scene;
 mo_scene* mo_scene_create(const mupsi_scene_desc* desc);
 void mo_scene_free(mo_scene* s);
+/* Skydrome with a BitmapTexture (skydrome.cpp:8-17, texture.cpp:52-69): w x h
+ * RGB floats, row 0 at the top; it replaces the constant sky. w = 0 removes it. */
+void mo_scene_set_sky_texture(mo_scene* s, int w, int h, const float* rgb);
 /* bvh.cpp:197-250 / :254-300 / :302-353 on scene mesh `mesh` (object space) */
 void mo_bvh_intersect(const mo_scene* s, int mesh, int64_t n, const mupsi_ray* rays, uint32_t* out_tri,
                       float* out_tuv);

@@ -1,10 +1,15 @@
 // OpenCV stand-in for the CPU oracle (test infrastructure). Only the handful of
-// types the reference's image IO names exist; images are kept in memory, imwrite
-// writes nothing and imread returns an empty image (the oracle never loads
-// bitmaps: skies are constant and meshes carry no textures in the test scenes).
+// types the reference's image IO names exist. imwrite writes nothing; imread
+// reads one project-defined raw format and nothing else: a text header
+// "MUPSI_RGBF <width> <height>\n" followed by width * height * 3 little-endian
+// float32 values, rows from the top, RGB (the tests write skydrome images this
+// way). The pixels come back already in RGB order and cvtColor is a copy, so
+// the reference's BGR-to-RGB conversion leaves them as written.
 #ifndef MUPSI_ORACLE_CV_STUB_CORE
 #define MUPSI_ORACLE_CV_STUB_CORE
 #include <cstdint>
+#include <cstdio>
+#include <cstring>
 #include <string>
 #include <vector>
 #define CV_8UC3 16
@@ -35,7 +40,24 @@ class Mat {
 };
 enum { IMREAD_COLOR = 1, IMREAD_ANYDEPTH = 2, COLOR_BGR2RGB = 4 };
 inline bool imwrite(const std::string&, const Mat&) { return false; }
-inline Mat imread(const std::string&, int = IMREAD_COLOR) { return Mat(); }
+// The raw float format above, read only as a float image (IMREAD_ANYDEPTH).
+inline Mat imread(const std::string& path, int flags = IMREAD_COLOR) {
+  if (!(flags & IMREAD_ANYDEPTH)) return Mat();
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) return Mat();
+  char magic[16] = {0};
+  int w = 0, h = 0;
+  if (std::fscanf(f, "%15s %d %d", magic, &w, &h) != 3 || std::strcmp(magic, "MUPSI_RGBF") != 0 || w <= 0 ||
+      h <= 0 || w > (1 << 15) || h > (1 << 15) || std::fgetc(f) != '\n') {
+    std::fclose(f);
+    return Mat();
+  }
+  Mat m(h, w, CV_32FC3);
+  const size_t got = std::fread(m.buf.data(), 1, m.buf.size(), f);
+  std::fclose(f);
+  if (got != m.buf.size()) return Mat();
+  return m;
+}
 inline void cvtColor(const Mat& src, Mat& dst, int) { dst = src; }
 }  // namespace cv
 #endif

@@ -6,7 +6,8 @@ inputs and stores inputs and outputs as .npz files next to this script. The
 reference ships no tests or golden vectors, so these fixtures are what pins
 the CPU oracle (oracle/libmupsi_oracle.so) in the CPU-only test suite.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # every fixture
+    python tests/golden/make_golden.py trace_sky  # one of them
 """
 import json
 import os
@@ -44,7 +45,34 @@ def psi_sweep(R, rng):
     return out
 
 
+def trace_sky(R, td):
+    """Skydrome with a BitmapTexture: configuration 0 at 24x24, 2 passes, the
+    sky a seeded 64x32 float image the reference loads through its
+    BitmapTexture (the oracle's OpenCV stand-in reads the raw format)."""
+    sc = S.config0_scene(24, 24, 2)
+    sky = np.random.default_rng(11).uniform(0.2, 3.0, (32, 64, 3)).astype(np.float32)
+    sc.sky_texture = sky
+    skyp = os.path.join(td, "sky.hdr")
+    S.save_sky_raw(skyp, sky)
+    j, _ = sc.to_json(sky_path=skyp)
+    jp = os.path.join(td, "sky.json")
+    json.dump(j, open(jp, "w"))
+    rh = R.scene_load(jp, sky=None)
+    xs, ys, ks = np.meshgrid(np.arange(24), np.arange(24), np.arange(2), indexing="ij")
+    xs, ys, ks = xs.ravel().astype(np.int32), ys.ravel().astype(np.int32), ks.ravel().astype(np.int32)
+    rad = R.trace(rh, xs, ys, ks)
+    # the texture was loaded (a failed load shows magenta (1, 0, 1))
+    assert len(np.unique(rad[:, 0])) > 100 and not np.all(rad[:, 1] == 0)
+    np.savez_compressed(os.path.join(OUT, "trace_sky.npz"), x=xs, y=ys, k=ks, radiance=rad, sky=sky)
+
+
 def main():
+    if len(sys.argv) > 1:
+        with tempfile.TemporaryDirectory() as td:
+            for name in sys.argv[1:]:
+                globals()[name](bind.RefOracle("ref"), td)
+        print("fixtures written to", OUT)
+        return
     R = bind.RefOracle("ref")
     rng = np.random.default_rng(20261203)
     data = {}
@@ -151,6 +179,7 @@ def main():
     xs, ys, ks = xs.ravel().astype(np.int32), ys.ravel().astype(np.int32), ks.ravel().astype(np.int32)
     rad = R.trace(rh, xs, ys, ks)
     np.savez_compressed(os.path.join(OUT, "trace_mesh.npz"), x=xs, y=ys, k=ks, radiance=rad)
+    trace_sky(R, td)
     print("fixtures written to", OUT)
 
 

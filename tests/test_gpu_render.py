@@ -38,6 +38,30 @@ def test_trace_fixture_mesh(gpu, golden):
     assert same.mean() >= 0.97, same.mean()
 
 
+def test_trace_fixture_sky_texture(gpu, golden):
+    """Escaping paths read the skydrome BitmapTexture (skydrome.cpp,
+    texture.cpp); the fixture is the reference's trace on the same image."""
+    g = golden("trace_sky.npz")
+    sc = S.config0_scene(24, 24, 2)
+    sc.sky_texture = g["sky"]
+    gs = GpuScene(sc)
+    rad = gs.trace(g["x"], g["y"], g["k"])
+    same = np.all(bits(rad) == bits(g["radiance"]), axis=1)
+    assert same.mean() >= 0.97, same.mean()
+    r = GpuRenderer()
+    r.prepare_render(gs)
+    fb = r.start_render_progressive(2)
+    rr = g["radiance"].reshape(24, 24, 2, 3)
+    ref = ((rr[:, :, 0] + rr[:, :, 1]).astype(np.float32) * np.float32(0.5)).transpose(1, 0, 2)
+    ok = np.all(bits(fb) == bits(ref), axis=2)
+    assert ok.mean() >= 0.95, ok.mean()
+    gs.set_sky_texture(None)  # back to the scene's constant skydrome
+    rad0 = gs.trace(g["x"], g["y"], g["k"])
+    plain = GpuScene(S.config0_scene(24, 24, 2)).trace(g["x"], g["y"], g["k"])
+    assert np.array_equal(bits(rad0), bits(plain))
+    assert not np.array_equal(bits(rad0), bits(rad))
+
+
 @pytest.mark.parametrize("mode", ["renewal_plus", "single_realization"])
 def test_trace_replay_vs_oracle(gpu, port, mode):
     sc = S.config0_scene(48, 48, 4)
