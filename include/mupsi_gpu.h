@@ -371,6 +371,21 @@ int mupsi_gpu_scene_set_surrogate(mupsi_scene* scene, int32_t medium, mupsi_mlp*
  * of the descriptor. width = height = 0 removes it. */
 int mupsi_gpu_scene_set_sky_texture(mupsi_scene* scene, int32_t width, int32_t height, const float* rgb);
 
+/* Lambertian BSDF with a BitmapTexture albedo on mesh primitive `primitive`
+ * (controller.cpp:240-243, bsdf.cpp:14-37): the albedo at a hit is the nearest
+ * texel (texture.cpp:52-69) at the hit's texture coordinate, which is the
+ * mesh's OBJ texcoords interpolated with the hit's barycentrics
+ * (mesh.cpp:175-181, 232), or the barycentrics themselves when num_texcoords
+ * is 0 (an OBJ without vt lines). texcoords: [num_texcoords*2] (u, v);
+ * face_texcoords: [num_faces*3] 0-based indices into texcoords, one triple per
+ * face of the primitive's mesh; rgb: width x height texels of 3 floats, row 0
+ * at the top. Host memory, copied. width = height = 0 removes the texture (the
+ * descriptor's constant albedo applies again). MUPSI_ERR_INVALID for a sphere
+ * or a non-Lambertian primitive and for indices out of range. */
+int mupsi_gpu_scene_set_albedo_texture(mupsi_scene* scene, int32_t primitive, int64_t num_texcoords,
+                                       const float* texcoords, const int32_t* face_texcoords, int32_t width,
+                                       int32_t height, const float* rgb);
+
 /* How a march evaluates a mesh mean (no reference counterpart: the reference
  * evaluates mu at every step, GPMedium::evalWithGradient per step,
  * medium/gpmedium.cpp:46-103). LAZY (the default) keeps the last exact value

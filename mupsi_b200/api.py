@@ -257,6 +257,10 @@ class GpuScene:
         self.h = h
         if getattr(scene, "sky_texture", None) is not None:
             self.set_sky_texture(scene.sky_texture)
+        for i, p in enumerate(scene.primitives):
+            if p.get("texture") is not None:
+                m = scene.meshes[p["mesh"]]
+                self.set_albedo_texture(i, p["texture"], m.texcoords, m.face_texcoords)
 
     def close(self):
         if self.h:
@@ -339,6 +343,25 @@ class GpuScene:
             return
         img = np.ascontiguousarray(img, np.float32)
         check(load().mupsi_gpu_scene_set_sky_texture(self.h, img.shape[1], img.shape[0], img.ctypes.data))
+
+    def set_albedo_texture(self, primitive, img, texcoords=None, face_texcoords=None):
+        """Lambertian BitmapTexture albedo of a mesh primitive: (h, w, 3) float
+        RGB, row 0 at the top, at the mesh's texcoords (T, 2) indexed per face
+        by face_texcoords (F, 3), or at the hit's barycentrics when texcoords is
+        None. img None removes it."""
+        if img is None:
+            check(load().mupsi_gpu_scene_set_albedo_texture(self.h, primitive, 0, None, None, 0, 0, None))
+            return
+        img = np.ascontiguousarray(img, np.float32)
+        if texcoords is None:
+            n, tc, ft = 0, None, None
+        else:
+            tc = np.ascontiguousarray(texcoords, np.float32).reshape(-1, 2)
+            ft = np.ascontiguousarray(face_texcoords, np.int32).reshape(-1, 3)
+            n = len(tc)
+        check(load().mupsi_gpu_scene_set_albedo_texture(
+            self.h, primitive, n, None if tc is None else tc.ctypes.data, None if ft is None else ft.ctypes.data,
+            img.shape[1], img.shape[0], img.ctypes.data))
 
     def set_occlusion(self, from_root):
         """Shadow rays: BVH::occluded from node 0 as the reference (default) or from the root."""

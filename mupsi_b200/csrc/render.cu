@@ -418,18 +418,19 @@ __global__ void __launch_bounds__(128) k_shade(const DScene* const* __restrict__
       if (hi.prim >= 0) {
         const DPrim& pr = S->prims[hi.prim];
         v3 wo = -ray.d, N = hi.Ng;
+        const v3 alb = pr.tex ? tex_lookup(pr.tex, pr.tex_w, pr.tex_h, hi.tu, hi.tv) : pr.albedo;
         LSample ls;
         if (choose_light(S, hi.p, rng, ls)) {  // handleSurface NEE (trace.cpp:40-56)
           Ray sr = make_ray(hi.p + N * S->eps, ls.d);
           float bias = ls.dist - S->eps * fabsf(dot(ls.d, N));
           sr.ft = bias * 0.99f;
           if (!scene_occluded(S, sr, ovf)) {
-            v3 a = bsdf_weight(pr.bsdf, pr.albedo, ls.d, wo, N);
+            v3 a = bsdf_weight(pr.bsdf, alb, ls.d, wo, N);
             em = em + cmul(thr, cmul(a, ls.weight)) * fabsf(dot(ls.d, N));
           }
         }
         v3 w;
-        v3 wi = bsdf_sample(pr.bsdf, pr.albedo, wo, N, rng, w);
+        v3 wi = bsdf_sample(pr.bsdf, alb, wo, N, rng, w);
         if (pr.has_emission) em = em + cmul(thr, pr.emission * fmax_std(0.0f, dot(N, wi)));
         thr = cmul(thr, w);
         float surv = maxc(thr);
@@ -630,6 +631,7 @@ struct mupsi_scene {
   PathBuf pb;  // wave buffers (grow-only)
   mupsi_mlp* surr_mlp = nullptr;  // surrogate of a mesh mean (not owned)
   void* sky_mem = nullptr;        // sky texture texels (owned)
+  void* tex_mem[MAX_PRIMS] = {};  // albedo texture texels + texcoords per primitive (owned)
   int surr_rounds = 1;            // march rounds per bounce iteration with it: predictions + 1
   int* err = nullptr;
   unsigned long long* counters = nullptr;
@@ -707,6 +709,8 @@ mupsi_scene::~mupsi_scene() {
     if (d_list) cudaFree(d_list);
     if (d_chunk) cudaFree(d_chunk);
     if (sky_mem) cudaFree(sky_mem);
+    for (void* p : tex_mem)
+      if (p) cudaFree(p);
     if (sum) cudaFree(sum);
     if (pb.mem) pool_give(pb.mem, pb.bytes);
     if (err) cudaFree(err);
@@ -1860,6 +1864,61 @@ int mupsi_gpu_scene_set_sky_texture(mupsi_scene* scene, int32_t width, int32_t h
     scene->h.sky_tex = static_cast<const float*>(scene->sky_mem);
     scene->h.sky_w = width;
     scene->h.sky_h = height;
+  }
+  MUPSI_CUDA(cudaMemcpy(scene->d, &scene->h, sizeof(DScene), cudaMemcpyHostToDevice));
+  return MUPSI_OK;
+}
+
+int mupsi_gpu_scene_set_albedo_texture(mupsi_scene* scene, int32_t primitive, int64_t num_texcoords,
+                                       const float* texcoords, const int32_t* face_texcoords, int32_t width,
+                                       int32_t height, const float* rgb) {
+  clear_error();
+  if (!scene) return fail(MUPSI_ERR_INVALID, "null scene");
+  if (primitive < 0 || primitive >= scene->h.nprim) return fail(MUPSI_ERR_INVALID, "primitive out of range");
+  DPrim& p = scene->h.prims[primitive];
+  if (p.type != MUPSI_PRIM_MESH) return fail(MUPSI_ERR_INVALID, "albedo textures are on mesh primitives");
+  if (p.bsdf != MUPSI_BSDF_LAMBERTIAN) return fail(MUPSI_ERR_INVALID, "albedo textures need a Lambertian BSDF");
+  if (width < 0 || height < 0 || width > (1 << 15) || height > (1 << 15))
+    return fail(MUPSI_ERR_INVALID, "albedo texture size out of range");
+  if ((width == 0) != (height == 0)) return fail(MUPSI_ERR_INVALID, "albedo texture needs width and height");
+  const int64_t nf = scene->h.meshes[p.mesh].num_faces;
+  if (width > 0) {
+    if (!rgb) return fail(MUPSI_ERR_INVALID, "null albedo texels");
+    if (num_texcoords < 0 || num_texcoords > (int64_t(1) << 28)) return fail(MUPSI_ERR_INVALID, "bad texcoord count");
+    if (num_texcoords > 0) {
+      if (!texcoords || !face_texcoords) return fail(MUPSI_ERR_INVALID, "null texcoords");
+      for (int64_t i = 0; i < 3 * nf; ++i)
+        if (face_texcoords[i] < 0 || face_texcoords[i] >= num_texcoords)
+          return fail(MUPSI_ERR_INVALID, "face texcoord index out of range");
+    }
+  }
+  MUPSI_CUDA(cudaDeviceSynchronize());
+  if (scene->tex_mem[primitive]) {
+    cudaFree(scene->tex_mem[primitive]);
+    scene->tex_mem[primitive] = nullptr;
+  }
+  p.tex = nullptr;
+  p.uvs = nullptr;
+  p.face_uv = nullptr;
+  p.tex_w = p.tex_h = 0;
+  if (width > 0) {
+    auto up16 = [](size_t b) { return (b + 15) & ~size_t(15); };
+    const size_t tb = up16((size_t)width * height * 3 * sizeof(float));
+    const size_t ub = num_texcoords > 0 ? up16((size_t)num_texcoords * 2 * sizeof(float)) : 0;
+    const size_t fb = num_texcoords > 0 ? (size_t)nf * 3 * sizeof(int32_t) : 0;
+    char* mem = nullptr;
+    MUPSI_CUDA(cudaMalloc(&mem, tb + ub + fb));
+    scene->tex_mem[primitive] = mem;
+    MUPSI_CUDA(cudaMemcpy(mem, rgb, (size_t)width * height * 3 * sizeof(float), cudaMemcpyHostToDevice));
+    p.tex = reinterpret_cast<const float*>(mem);
+    p.tex_w = width;
+    p.tex_h = height;
+    if (num_texcoords > 0) {
+      MUPSI_CUDA(cudaMemcpy(mem + tb, texcoords, (size_t)num_texcoords * 2 * sizeof(float), cudaMemcpyHostToDevice));
+      MUPSI_CUDA(cudaMemcpy(mem + tb + ub, face_texcoords, fb, cudaMemcpyHostToDevice));
+      p.uvs = reinterpret_cast<const float*>(mem + tb);
+      p.face_uv = reinterpret_cast<const int32_t*>(mem + tb + ub);
+    }
   }
   MUPSI_CUDA(cudaMemcpy(scene->d, &scene->h, sizeof(DScene), cudaMemcpyHostToDevice));
   return MUPSI_OK;

@@ -17,6 +17,14 @@ struct DPrim {
   int int_medium, ext_medium;
   int identity;
   m4 T, Tinv;
+  // Lambertian BitmapTexture albedo of a mesh primitive (nullable; replaces
+  // `albedo`): RGB texels, row 0 at the top, looked up at the hit's texture
+  // coordinate: the mesh's texcoords `uvs` [n*2] interpolated over the face's
+  // `face_uv` [F*3], or the hit's barycentrics when `uvs` is null
+  const float* tex;
+  const float* uvs;
+  const int32_t* face_uv;
+  int tex_w, tex_h;
 };
 struct DMedium {
   int mean_type;
@@ -685,6 +693,7 @@ struct Hit {
   int prim;
   float t;
   v3 p, Ng;
+  float tu, tv;  // texture coordinate (only for a primitive with an albedo texture)
 };
 
 // Scene::intersect (scene.cpp:25-39) with Sphere/Mesh intersect and intersectInfo
@@ -758,9 +767,38 @@ MD Hit scene_intersect(const DScene* S, Ray& r, bool& ovf) {
         ln = len > 1e-12f ? n / len : ld3(m.face_n + 3 * (int64_t)tri);
       }
       hi.Ng = p.identity ? ln : normalized(apply3t(p.Tinv, ln));
+      if (p.tex) {  // Mesh::interpolateTexcoord (mesh.cpp:175-181)
+        if (!p.uvs) {
+          hi.tu = bu;
+          hi.tv = bv;
+        } else {
+          const int32_t* ft = p.face_uv + 3 * (int64_t)tri;
+          const float* t0 = p.uvs + 2 * (int64_t)ft[0];
+          const float* t1 = p.uvs + 2 * (int64_t)ft[1];
+          const float* t2 = p.uvs + 2 * (int64_t)ft[2];
+          float w = 1.0f - bu - bv;
+          hi.tu = (w * t0[0] + bu * t1[0]) + bv * t2[0];
+          hi.tv = (w * t0[1] + bu * t1[1]) + bv * t2[1];
+        }
+      }
     }
   }
   return hi;
+}
+
+// BitmapTexture::operator[] (texture.cpp:52-69): wrap (u, v) to [0, 1), flip v
+// (row 0 is the top), nearest texel. Every int the casts produce lands inside
+// the image after the modulo.
+MD v3 tex_lookup(const float* tex, int w, int h, float u, float v) {
+  u = u - floorf(u);
+  v = v - floorf(v);
+  v = 1.0f - v;
+  int x = (int)(u * (float)w) % w;
+  int y = (int)(v * (float)h) % h;
+  if (x < 0) x += w;
+  if (y < 0) y += h;
+  const float* t = tex + 3 * ((int64_t)y * w + x);
+  return mk3(__ldg(t), __ldg(t + 1), __ldg(t + 2));
 }
 
 // Skydrome::intersect (skydrome.cpp:8-17) + BitmapTexture::operator[]
@@ -772,15 +810,7 @@ MD v3 sky_lookup(const DScene* S, v3 dir) {
   float cy = -dir.y;
   cy = cy < -1.0f ? -1.0f : (cy > 1.0f ? 1.0f : cy);
   float v = (float)((double)acosf(cy) / pi);
-  u = u - floorf(u);
-  v = v - floorf(v);
-  v = 1.0f - v;
-  int x = (int)(u * (float)S->sky_w) % S->sky_w;
-  int y = (int)(v * (float)S->sky_h) % S->sky_h;
-  if (x < 0) x += S->sky_w;
-  if (y < 0) y += S->sky_h;
-  const float* t = S->sky_tex + 3 * ((int64_t)y * S->sky_w + x);
-  return mk3(__ldg(t), __ldg(t + 1), __ldg(t + 2));
+  return tex_lookup(S->sky_tex, S->sky_w, S->sky_h, u, v);
 }
 
 // Scene::occluded (scene.cpp:41-48)

@@ -63,6 +63,7 @@ def _setup(L):
     L.mupsi_gpu_mesh_set_occlusion.argtypes = [vp, i32]
     L.mupsi_gpu_scene_set_occlusion.argtypes = [vp, i32]
     L.mupsi_gpu_scene_set_sky_texture.argtypes = [vp, i32, i32, vp]
+    L.mupsi_gpu_scene_set_albedo_texture.argtypes = [vp, i32, i64, vp, vp, i32, i32, vp]
     return L
 
 

@@ -20,13 +20,25 @@ DEFAULT_ALBEDO = 0.8  # Bsdf::default_albedo_ (bsdf/bsdf.cpp:11)
 class Mesh:
     """Triangle mesh (primitives/mesh.h): object-space vertices/faces + T*S transform."""
 
-    def __init__(self, vertices, faces, vertex_normals=None, position=(0.0, 0.0, 0.0), scale=1.0):
+    def __init__(self, vertices, faces, vertex_normals=None, position=(0.0, 0.0, 0.0), scale=1.0, texcoords=None,
+                 face_texcoords=None):
         self.vertices = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
         self.faces = np.ascontiguousarray(faces, dtype=np.int32).reshape(-1, 3)
         self.vertex_normals = (None if vertex_normals is None else
                                np.ascontiguousarray(vertex_normals, dtype=np.float32).reshape(-1, 3))
         self.position = tuple(float(v) for v in position)
         self.scale = float(scale)
+        # OBJ texture coordinates (vt) and per-face indices into them; None:
+        # a textured primitive reads its texture at the hit's barycentrics
+        self.texcoords = None if texcoords is None else np.ascontiguousarray(texcoords, np.float32).reshape(-1, 2)
+        self.face_texcoords = (None if face_texcoords is None else
+                               np.ascontiguousarray(face_texcoords, np.int32).reshape(-1, 3))
+        if (self.texcoords is None) != (self.face_texcoords is None):
+            raise ValueError("texcoords and face_texcoords go together")
+        if self.face_texcoords is not None and (len(self.face_texcoords) != len(self.faces) or (
+                self.face_texcoords.size and (self.face_texcoords.min() < 0 or
+                                              self.face_texcoords.max() >= len(self.texcoords)))):
+            raise ValueError("face_texcoords must index texcoords, one triple per face")
 
     def desc(self):
         return _abi.MeshDesc(
@@ -35,11 +47,19 @@ class Mesh:
             _abi.f3(*self.position), self.scale)
 
 
-def load_obj(path):
+def load_obj(path, texcoords=False):
     """OBJ reader following Mesh::fetchFrom (primitives/mesh.cpp:20-136): v, vn,
     vt, triangular f in v, v/vt, v//vn, v/vt/vn forms, 1-based or negative indices;
-    faces with other vertex counts are skipped."""
-    verts, normals, faces = [], [], []
+    faces with other vertex counts are skipped. Returns (vertices, faces,
+    normals), plus (texcoords, face_texcoords) with texcoords=True: None, None
+    for a file without vt lines (interpolateTexcoord then yields the
+    barycentrics, mesh.cpp:175-177); a face corner without a vt index takes
+    texcoord 0, as normIdx maps index 0 there."""
+    verts, normals, faces, tcs, ftcs = [], [], [], [], []
+
+    def norm_idx(i, count):
+        return i - 1 if i > 0 else (count + i if i < 0 else 0)
+
     with open(path) as fh:
         for line in fh:
             line = line.rstrip("\r\n")
@@ -53,25 +73,47 @@ def load_obj(path):
                 verts.append([float(v) for v in parts[1:4]])
             elif t == "vn":
                 normals.append([float(v) for v in parts[1:4]])
+            elif t == "vt":
+                tcs.append([float(v) for v in parts[1:3]])
             elif t == "f":
-                idx = []
+                idx, tidx = [], []
                 for spec in parts[1:]:
-                    vi = int(spec.split("/")[0])
-                    idx.append(vi - 1 if vi > 0 else (len(verts) + vi if vi < 0 else 0))
+                    fields = spec.split("/")
+                    vi = int(fields[0])
+                    ti = int(fields[1]) if len(fields) > 1 and fields[1] else 0
+                    idx.append(norm_idx(vi, len(verts)))
+                    tidx.append(norm_idx(ti, len(tcs)))
                 if len(idx) == 3:
                     faces.append(idx)
+                    ftcs.append(tidx)
     if not verts or not faces:
         raise ValueError(f"{path}: no valid geometry")
-    return np.array(verts, np.float32), np.array(faces, np.int32), (np.array(normals, np.float32) if normals else None)
+    out = (np.array(verts, np.float32), np.array(faces, np.int32), (np.array(normals, np.float32) if normals else None))
+    if not texcoords:
+        return out
+    if not tcs:
+        return out + (None, None)
+    ft = np.array(ftcs, np.int32)
+    if ft.min() < 0 or ft.max() >= len(tcs):
+        raise ValueError(f"{path}: texcoord index out of range")
+    return out + (np.array(tcs, np.float32), ft)
 
 
-def save_obj(path, vertices, faces):
-    """Write a mesh as OBJ (vertices at full float32 precision, 1-based faces)."""
+def save_obj(path, vertices, faces, texcoords=None, face_texcoords=None):
+    """Write a mesh as OBJ (vertices and texcoords at full float32 precision,
+    1-based faces, v/vt corners when texcoords are given)."""
     v = np.asarray(vertices, np.float32)
     f = np.asarray(faces, np.int64) + 1
     with open(path, "w") as fh:
         fh.write("".join("v %.9g %.9g %.9g\n" % tuple(r) for r in v.tolist()))
-        fh.write("".join("f %d %d %d\n" % tuple(r) for r in f.tolist()))
+        if texcoords is None:
+            fh.write("".join("f %d %d %d\n" % tuple(r) for r in f.tolist()))
+        else:
+            t = np.asarray(texcoords, np.float32).reshape(-1, 2)
+            ft = np.asarray(face_texcoords, np.int64).reshape(-1, 3) + 1
+            fh.write("".join("vt %.9g %.9g\n" % tuple(r) for r in t.tolist()))
+            fh.write("".join("f %d/%d %d/%d %d/%d\n" % (a, ta, b, tb, c, tc)
+                             for (a, b, c), (ta, tb, tc) in zip(f.tolist(), ft.tolist())))
 
 
 class Scene:
@@ -116,10 +158,18 @@ class Scene:
                                     ext_medium=ext_medium))
 
     def add_mesh_primitive(self, mesh_index, bsdf=_abi.BSDF_LAMBERTIAN, albedo=DEFAULT_ALBEDO, emission=None,
-                           int_medium=-1, ext_medium=-1):
+                           int_medium=-1, ext_medium=-1, texture=None):
+        """texture: (h, w, 3) float RGB albedo image (row 0 at the top) of a
+        Lambertian mesh, read at the mesh's texcoords; replaces `albedo`."""
+        if texture is not None:
+            if bsdf != _abi.BSDF_LAMBERTIAN:
+                raise ValueError("albedo textures need a Lambertian BSDF")
+            texture = np.ascontiguousarray(texture, np.float32)
+            if texture.ndim != 3 or texture.shape[2] != 3 or texture.shape[0] < 1 or texture.shape[1] < 1:
+                raise ValueError("texture must be (h, w, 3)")
         self.primitives.append(dict(type=_abi.PRIM_MESH, center=(0, 0, 0), radius=1.0, mesh=mesh_index, bsdf=bsdf,
                                     albedo=_rgb(albedo), emission=emission, int_medium=int_medium,
-                                    ext_medium=ext_medium))
+                                    ext_medium=ext_medium, texture=texture))
 
     # -- scene.json (controller.cpp:40-264) ------------------------------------
     @classmethod
@@ -169,7 +219,7 @@ class Scene:
             if key in j:
                 raise NotImplementedError(f"{key} is not part of the GPIS GPU path")
         if "skydrome" in j:
-            s.sky_texture = load_sky_image(_resolve(base_dir, j["skydrome"]))
+            s.sky_texture = load_texture_image(_resolve(base_dir, j["skydrome"]))
         if sky is not None:
             s.sky = _rgb(sky)
         if "primitives" not in j or not isinstance(j["primitives"], list):
@@ -183,12 +233,14 @@ class Scene:
                 s.add_sphere(pj["center"], pj.get("radius", 100.0), bsdf=bsdf, emission=em,
                              int_medium=gpm_index if "int_medium" in pj else -1)
             elif typ == "mesh":
-                if "texture" in pj:
-                    raise NotImplementedError("bitmap textures are not supported yet")
-                v, f, n = load_obj(_resolve(base_dir, pj["file"]))
+                tex = None
+                if "texture" in pj and pj.get("bsdf", "lambertian") == "lambertian":  # controller.cpp:240-243
+                    tex = load_texture_image(_resolve(base_dir, pj["texture"]))
+                v, f, n, tc, ftc = load_obj(_resolve(base_dir, pj["file"]), texcoords=True)
                 t = pj.get("transform", {})
-                mi = s.add_mesh(Mesh(v, f, n, position=t.get("position", (0, 0, 0)), scale=t.get("scale", 1.0)))
-                s.add_mesh_primitive(mi, bsdf=bsdf)
+                mi = s.add_mesh(Mesh(v, f, n, position=t.get("position", (0, 0, 0)), scale=t.get("scale", 1.0),
+                                     texcoords=tc, face_texcoords=ftc))
+                s.add_mesh_primitive(mi, bsdf=bsdf, texture=tex)
             # unknown primitive types are skipped, as the reference does
         return s
 
@@ -221,12 +273,13 @@ class Scene:
         self._keep = [media, meshes, prims]
         return d
 
-    def to_json(self, obj_paths=None, sky_path=None):
+    def to_json(self, obj_paths=None, sky_path=None, texture_paths=None):
         """scene.json dict the reference's Controller::load accepts for this scene
-        (meshes must have been written to `obj_paths`, a sky texture to `sky_path`
-        with save_sky_raw). Returns (dict, extra_meshes):
-        primitives the schema cannot express (non-default albedo) are returned as
-        (obj_path, albedo) pairs for a harness to add."""
+        (meshes must have been written to `obj_paths` with their texcoords, a sky
+        texture to `sky_path` and albedo textures to `texture_paths`, a dict
+        primitive index -> path, with save_image_raw). Returns (dict,
+        extra_meshes): primitives the schema cannot express (non-default
+        albedo) are returned as (obj_path, albedo) pairs for a harness to add."""
         j = {"width": self.width, "height": self.height, "spp": self.spp, "max_bounce": self.max_bounce,
              "max_medium_bounce": self.max_medium_bounce,
              "gp_mode": "renewal_plus" if self.gp_mode == _abi.GP_RENEWAL_PLUS else "single_realization",
@@ -250,7 +303,7 @@ class Scene:
                 j["gp_medium"] = {"mean_type": "mesh", "file": obj_paths[m["mesh"]],
                                   "transform": {"position": list(mm.position), "scale": mm.scale}}
         names = {_abi.BSDF_LAMBERTIAN: "lambertian", _abi.BSDF_NULL: "null", _abi.BSDF_SPECULAR: "specular"}
-        for p in self.primitives:
+        for pi, p in enumerate(self.primitives):
             if p["type"] == _abi.PRIM_SPHERE:
                 pj = {"type": "sphere", "center": list(p["center"]), "radius": p["radius"], "bsdf": names[p["bsdf"]]}
                 if p["emission"] is not None:
@@ -260,24 +313,36 @@ class Scene:
                 j["primitives"].append(pj)
             else:
                 mm = self.meshes[p["mesh"]]
-                if p["albedo"] != _rgb(DEFAULT_ALBEDO) or mm.position != (0, 0, 0) or mm.scale != 1.0:
+                tex = p.get("texture")
+                if tex is None and (p["albedo"] != _rgb(DEFAULT_ALBEDO) or mm.position != (0, 0, 0) or
+                                    mm.scale != 1.0):
                     extra.append((obj_paths[p["mesh"]], p["albedo"][0]))
                 else:
-                    j["primitives"].append({"type": "mesh", "file": obj_paths[p["mesh"]], "bsdf": names[p["bsdf"]]})
+                    pj = {"type": "mesh", "file": obj_paths[p["mesh"]], "bsdf": names[p["bsdf"]]}
+                    if tex is not None:
+                        pj["texture"] = texture_paths[pi]
+                        if mm.position != (0, 0, 0) or mm.scale != 1.0:
+                            pj["transform"] = {"position": list(mm.position), "scale": mm.scale}
+                    j["primitives"].append(pj)
         return j, extra
 
 
-def load_sky_image(path):
-    """A skydrome image as BitmapTexture::load reads it (texture.cpp:12-50):
-    .hdr/.exr as float, other formats as 8-bit / 255, RGB, row 0 at the top.
-    Files written by save_sky_raw are read directly; everything else needs
-    OpenCV (cv2)."""
+def load_texture_image(path):
+    """An image as BitmapTexture::load reads it (texture.cpp:12-50): .hdr/.exr
+    as float, other formats as 8-bit / 255, RGB, row 0 at the top. Files
+    written by save_image_raw are read directly (a float one only under a
+    .hdr/.exr name, as the reference asks for float pixels only there);
+    everything else needs OpenCV (cv2)."""
     with open(path, "rb") as fh:
         head = fh.read(10)
+    is_hdr = os.path.splitext(path)[1] in (".hdr", ".exr")
     if head == b"MUPSI_RGBF":
-        return load_sky_raw(path)
+        if not is_hdr:
+            raise OSError(f"{path}: a float image needs a .hdr or .exr name")
+        return load_image_raw(path)
+    if head == b"MUPSI_RGB8":
+        return (load_image_raw(path).astype(np.float32) / np.float32(255.0)).astype(np.float32)
     import cv2
-    is_hdr = os.path.splitext(path)[1].lower() in (".hdr", ".exr")
     img = cv2.imread(path, (cv2.IMREAD_ANYDEPTH | cv2.IMREAD_COLOR) if is_hdr else cv2.IMREAD_COLOR)
     if img is None:
         raise OSError(f"cannot load {path}")
@@ -285,23 +350,38 @@ def load_sky_image(path):
     return (img.astype(np.float32) if is_hdr else img.astype(np.float32) / np.float32(255.0)).copy()
 
 
-def save_sky_raw(path, img):
-    """Write a float RGB image (h, w, 3) as "MUPSI_RGBF w h\n" + float32 texels
-    (rows from the top): the format the CPU oracle's image reader takes."""
-    img = np.ascontiguousarray(img, np.float32)
+def save_image_raw(path, img):
+    """Write an RGB image (h, w, 3), rows from the top, in the raw formats the
+    CPU oracle's image reader takes: float32 texels after "MUPSI_RGBF w h\n",
+    or uint8 texels after "MUPSI_RGB8 w h\n" for a uint8 array."""
+    img = np.asarray(img)
+    if img.dtype != np.uint8:
+        img = img.astype(np.float32)
+    img = np.ascontiguousarray(img)
+    magic = "MUPSI_RGB8" if img.dtype == np.uint8 else "MUPSI_RGBF"
     with open(path, "wb") as fh:
-        fh.write(f"MUPSI_RGBF {img.shape[1]} {img.shape[0]}\n".encode())
+        fh.write(f"{magic} {img.shape[1]} {img.shape[0]}\n".encode())
         fh.write(img.tobytes())
 
 
-def load_sky_raw(path):
+def load_image_raw(path):
+    """Read save_image_raw's formats: float32 or uint8 (h, w, 3)."""
     with open(path, "rb") as fh:
         magic, w, h = fh.readline().split()
-        if magic != b"MUPSI_RGBF":
-            raise OSError(f"{path} is not a MUPSI_RGBF image")
+        if magic not in (b"MUPSI_RGBF", b"MUPSI_RGB8"):
+            raise OSError(f"{path} is not a raw MUPSI image")
         w, h = int(w), int(h)
-        data = np.frombuffer(fh.read(w * h * 12), np.float32)
+        dt = np.float32 if magic == b"MUPSI_RGBF" else np.uint8
+        n = w * h * 3
+        data = np.frombuffer(fh.read(n * np.dtype(dt).itemsize), dt)
+    if data.size != n:
+        raise OSError(f"{path}: truncated")
     return data.reshape(h, w, 3).copy()
+
+
+# the skydrome reads its image through the same BitmapTexture
+load_sky_image = load_texture_image
+save_sky_raw = save_image_raw
 
 
 def _rgb(v):
@@ -416,6 +496,24 @@ def config0_scene(width=256, height=256, spp=20):
                      points_per_cell=3)
     s.add_sphere((0, 0, -500), 130.0, bsdf=_abi.BSDF_NULL, int_medium=m)
     return s
+
+
+def textured_floor_scene(texture, with_texcoords=True, width=24, height=24, spp=2):
+    """Configuration 0 plus an emissive Lambertian sphere (a light for
+    next-event estimation) and the floor quad under a Lambertian BitmapTexture
+    albedo `texture` ((h, w, 3) float RGB, row 0 at the top): at texcoords from
+    -0.75 to 3.5, so the lookup wraps, or, without texcoords, at the hit's
+    barycentrics. The floor is primitive 2."""
+    sc = config0_scene(width, height, spp)
+    sc.add_sphere((40.0, 160.0, -380.0), 45.0, emission=(6.0, 5.0, 4.0))
+    fv, ff = floor_quad()
+    tc = ftc = None
+    if with_texcoords:
+        tc = np.array([[-0.75, -0.5], [3.5, -0.5], [3.5, 2.25], [-0.75, 2.25]], np.float32)
+        ftc = ff.copy()
+    fm = sc.add_mesh(Mesh(fv, ff, texcoords=tc, face_texcoords=ftc))
+    sc.add_mesh_primitive(fm, texture=texture)
+    return sc
 
 
 def config_mesh_scene(level=6, width=512, height=512, spp=64, seed=0):

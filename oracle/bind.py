@@ -81,6 +81,8 @@ class _Port:
         L.mo_trace.argtypes = [C.c_void_p, C.c_int64, _i32, _i32, _i32, _f32]
         L.mo_trace_work.argtypes = [C.c_void_p, C.c_int64, _i32, _i32, _i32, _i64]
         L.mo_scene_set_sky_texture.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        L.mo_scene_set_albedo_texture.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.c_void_p, C.c_void_p, C.c_int,
+                                                  C.c_int, C.c_void_p]
         L.mo_mlp_forward.argtypes = [_f32, _f32, _f32, C.c_float, C.c_int64, _f32, _f32]
         L.mo_mlp_grad.argtypes = [_f32, _f32, _f32, C.c_float, C.c_int64, _f32, _f32, _f64,
                                   C.POINTER(C.c_double)]
@@ -194,6 +196,36 @@ class PortOracle:
             return
         img = np.ascontiguousarray(img, np.float32)
         self.L.mo_scene_set_sky_texture(h, img.shape[1], img.shape[0], img.ctypes.data)
+
+    def scene_set_albedo(self, h, prim, img, texcoords=None, face_texcoords=None):
+        """LambertianBsdf(BitmapTexture) on a mesh primitive: (h, w, 3) float RGB
+        at the mesh's texcoords (None: the barycentrics); None removes it."""
+        if img is None:
+            rc = self.L.mo_scene_set_albedo_texture(h, prim, 0, None, None, 0, 0, None)
+        else:
+            img = np.ascontiguousarray(img, np.float32)
+            if texcoords is None:
+                n, tc, ft = 0, None, None
+            else:
+                tc = np.ascontiguousarray(texcoords, np.float32).reshape(-1, 2)
+                ft = np.ascontiguousarray(face_texcoords, np.int32).reshape(-1, 3)
+                n = len(tc)
+            rc = self.L.mo_scene_set_albedo_texture(h, prim, n, None if tc is None else tc.ctypes.data,
+                                                    None if ft is None else ft.ctypes.data, img.shape[1],
+                                                    img.shape[0], img.ctypes.data)
+        if rc != 0:
+            raise ValueError("bad albedo texture arguments")
+
+    def scene_from(self, sc):
+        """scene_create(sc.desc()) plus the scene's sky and albedo textures."""
+        h = self.scene_create(sc.desc())
+        if getattr(sc, "sky_texture", None) is not None:
+            self.scene_set_sky(h, sc.sky_texture)
+        for i, p in enumerate(sc.primitives):
+            if p.get("texture") is not None:
+                m = sc.meshes[p["mesh"]]
+                self.scene_set_albedo(h, i, p["texture"], m.texcoords, m.face_texcoords)
+        return h
 
     def scene_free(self, h):
         self.L.mo_scene_free(h)

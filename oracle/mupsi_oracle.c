@@ -527,6 +527,13 @@ typedef struct {
   mupsi_primitive_desc d;
   m4 T, Tinv;
   int identity;
+  /* LambertianBsdf(BitmapTexture) albedo (bsdf.cpp:14-37, texture.cpp): RGB,
+   * row 0 at the top; uvs [n*2] + face_uv [F*3] are the mesh's texcoords
+   * (NULL: the hit's barycentrics are the uv, mesh.cpp:175-177) */
+  float* tex;
+  int tex_w, tex_h;
+  float* uvs;
+  int32_t* face_uv;
 } oprim;
 
 typedef struct {
@@ -647,6 +654,11 @@ void mo_scene_free(mo_scene* s) {
     free(m->cdf);
   }
   free(s->meshes);
+  for (int i = 0; i < s->nprim; ++i) {
+    free(s->prims[i].tex);
+    free(s->prims[i].uvs);
+    free(s->prims[i].face_uv);
+  }
   free(s->prims);
   free(s->lights);
   free(s->media);
@@ -665,24 +677,59 @@ void mo_scene_set_sky_texture(mo_scene* s, int w, int h, const float* rgb) {
   s->sky_h = h;
 }
 
-/* Skydrome::intersect (skydrome.cpp:8-17) and BitmapTexture::operator[]
- * (texture.cpp:52-69): equirectangular (u, v) of the direction, nearest texel
- * with v flipped (row 0 is the top). */
+int mo_scene_set_albedo_texture(mo_scene* s, int prim, int64_t ntc, const float* tc, const int32_t* ftc, int w,
+                                int h, const float* rgb) {
+  if (prim < 0 || prim >= s->nprim) return -1;
+  oprim* p = &s->prims[prim];
+  if (p->d.type != MUPSI_PRIM_MESH || p->d.bsdf != MUPSI_BSDF_LAMBERTIAN) return -1;
+  const int64_t nf = s->meshes[p->d.mesh].nf;
+  if (w > 0 && ntc > 0)
+    for (int64_t i = 0; i < 3 * nf; ++i)
+      if (ftc[i] < 0 || ftc[i] >= ntc) return -1;
+  free(p->tex);
+  free(p->uvs);
+  free(p->face_uv);
+  p->tex = NULL;
+  p->uvs = NULL;
+  p->face_uv = NULL;
+  p->tex_w = p->tex_h = 0;
+  if (w <= 0 || h <= 0 || !rgb) return 0;
+  p->tex = (float*)malloc(sizeof(float) * 3 * (size_t)w * h);
+  memcpy(p->tex, rgb, sizeof(float) * 3 * (size_t)w * h);
+  p->tex_w = w;
+  p->tex_h = h;
+  if (ntc > 0) {
+    p->uvs = (float*)malloc(sizeof(float) * 2 * (size_t)ntc);
+    memcpy(p->uvs, tc, sizeof(float) * 2 * (size_t)ntc);
+    p->face_uv = (int32_t*)malloc(sizeof(int32_t) * 3 * (size_t)nf);
+    memcpy(p->face_uv, ftc, sizeof(int32_t) * 3 * (size_t)nf);
+  }
+  return 0;
+}
+
+/* BitmapTexture::operator[] (texture.cpp:52-69): wrap to [0, 1), flip v (row
+ * 0 is the top), nearest texel. */
+static v3 tex_lookup(const float* tex, int w, int h, float u, float v) {
+  u = u - floorf(u);
+  v = v - floorf(v);
+  v = 1.0f - v;
+  int x = (int)(u * (float)w) % w;
+  int y = (int)(v * (float)h) % h;
+  if (x < 0) x += w;
+  if (y < 0) y += h;
+  const float* t = tex + 3 * ((size_t)y * w + x);
+  return (v3){t[0], t[1], t[2]};
+}
+
+/* Skydrome::intersect (skydrome.cpp:8-17): equirectangular (u, v) of the
+ * direction, then the texture lookup. */
 static v3 sky_lookup(const mo_scene* s, v3 dir) {
   const double pi = 3.14159265358979323846;
   float u = (float)(((double)atan2f(dir.z, dir.x) + pi) / (2.0f * pi));
   float cy = -dir.y;
   cy = cy < -1.0f ? -1.0f : (cy > 1.0f ? 1.0f : cy);
   float v = (float)((double)acosf(cy) / pi);
-  u = u - floorf(u);
-  v = v - floorf(v);
-  v = 1.0f - v;
-  int x = (int)(u * (float)s->sky_w) % s->sky_w;
-  int y = (int)(v * (float)s->sky_h) % s->sky_h;
-  if (x < 0) x += s->sky_w;
-  if (y < 0) y += s->sky_h;
-  const float* t = s->sky_tex + 3 * ((size_t)y * s->sky_w + x);
-  return (v3){t[0], t[1], t[2]};
+  return tex_lookup(s->sky_tex, s->sky_w, s->sky_h, u, v);
 }
 
 /* --------------------------------------------------------- rays / BVH -- */
@@ -1179,6 +1226,7 @@ typedef struct {
   int prim; /* -1 none */
   float t;
   v3 p, Ng;
+  float tu, tv; /* texture coordinate (primitives with an albedo texture) */
 } hitinfo;
 
 /* intersectUnitSphere (sphere.cpp:11-30) */
@@ -1268,6 +1316,18 @@ static hitinfo scene_intersect(const mo_scene* s, oray* r) {
         ln = len > 1e-12f ? vdiv(n, len) : m->face_n[tri];
       }
       hi.Ng = p->identity ? ln : vnormalized(m3t_apply(&p->Tinv, ln));
+      if (p->tex) { /* Mesh::interpolateTexcoord (mesh.cpp:175-181) */
+        if (!p->uvs) {
+          hi.tu = bu;
+          hi.tv = bv;
+        } else {
+          const int32_t* ft = p->face_uv + 3 * tri;
+          const float *t0 = p->uvs + 2 * ft[0], *t1 = p->uvs + 2 * ft[1], *t2 = p->uvs + 2 * ft[2];
+          float w = 1.0f - bu - bv;
+          hi.tu = (w * t0[0] + bu * t1[0]) + bv * t2[0];
+          hi.tv = (w * t0[1] + bu * t1[1]) + bv * t2[1];
+        }
+      }
     }
   }
   return hi;
@@ -1467,7 +1527,7 @@ static v3 trace_sample(const mo_scene* s, int x, int y, int k, int64_t* work) {
       if (hi.prim >= 0) {
         const oprim* pr = &s->prims[hi.prim];
         v3 wo = vneg(ray.d), N = hi.Ng;
-        v3 alb = vload(pr->d.albedo);
+        v3 alb = pr->tex ? tex_lookup(pr->tex, pr->tex_w, pr->tex_h, hi.tu, hi.tv) : vload(pr->d.albedo);
         lsample ls;
         if (choose_light(s, hi.p, &ps, &ls)) { /* handleSurface NEE (trace.cpp:40-56) */
           oray sr = mkray(vadd(hi.p, vmul(N, eps)), ls.d);

@@ -54,6 +54,11 @@ void mo_scene_free(mo_scene* s);
 /* Skydrome with a BitmapTexture (skydrome.cpp:8-17, texture.cpp:52-69): w x h
  * RGB floats, row 0 at the top; it replaces the constant sky. w = 0 removes it. */
 void mo_scene_set_sky_texture(mo_scene* s, int w, int h, const float* rgb);
+/* LambertianBsdf(BitmapTexture) albedo on mesh primitive `prim`: texcoords
+ * tc [ntc*2] indexed per face by ftc [F*3] (ntc 0: the barycentrics), RGB
+ * texels w x h, row 0 at the top; w = 0 removes it. 0 ok, -1 bad arguments. */
+int mo_scene_set_albedo_texture(mo_scene* s, int prim, int64_t ntc, const float* tc, const int32_t* ftc, int w,
+                                int h, const float* rgb);
 /* bvh.cpp:197-250 / :254-300 / :302-353 on scene mesh `mesh` (object space) */
 void mo_bvh_intersect(const mo_scene* s, int mesh, int64_t n, const mupsi_ray* rays, uint32_t* out_tri,
                       float* out_tuv);

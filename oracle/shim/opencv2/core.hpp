@@ -1,10 +1,12 @@
 // OpenCV stand-in for the CPU oracle (test infrastructure). Only the handful of
 // types the reference's image IO names exist. imwrite writes nothing; imread
-// reads one project-defined raw format and nothing else: a text header
+// reads two project-defined raw formats and nothing else: a text header
 // "MUPSI_RGBF <width> <height>\n" followed by width * height * 3 little-endian
-// float32 values, rows from the top, RGB (the tests write skydrome images this
-// way). The pixels come back already in RGB order and cvtColor is a copy, so
-// the reference's BGR-to-RGB conversion leaves them as written.
+// float32 values (read only with IMREAD_ANYDEPTH, as a float image), or
+// "MUPSI_RGB8 <width> <height>\n" followed by width * height * 3 bytes (an
+// 8-bit image); rows from the top, RGB. The tests write skydrome and albedo
+// images this way. The pixels come back already in RGB order and cvtColor is a
+// copy, so the reference's BGR-to-RGB conversion leaves them as written.
 #ifndef MUPSI_ORACLE_CV_STUB_CORE
 #define MUPSI_ORACLE_CV_STUB_CORE
 #include <cstdint>
@@ -40,19 +42,27 @@ class Mat {
 };
 enum { IMREAD_COLOR = 1, IMREAD_ANYDEPTH = 2, COLOR_BGR2RGB = 4 };
 inline bool imwrite(const std::string&, const Mat&) { return false; }
-// The raw float format above, read only as a float image (IMREAD_ANYDEPTH).
+// The raw formats above.
 inline Mat imread(const std::string& path, int flags = IMREAD_COLOR) {
-  if (!(flags & IMREAD_ANYDEPTH)) return Mat();
   FILE* f = std::fopen(path.c_str(), "rb");
   if (!f) return Mat();
   char magic[16] = {0};
   int w = 0, h = 0;
-  if (std::fscanf(f, "%15s %d %d", magic, &w, &h) != 3 || std::strcmp(magic, "MUPSI_RGBF") != 0 || w <= 0 ||
-      h <= 0 || w > (1 << 15) || h > (1 << 15) || std::fgetc(f) != '\n') {
+  if (std::fscanf(f, "%15s %d %d", magic, &w, &h) != 3 || w <= 0 || h <= 0 || w > (1 << 15) || h > (1 << 15) ||
+      std::fgetc(f) != '\n') {
     std::fclose(f);
     return Mat();
   }
-  Mat m(h, w, CV_32FC3);
+  int type;
+  if (std::strcmp(magic, "MUPSI_RGBF") == 0 && (flags & IMREAD_ANYDEPTH))
+    type = CV_32FC3;
+  else if (std::strcmp(magic, "MUPSI_RGB8") == 0)
+    type = CV_8UC3;
+  else {
+    std::fclose(f);
+    return Mat();
+  }
+  Mat m(h, w, type);
   const size_t got = std::fread(m.buf.data(), 1, m.buf.size(), f);
   std::fclose(f);
   if (got != m.buf.size()) return Mat();

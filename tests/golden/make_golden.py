@@ -66,6 +66,35 @@ def trace_sky(R, td):
     np.savez_compressed(os.path.join(OUT, "trace_sky.npz"), x=xs, y=ys, k=ks, radiance=rad, sky=sky)
 
 
+def trace_tex(R, td):
+    """Lambertian meshes with a BitmapTexture albedo: an 8-bit 16x12 image at
+    OBJ texcoords (scene a) and a float 8x8 image at the barycentrics (scene b,
+    an OBJ without vt lines)."""
+    rng = np.random.default_rng(12)
+    tex8 = rng.integers(0, 256, (12, 16, 3), dtype=np.uint8)
+    texf = rng.uniform(0.05, 0.95, (8, 8, 3)).astype(np.float32)
+    xs, ys, ks = np.meshgrid(np.arange(24), np.arange(24), np.arange(2), indexing="ij")
+    xs, ys, ks = xs.ravel().astype(np.int32), ys.ravel().astype(np.int32), ks.ravel().astype(np.int32)
+    out = dict(x=xs, y=ys, k=ks, tex8=tex8, texf=texf)
+    for name, with_tc, tex, tname in (("a", True, tex8, "albedo.png"), ("b", False, texf, "albedo.hdr")):
+        tp = os.path.join(td, name + tname)
+        S.save_image_raw(tp, tex)
+        sc = S.textured_floor_scene(S.load_texture_image(tp), with_tc)
+        m = sc.meshes[-1]
+        obj = os.path.join(td, name + "floor.obj")
+        S.save_obj(obj, m.vertices, m.faces, m.texcoords, m.face_texcoords)
+        j, extra = sc.to_json(obj_paths=[obj], texture_paths={2: tp})
+        assert not extra
+        jp = os.path.join(td, name + "tex.json")
+        json.dump(j, open(jp, "w"))
+        rh = R.scene_load(jp, sky=1.0)
+        rad = R.trace(rh, xs, ys, ks)
+        # the texture was loaded (a failed load shows magenta (1, 0, 1))
+        assert len(np.unique(rad[:, 0])) > 100
+        out["radiance_" + name] = rad
+    np.savez_compressed(os.path.join(OUT, "trace_tex.npz"), **out)
+
+
 def main():
     if len(sys.argv) > 1:
         with tempfile.TemporaryDirectory() as td:
@@ -180,6 +209,7 @@ def main():
     rad = R.trace(rh, xs, ys, ks)
     np.savez_compressed(os.path.join(OUT, "trace_mesh.npz"), x=xs, y=ys, k=ks, radiance=rad)
     trace_sky(R, td)
+    trace_tex(R, td)
     print("fixtures written to", OUT)
 
 

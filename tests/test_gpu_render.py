@@ -62,6 +62,29 @@ def test_trace_fixture_sky_texture(gpu, golden):
     assert not np.array_equal(bits(rad0), bits(rad))
 
 
+@pytest.mark.parametrize("name", ["a", "b"])
+def test_trace_fixture_albedo_texture(gpu, golden, name):
+    """Lambertian meshes with a BitmapTexture albedo (bsdf.cpp:14-37,
+    mesh.cpp:175-181): at OBJ texcoords with an 8-bit image (a) and at the
+    barycentrics with a float image (b); the fixture is the reference's trace."""
+    g = golden("trace_tex.npz")
+    if name == "a":
+        sc = S.textured_floor_scene((g["tex8"].astype(np.float32) / np.float32(255.0)).astype(np.float32), True)
+    else:
+        sc = S.textured_floor_scene(g["texf"], False)
+    gs = GpuScene(sc)
+    rad = gs.trace(g["x"], g["y"], g["k"])
+    same = np.all(bits(rad) == bits(g["radiance_" + name]), axis=1)
+    assert same.mean() >= 0.97, same.mean()
+    with pytest.raises(Exception):  # spheres take no albedo texture
+        gs.set_albedo_texture(1, g["texf"])
+    with pytest.raises(Exception):  # face texcoord index out of range
+        gs.set_albedo_texture(2, g["texf"], np.zeros((2, 2), np.float32), np.full((2, 3), 2, np.int32))
+    gs.set_albedo_texture(2, None)
+    flat = gs.trace(g["x"], g["y"], g["k"])
+    assert (np.any(bits(flat) != bits(rad), axis=1)).mean() > 0.2
+
+
 @pytest.mark.parametrize("mode", ["renewal_plus", "single_realization"])
 def test_trace_replay_vs_oracle(gpu, port, mode):
     sc = S.config0_scene(48, 48, 4)

@@ -2,6 +2,7 @@
 own sources (tests/golden/make_golden.py). Integer outputs and every float the
 reference computes are compared bit for bit."""
 import numpy as np
+import pytest
 
 from oracle import bind
 from mupsi_b200 import scene as S
@@ -133,3 +134,67 @@ def test_skydrome_json_round_trip(tmp_path):
     sc.sky_texture = None
     j, _ = sc.to_json()
     assert "skydrome" not in j
+
+
+def textured_scene(g, name):
+    """The fixture's scenes: an 8-bit image at OBJ texcoords (a) or a float
+    image at the barycentrics (b)."""
+    if name == "a":
+        return S.textured_floor_scene((g["tex8"].astype(np.float32) / np.float32(255.0)).astype(np.float32), True)
+    return S.textured_floor_scene(g["texf"], False)
+
+
+@pytest.mark.parametrize("name", ["a", "b"])
+def test_trace_albedo_texture(port, golden, name):
+    """LambertianBsdf(BitmapTexture) on a mesh (bsdf.cpp:14-37, mesh.cpp:175-181,
+    texture.cpp:52-69) against the reference run on the same images."""
+    g = golden("trace_tex.npz")
+    sc = textured_scene(g, name)
+    h = port.scene_from(sc)
+    try:
+        rad = port.trace(h, g["x"], g["y"], g["k"])
+        assert np.array_equal(bits(rad), bits(g["radiance_" + name]))
+        port.scene_set_albedo(h, 2, None)  # the constant albedo again: a different image
+        flat = port.trace(h, g["x"], g["y"], g["k"])
+        assert (np.any(bits(flat) != bits(rad), axis=1)).mean() > 0.2
+    finally:
+        port.scene_free(h)
+
+
+def test_obj_texcoords_round_trip(tmp_path):
+    """load_obj follows Mesh::fetchFrom's vt and face-index rules (mesh.cpp:55-111)."""
+    p = tmp_path / "m.obj"
+    p.write_text("v 0 0 0\nv 1 0 0\nv 0 1 0\nv 1 1 0\nvt 0.25 0.5\nvt 1 0\nvt 0 1\n"
+                 "f 1/1 2/2 3/3\nf 2/-2 4 -1/-1\nf 1 2 3 4\n")
+    v, f, n, tc, ftc = S.load_obj(str(p), texcoords=True)
+    assert f.tolist() == [[0, 1, 2], [1, 3, 3]]
+    assert ftc.tolist() == [[0, 1, 2], [1, 0, 2]]  # missing vt -> 0; negative -> count + i
+    assert tc.tolist() == [[0.25, 0.5], [1.0, 0.0], [0.0, 1.0]]
+    q = tmp_path / "q.obj"
+    S.save_obj(str(q), v, f, tc, ftc)
+    v2, f2, n2, tc2, ftc2 = S.load_obj(str(q), texcoords=True)
+    assert np.array_equal(v2, v) and np.array_equal(f2, f) and np.array_equal(tc2, tc) and np.array_equal(ftc2, ftc)
+    S.save_obj(str(q), v, f)
+    assert S.load_obj(str(q), texcoords=True)[3:] == (None, None)
+
+
+def test_texture_json_round_trip(tmp_path):
+    sc = S.config0_scene(8, 8, 1)
+    fv, ff = S.floor_quad()
+    tc = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
+    fm = sc.add_mesh(S.Mesh(fv, ff, texcoords=tc, face_texcoords=ff.copy()))
+    tex8 = np.random.default_rng(1).integers(0, 256, (4, 6, 3), dtype=np.uint8)
+    sc.add_mesh_primitive(fm, texture=tex8.astype(np.float32) / np.float32(255.0))
+    S.save_image_raw(str(tmp_path / "t.png"), tex8)
+    S.save_obj(str(tmp_path / "f.obj"), fv, ff, tc, ff)
+    j, extra = sc.to_json(obj_paths=["f.obj"], texture_paths={1: "t.png"})
+    assert not extra and j["primitives"][1]["texture"] == "t.png"
+    back = S.Scene.from_json(j, base_dir=str(tmp_path))
+    p = back.primitives[1]
+    assert np.array_equal(p["texture"], sc.primitives[1]["texture"])
+    assert np.array_equal(back.meshes[p["mesh"]].texcoords, tc)
+    j["primitives"][1]["bsdf"] = "specular"  # the reference reads a texture for Lambertian meshes only
+    assert S.Scene.from_json(j, base_dir=str(tmp_path)).primitives[1]["texture"] is None
+    with pytest.raises(OSError):  # float pixels only under .hdr / .exr names
+        S.save_image_raw(str(tmp_path / "f.png"), tex8.astype(np.float32))
+        S.load_texture_image(str(tmp_path / "f.png"))
