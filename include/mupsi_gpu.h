@@ -52,6 +52,12 @@ typedef enum { MUPSI_GP_SINGLE_REALIZATION = 0, MUPSI_GP_RENEWAL_PLUS = 1 } mups
 typedef enum { MUPSI_BSDF_LAMBERTIAN = 0, MUPSI_BSDF_NULL = 1, MUPSI_BSDF_SPECULAR = 2 } mupsi_bsdf;
 /* mean functions (gp/meanfunction.h:10-57) */
 typedef enum { MUPSI_MEAN_SPHERE = 0, MUPSI_MEAN_MESH = 1 } mupsi_mean_type;
+
+/* What a scene medium is: a GPMedium (medium/gpmedium.h, the descriptor's
+ * default), an SDFMedium (medium/sdfmedium.h) or an ExternalGPMedium
+ * (medium/externalgpmedium.h); see mupsi_gpu_scene_set_sdf_medium and
+ * mupsi_gpu_scene_set_external_gp_medium. */
+typedef enum { MUPSI_MEDIUM_GP = 0, MUPSI_MEDIUM_SDF = 1, MUPSI_MEDIUM_EXTERNAL_GP = 2 } mupsi_medium_kind;
 /* primitives (geometry/primitive.h:17-67) */
 typedef enum { MUPSI_PRIM_SPHERE = 0, MUPSI_PRIM_MESH = 1 } mupsi_prim_type;
 
@@ -214,20 +220,30 @@ int mupsi_gpu_mesh_queries(const mupsi_mesh* mesh, int64_t n, const float* p, ui
 int mupsi_gpu_scene_create(const mupsi_scene_desc* desc, mupsi_scene** out);
 void mupsi_gpu_scene_destroy(mupsi_scene* scene);
 
-/* MeanFunction::eval + gradient of medium `medium` (gp/meanfunction.cpp:13-39):
+/* MeanFunction::eval + gradient of medium `medium` (gp/meanfunction.cpp:13-39;
+ * an external GP medium's GridMeanFunction, meanfunction.cpp:58-86):
  * out[n*4] = (mu, grad xyz). */
 int mupsi_gpu_mean(const mupsi_scene* scene, int32_t medium, int64_t n, const float* p, float* out,
                    mupsi_mem mem, void* stream);
-/* GPMedium::evalWithGradient(p, seed, state) (gpmedium.cpp:19-41): out[n*4]. */
+/* GPMedium::evalWithGradient(p, seed, state) (gpmedium.cpp:19-41): out[n*4].
+ * A field medium gives its own evalWithGradient (sdfmedium.cpp:10-14,
+ * externalgpmedium.cpp:33-58; cond unused). */
 int mupsi_gpu_medium_eval(const mupsi_scene* scene, int32_t medium, int64_t n, const float* p,
                           const uint32_t* seed, const mupsi_cond* cond, float* out, mupsi_mem mem, void* stream);
 /* GPMedium::sampleDistance (gpmedium.cpp:46-103) for n rays; seed[i] is the value
- * the march draws from its ConstantSampler (medium_sampler.nextI()). */
+ * the march draws from its ConstantSampler (medium_sampler.nextI()). Field
+ * media march as SDFMedium / ExternalGPMedium::sampleDistance. */
 int mupsi_gpu_sample_distance(const mupsi_scene* scene, int32_t medium, int64_t n, const mupsi_ray* rays,
                               const uint32_t* seed, const mupsi_cond* cond, mupsi_medium_sample* out,
                               mupsi_mem mem, void* stream);
+/* Medium::transmittance for n rays (gpmedium.cpp:105-129, sdfmedium.cpp:65-96,
+ * externalgpmedium.cpp:111-130): out[n] = 0 where the field changes sign along
+ * the ray, else 1. seed[i] as for sampleDistance. */
+int mupsi_gpu_transmittance(const mupsi_scene* scene, int32_t medium, int64_t n, const mupsi_ray* rays,
+                            const uint32_t* seed, const mupsi_cond* cond, float* out, mupsi_mem mem, void* stream);
 /* GPMedium::sampleCondition (gpmedium.cpp:133-161) for n medium samples; seed[i]
- * is the next bounce's ConstantSampler draw. */
+ * is the next bounce's ConstantSampler draw. MUPSI_ERR_INVALID for a field
+ * medium (only a GPMedium conditions, trace.cpp:144-147). */
 int mupsi_gpu_sample_condition(const mupsi_scene* scene, int32_t medium, int64_t n,
                                const mupsi_medium_sample* samples, const uint32_t* seed, mupsi_cond* out,
                                mupsi_mem mem, void* stream);
@@ -370,6 +386,25 @@ int mupsi_gpu_scene_set_surrogate(mupsi_scene* scene, int32_t medium, mupsi_mlp*
  * floats, row 0 at the top, host memory (copied); it replaces the constant sky
  * of the descriptor. width = height = 0 removes it. */
 int mupsi_gpu_scene_set_sky_texture(mupsi_scene* scene, int32_t width, int32_t height, const float* rgb);
+
+/* Turn medium `medium` into an SDFMedium (controller.cpp:154-182,
+ * sdfmedium.cpp:16-98): its descriptor's mean function (sphere or mesh) is the
+ * field itself, sphere traced from the ray's nearT (steps max(|f|, 1e-3), at
+ * most 512, farT capped at 2000) to the first sign change, refined by 16
+ * bisections; transmittance is 0 past a sign change. The kernel, the Renewal+
+ * conditioning and any surrogate play no part. */
+int mupsi_gpu_scene_set_sdf_medium(mupsi_scene* scene, int32_t medium);
+
+/* Turn medium `medium` into an ExternalGPMedium (controller.cpp:184-189,
+ * externalgpmedium.cpp:9-130): f(p) = mean(p) + noise_scale * sqrt(var(p)) *
+ * hash(p, seed), mean and var GridMeanFunctions (meanfunction.cpp:41-86) of
+ * resolution^3 float samples, x-major (index (i * res + j) * res + k), over
+ * [bounds_min, bounds_max]; variance_grid NULL: no noise. Sphere traced with
+ * steps max(|f|, 0.005), at most 1024, refined by 16 bisections. Grids are
+ * host memory, copied; resolution in [2, 1024]. */
+int mupsi_gpu_scene_set_external_gp_medium(mupsi_scene* scene, int32_t medium, int32_t resolution,
+                                           const float bounds_min[3], const float bounds_max[3],
+                                           const float* mean_grid, const float* variance_grid, float noise_scale);
 
 /* Lambertian BSDF with a BitmapTexture albedo on mesh primitive `primitive`
  * (controller.cpp:240-243, bsdf.cpp:14-37): the albedo at a hit is the nearest

@@ -255,6 +255,12 @@ class GpuScene:
         h = C.c_void_p()
         check(load().mupsi_gpu_scene_create(C.byref(self._desc), C.byref(h)))
         self.h = h
+        for i, m in enumerate(scene.media):
+            if m.get("kind") == "sdf":
+                self.set_sdf_medium(i)
+            elif m.get("kind") == "external_gp":
+                self.set_external_gp_medium(i, m["res"], m["bmin"], m["bmax"], m["mean_grid"], m["var_grid"],
+                                            m["noise_scale"])
         if getattr(scene, "sky_texture", None) is not None:
             self.set_sky_texture(scene.sky_texture)
         for i, p in enumerate(scene.primitives):
@@ -309,6 +315,17 @@ class GpuScene:
         res[:, 0] = out.view(np.uint32)[:, 0].astype(np.float32)
         return res
 
+    def transmittance(self, medium, rays, seed, cond=None, stream=None):
+        """Medium::transmittance of (n, 8) rays [o xyz, d xyz, near, far] -> (n,) in {0, 1}."""
+        rays = _host(rays, np.float32)
+        seed = _host(seed, np.uint32)
+        c = cond_records(cond)
+        mem = _mem(rays, seed, c)
+        out = _empty(mem == _abi.MEM_DEVICE, (rays.shape[0],), np.float32)
+        check(load().mupsi_gpu_transmittance(self.h, medium, rays.shape[0], _ptr(rays), _ptr(seed), _ptr(c),
+                                             _ptr(out), mem, _stream(stream)))
+        return out
+
     def sample_condition(self, medium, samples, seed, stream=None):
         """GPMedium::sampleCondition: samples (n, 7) [exited, p xyz, normal xyz] -> (n, 8) [C, u, g, active]."""
         samples = np.asarray(samples, np.float32)
@@ -343,6 +360,25 @@ class GpuScene:
             return
         img = np.ascontiguousarray(img, np.float32)
         check(load().mupsi_gpu_scene_set_sky_texture(self.h, img.shape[1], img.shape[0], img.ctypes.data))
+
+    def set_sdf_medium(self, medium):
+        """Make medium `medium` an SDFMedium over its mean function."""
+        check(load().mupsi_gpu_scene_set_sdf_medium(self.h, medium))
+
+    def set_external_gp_medium(self, medium, resolution, bounds_min, bounds_max, mean_grid, variance_grid=None,
+                               noise_scale=1.0):
+        """Make medium `medium` an ExternalGPMedium over GridMeanFunction grids
+        (resolution^3 float32, x-major; variance None: no noise)."""
+        mg = np.ascontiguousarray(mean_grid, np.float32).reshape(-1)
+        vg = None if variance_grid is None else np.ascontiguousarray(variance_grid, np.float32).reshape(-1)
+        cells = int(resolution) ** 3
+        if mg.size != cells or (vg is not None and vg.size != cells):
+            raise ValueError("grids need resolution^3 samples")
+        lo = (C.c_float * 3)(*bounds_min)
+        hi = (C.c_float * 3)(*bounds_max)
+        check(load().mupsi_gpu_scene_set_external_gp_medium(self.h, medium, int(resolution), lo, hi, mg.ctypes.data,
+                                                            None if vg is None else vg.ctypes.data,
+                                                            float(noise_scale)))
 
     def set_albedo_texture(self, primitive, img, texcoords=None, face_texcoords=None):
         """Lambertian BitmapTexture albedo of a mesh primitive: (h, w, 3) float

@@ -6,7 +6,9 @@
 // Each bounce iteration runs two kernels:
 //   k_march  - persistent warps march every path that is inside a GP medium;
 //              idle lanes pull the next path from the medium queue, so long and
-//              short marches never stall a warp;
+//              short marches never stall a warp; (scenes with an SDF or
+//              external GP medium add k_march_field, which sphere traces those
+//              paths, one thread each)
 //   k_shade  - every live path: medium event (NEE, Lambertian sample, Russian
 //              roulette, Renewal+ conditioning) or surface event (scene
 //              intersection, NEE, BSDF sample, RR, medium switch) or sky; the
@@ -235,6 +237,7 @@ __global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? 6 : 1) k_march(c
   bool ovf = false;
   unsigned long long steps = 0, psis = 0, marches = 0, imps = 0, mus = 0, pars = 0, reqs = 0, accs = 0;
   while (true) {
+    bool skipped = false;  // this group drew a path of a field medium (k_march_field marches it)
     // refill idle groups from the queue (warp-aggregated over group leaders)
     unsigned need = __ballot_sync(0xffffffffu, !active && grp.sub == 0);
     if (need) {
@@ -251,32 +254,35 @@ __global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? 6 : 1) k_march(c
           int4 meta = P.meta[idx];
           int med = __float_as_int(d.w);
           S = scenes[meta_inst(meta.w)];
-          march_begin(S, m, mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), o.w, 3.402823466e+38f, med,
-                      medium_seed(S, meta.x, meta.y, meta.z, meta_bounce(meta.w)), load_cond(P, idx));
-          m.may_request = MK != MEAN_SPHERE_ONLY && can_suspend && m.lazy && S->media[med].surr;
-          if (MK != MEAN_SPHERE_ONLY && resume) {
-            const float4 a = P.ms0[idx], b = P.ms1[idx];
-            const int fl = __float_as_int(a.w);
-            m.t = a.x;
-            m.k = __float_as_int(a.y);
-            m.fprev = a.z;
-            m.fprev_pos = (fl & 1) != 0;
-            m.fprev_big = (fl & 2) != 0;
-            m.n_req = fl >> 8;
-            m.init = false;
-            m.mu_j = b.x;
-            m.mu_hi = b.y;
-            m.t_j = b.z;
-            const bool used = march_apply_prediction(S->media[med], m, P.pred[(round - 1) & 1][j]);
-            if (grp.sub == 0 && used) accs++;
-          } else if (grp.sub == 0) {
-            marches++;
+          skipped = !resume && S->media[med].kind != MUPSI_MEDIUM_GP;  // k_march_field marches it
+          if (!skipped) {
+            march_begin(S, m, mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), o.w, 3.402823466e+38f, med,
+                        medium_seed(S, meta.x, meta.y, meta.z, meta_bounce(meta.w)), load_cond(P, idx));
+            m.may_request = MK != MEAN_SPHERE_ONLY && can_suspend && m.lazy && S->media[med].surr;
+            if (MK != MEAN_SPHERE_ONLY && resume) {
+              const float4 a = P.ms0[idx], b = P.ms1[idx];
+              const int fl = __float_as_int(a.w);
+              m.t = a.x;
+              m.k = __float_as_int(a.y);
+              m.fprev = a.z;
+              m.fprev_pos = (fl & 1) != 0;
+              m.fprev_big = (fl & 2) != 0;
+              m.n_req = fl >> 8;
+              m.init = false;
+              m.mu_j = b.x;
+              m.mu_hi = b.y;
+              m.t_j = b.z;
+              const bool used = march_apply_prediction(S->media[med], m, P.pred[(round - 1) & 1][j]);
+              if (grp.sub == 0 && used) accs++;
+            } else if (grp.sub == 0) {
+              marches++;
+            }
+            active = true;
           }
-          active = true;
         }
       }
     }
-    if (!__any_sync(0xffffffffu, active)) break;
+    if (!__any_sync(0xffffffffu, active || skipped)) break;
     if (active) {
       v3 p;
       if (march_cheap<MK>(S, m, p, ovf, &grp)) march_psi<MK, true>(S, m, p, grp, ovf);
@@ -336,8 +342,36 @@ __global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? 6 : 1) k_march(c
   }
 }
 
-// GPMedium::transmittance (gpmedium.cpp:105-129): 0 at the first sign change.
+// SDFMedium / ExternalGPMedium::sampleDistance for the paths of iteration `it`
+// whose medium is a field medium (k_march leaves them): one thread per path,
+// sphere tracing bounded by the reference's iteration limits (512 / 1024).
+__global__ void __launch_bounds__(128) k_march_field(const DScene* const* __restrict__ scenes, Paths P, int it,
+                                                     WaveCfg cfg) {
+  const uint32_t n = P.counts[2 * it];
+  const uint32_t* q = P.q[it & 1];
+  bool ovf = false;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const uint32_t idx = q[j];
+    const float4 d = P.d[idx];
+    const int4 meta = P.meta[idx];
+    const DScene* S = scenes[meta_inst(meta.w)];
+    const DMedium& md = S->media[__float_as_int(d.w)];
+    if (md.kind == MUPSI_MEDIUM_GP) continue;
+    const float4 o = P.o[idx];
+    mupsi_medium_sample r;
+    field_sample_distance(S, md, mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), o.w, 3.402823466e+38f,
+                          medium_seed(S, meta.x, meta.y, meta.z, meta_bounce(meta.w)), r, ovf);
+    P.ha[idx] = make_float4(r.t, r.p[0], r.p[1], r.p[2]);
+    P.hb[idx] = make_float4(r.normal[0], r.normal[1], r.normal[2], __uint_as_float(r.exited));
+  }
+  if (ovf) atomicOr(cfg.err, ERR_BVH_STACK);
+}
+
+// Medium::transmittance: GPMedium (gpmedium.cpp:105-129) or a field medium;
+// 0 at the first sign change.
 MD float transmittance(const DScene* S, int medium, const Ray& r, uint32_t seed, const Cond& c, bool& ovf) {
+  const DMedium& md = S->media[medium];
+  if (md.kind != MUPSI_MEDIUM_GP) return field_transmittance(S, md, r.o, r.d, r.nt, r.ft, seed, ovf);
   March m;
   march_begin(S, m, r.o, r.d, r.nt, r.ft, medium, seed, c);
   march_full(S, m, ovf);
@@ -403,8 +437,10 @@ __global__ void __launch_bounds__(128) k_shade(const DScene* const* __restrict__
           dead = true;
         } else {
           thr = thr / surv;
-          uint32_t ns = medium_seed(S, meta.x, meta.y, meta.z, bounce + 1);
-          cond = sample_condition(S, S->media[medium], Pt, N, false, ns, !single, ovf);
+          if (S->media[medium].kind == MUPSI_MEDIUM_GP) {  // only a GPMedium conditions (trace.cpp:144-147)
+            uint32_t ns = medium_seed(S, meta.x, meta.y, meta.z, bounce + 1);
+            cond = sample_condition(S, S->media[medium], Pt, N, false, ns, !single, ovf);
+          }
           ray = make_ray(Pt + N * S->eps, wi);
           ray.nt = S->nearteps;
           bounce++;
@@ -534,7 +570,15 @@ __global__ void k_average(const float* __restrict__ sum, int64_t n3, float inv, 
 __global__ void k_mean(const DScene* S, int medium, int64_t n, const float* p, float* out) {
   bool ovf = false;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    float4 r = mean_value_grad(S, S->media[medium], ld3(p + 3 * i), ovf);
+    const DMedium& md = S->media[medium];
+    float4 r;
+    if (md.kind == MUPSI_MEDIUM_EXTERNAL_GP) {  // its GridMeanFunction
+      const v3 P3 = ld3(p + 3 * i);
+      const v3 g = grid_gradient(md.gmean, P3);
+      r = make_float4(grid_eval(md.gmean, P3), g.x, g.y, g.z);
+    } else {
+      r = mean_value_grad(S, md, ld3(p + 3 * i), ovf);
+    }
     out[4 * i] = r.x;
     out[4 * i + 1] = r.y;
     out[4 * i + 2] = r.z;
@@ -552,7 +596,9 @@ __global__ void k_medium_eval(const DScene* S, int medium, int64_t n, const floa
     } else {
       c.active = 0;
     }
-    float4 r = medium_eval(S, S->media[medium], ld3(p + 3 * i), seed[i], c, ovf);
+    const DMedium& md = S->media[medium];
+    float4 r = md.kind == MUPSI_MEDIUM_GP ? medium_eval(S, md, ld3(p + 3 * i), seed[i], c, ovf)
+                                          : field_value_grad(S, md, ld3(p + 3 * i), seed[i], ovf);
     out[4 * i] = r.x;
     out[4 * i + 1] = r.y;
     out[4 * i + 2] = r.z;
@@ -574,13 +620,38 @@ __global__ void k_sample_distance(const DScene* S, int medium, int64_t n, const 
       c.g = mk3(0, 0, 0);
     }
     const mupsi_ray& r = rays[i];
-    March m;
-    // Ray(origin, direction) normalises the direction (geometry/ray.h:12)
-    march_begin(S, m, ld3(r.o), normalized(ld3(r.d)), r.near_t, r.far_t, medium, seed[i], c);
-    march_full(S, m, ovf);
     mupsi_medium_sample res;
-    march_result(S, m, res, ovf, single_lane());
+    // Ray(origin, direction) normalises the direction (geometry/ray.h:12)
+    if (S->media[medium].kind != MUPSI_MEDIUM_GP) {
+      field_sample_distance(S, S->media[medium], ld3(r.o), normalized(ld3(r.d)), r.near_t, r.far_t, seed[i], res, ovf);
+    } else {
+      March m;
+      march_begin(S, m, ld3(r.o), normalized(ld3(r.d)), r.near_t, r.far_t, medium, seed[i], c);
+      march_full(S, m, ovf);
+      march_result(S, m, res, ovf, single_lane());
+    }
     out[i] = res;
+  }
+  if (ovf) atomicOr(S->err, ERR_BVH_STACK);
+}
+__global__ void k_transmittance(const DScene* S, int medium, int64_t n, const mupsi_ray* rays, const uint32_t* seed,
+                                const Cond* cond, float* out) {
+  bool ovf = false;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    Cond c;
+    if (cond) {
+      c = cond[i];
+    } else {
+      c.active = 0;
+      c.C = mk3(0, 0, 0);
+      c.u = 0;
+      c.g = mk3(0, 0, 0);
+    }
+    const mupsi_ray& r = rays[i];
+    Ray R = make_ray(ld3(r.o), ld3(r.d));
+    R.nt = r.near_t;
+    R.ft = r.far_t;
+    out[i] = transmittance(S, medium, R, seed[i], c, ovf);
   }
   if (ovf) atomicOr(S->err, ERR_BVH_STACK);
 }
@@ -632,6 +703,7 @@ struct mupsi_scene {
   mupsi_mlp* surr_mlp = nullptr;  // surrogate of a mesh mean (not owned)
   void* sky_mem = nullptr;        // sky texture texels (owned)
   void* tex_mem[MAX_PRIMS] = {};  // albedo texture texels + texcoords per primitive (owned)
+  void* grid_mem[MAX_MEDIA] = {};  // external GP mean + variance grids per medium (owned)
   int surr_rounds = 1;            // march rounds per bounce iteration with it: predictions + 1
   int* err = nullptr;
   unsigned long long* counters = nullptr;
@@ -710,6 +782,8 @@ mupsi_scene::~mupsi_scene() {
     if (d_chunk) cudaFree(d_chunk);
     if (sky_mem) cudaFree(sky_mem);
     for (void* p : tex_mem)
+      if (p) cudaFree(p);
+    for (void* p : grid_mem)
       if (p) cudaFree(p);
     if (sum) cudaFree(sum);
     if (pb.mem) pool_give(pb.mem, pb.bytes);
@@ -968,6 +1042,7 @@ struct WaveExec {
   Paths P;
   int iters;                    // bounce iterations: max over the wave's scenes of max(1, max_bounce)
   bool sphere_only;
+  bool field = false;           // some scene of the wave has a field medium: k_march_field runs too
   WaveCfg cfg;
   mupsi_mlp* mlp = nullptr;     // surrogate answering suspended marches (rounds > 1)
 };
@@ -975,6 +1050,7 @@ struct WaveExec {
 // The march of bounce iteration `it`: round 0, then, with a surrogate, the
 // inference of the round's requests and the round that resumes them.
 void launch_march_rounds(const WaveExec& w, const MarchLaunch& ml, int it, cudaStream_t st) {
+  if (w.field) k_march_field<<<num_sms() * 16, 128, 0, st>>>(w.scenes, w.P, it, w.cfg);
   const int R = w.P.rounds;
   for (int r = 0; r < R; ++r) {
     ml.fn<<<ml.blocks, ml.block, 0, st>>>(w.scenes, w.P, it, r, w.cfg);
@@ -1013,7 +1089,7 @@ void launch_wave(const WaveExec& w, const WaveSrc& src, cudaStream_t st, mupsi_s
     }
   }
 }
-int wave_launches(int iters, int rounds = 1) { return 2 + (2 * rounds) * iters; }
+int wave_launches(int iters, int rounds = 1, bool field = false) { return 2 + (2 * rounds + (field ? 1 : 0)) * iters; }
 
 WaveExec scene_exec(mupsi_scene* s) {
   WaveExec w;
@@ -1021,6 +1097,7 @@ WaveExec scene_exec(mupsi_scene* s) {
   w.P = s->pb.paths;
   w.iters = wave_iters(s);
   w.sphere_only = s->h.sphere_only != 0;
+  w.field = s->h.field != 0;
   w.cfg.min_group = g_tuning.min_group;
   w.cfg.err = s->err;
   w.cfg.counters = s->profile ? s->counters : nullptr;
@@ -1047,7 +1124,7 @@ int run_wave(mupsi_scene* s, int64_t n, int pass0, const int32_t* xs, const int3
     src.nchunks = 1;
   }
   launch_wave(w, src, st, s);
-  count_launch(wave_launches(w.iters, w.P.rounds));
+  count_launch(wave_launches(w.iters, w.P.rounds, w.field));
   MUPSI_CUDA(cudaGetLastError());
   return MUPSI_OK;
 }
@@ -1197,7 +1274,8 @@ struct mupsi_batch {
   WaveDesc* d_waves = nullptr;
   size_t wave_cap = 0;
   PathBuf pb;
-  bool sphere_only = true;
+  bool sphere_only = true;     // k_march variant for every instance
+  bool field = false;          // some instance has a field medium
   cudaStream_t bs = nullptr;  // graphs are captured and replayed on this stream
   std::vector<BatchGraph> graphs;
   mupsi_tuning graph_tuning{};  // launch shapes the graphs were captured with
@@ -1241,6 +1319,7 @@ void batch_wave_launches(mupsi_batch* b, int iters) {
   w.P = b->pb.paths;
   w.iters = iters;
   w.sphere_only = b->sphere_only;
+  w.field = b->field;
   w.cfg.min_group = g_tuning.min_group;
   w.cfg.err = b->err;
   w.cfg.counters = nullptr;
@@ -1257,6 +1336,18 @@ bool same_tuning(const mupsi_tuning& a, const mupsi_tuning& c) {
 }
 
 // The graph of a wave with `iters` bounce iterations, captured on first use.
+// The instances' medium flags as they are now; graphs captured under others go.
+void batch_flags(mupsi_batch* b) {
+  bool so = true, fd = false;
+  for (mupsi_scene* s : b->inst) {
+    so = so && s->h.sphere_only != 0;
+    fd = fd || s->h.field != 0;
+  }
+  if (so != b->sphere_only || fd != b->field) b->drop_graphs();
+  b->sphere_only = so;
+  b->field = fd;
+}
+
 int batch_graph(mupsi_batch* b, int iters, cudaGraphExec_t* out) {
   if (!same_tuning(b->graph_tuning, g_tuning)) {
     b->drop_graphs();
@@ -1381,9 +1472,34 @@ int mupsi_gpu_sample_distance(const mupsi_scene* scene, int32_t medium, int64_t 
   return check_err(const_cast<mupsi_scene*>(scene), st);
 }
 
+int mupsi_gpu_transmittance(const mupsi_scene* scene, int32_t medium, int64_t n, const mupsi_ray* rays,
+                            const uint32_t* seed, const mupsi_cond* cond, float* out, mupsi_mem mem, void* stream) {
+  clear_error();
+  if (!scene || medium < 0 || medium >= scene->h.nmed || n < 0) return fail(MUPSI_ERR_INVALID, "bad argument");
+  if (n == 0) return MUPSI_OK;
+  if (!rays || !seed || !out) return fail(MUPSI_ERR_INVALID, "null buffer");
+  cudaStream_t st = resolve_stream(stream);
+  Staged<mupsi_ray> dr(st);
+  Staged<uint32_t> ds(st);
+  Staged<mupsi_cond> dc(st);
+  Staged<float> dout(st);
+  MUPSI_CUDA(dr.in(rays, n, mem));
+  MUPSI_CUDA(ds.in(seed, n, mem));
+  if (cond) MUPSI_CUDA(dc.in(cond, n, mem));
+  MUPSI_CUDA(dout.out(out, n, mem));
+  k_transmittance<<<grid_n(n), 128, 0, st>>>(scene->d, medium, n, dr.ptr, ds.ptr,
+                                             cond ? reinterpret_cast<const Cond*>(dc.ptr) : nullptr, dout.ptr);
+  count_launch();
+  MUPSI_CUDA(cudaGetLastError());
+  MUPSI_CUDA(dout.finish());
+  return check_err(const_cast<mupsi_scene*>(scene), st);
+}
+
 int mupsi_gpu_sample_condition(const mupsi_scene* scene, int32_t medium, int64_t n, const mupsi_medium_sample* samples,
                                const uint32_t* seed, mupsi_cond* out, mupsi_mem mem, void* stream) {
   clear_error();
+  if (scene && medium >= 0 && medium < scene->h.nmed && scene->h.media[medium].kind != MUPSI_MEDIUM_GP)
+    return fail(MUPSI_ERR_INVALID, "only a GP medium conditions");
   if (!scene || medium < 0 || medium >= scene->h.nmed || n < 0) return fail(MUPSI_ERR_INVALID, "bad argument");
   if (n == 0) return MUPSI_OK;
   if (!samples || !seed || !out) return fail(MUPSI_ERR_INVALID, "null buffer");
@@ -1517,7 +1633,7 @@ int mupsi_gpu_trace_samples_noalloc(mupsi_scene* scene, int64_t n, const int32_t
   src.ys = y;
   src.ks = k;
   launch_wave(w, src, st, nullptr);
-  count_launch(wave_launches(w.iters));
+  count_launch(wave_launches(w.iters, 1, w.field));
   MUPSI_CUDA(cudaGetLastError());
   const Paths& P = w.P;
   MUPSI_CUDA(cudaMemcpyAsync(out_rgb, P.rad, n * 12, cudaMemcpyDeviceToDevice, st));
@@ -1606,7 +1722,6 @@ int mupsi_gpu_batch_create(int32_t num_scenes, mupsi_scene* const* scenes, mupsi
     b->inst.push_back(scenes[i]);
     list.push_back(scenes[i]->d);
     sums.push_back(scenes[i]->sum);
-    if (!scenes[i]->h.sphere_only) b->sphere_only = false;
   }
   MUPSI_CUDA(cudaMalloc((void**)&b->d_list, list.size() * sizeof(DScene*)));
   MUPSI_CUDA(cudaMemcpy(b->d_list, list.data(), list.size() * sizeof(DScene*), cudaMemcpyHostToDevice));
@@ -1645,6 +1760,7 @@ int mupsi_gpu_batch_render(mupsi_batch* b, const mupsi_batch_args* a) {
     return fail(MUPSI_ERR_INVALID, "unknown schedule");
   b->info.waves = b->info.graph_launches = b->info.max_iters = 0;
   b->info.paths = 0;
+  batch_flags(b);
   // ---- plan: instances in schedule order, their passes packed into waves of
   // at most wave_paths() paths (a pass is never split across waves)
   std::vector<int> order(n);
@@ -1746,7 +1862,7 @@ int mupsi_gpu_batch_render(mupsi_batch* b, const mupsi_batch_args* a) {
     } else {
       batch_wave_launches(b, iters);
     }
-    count_launch(wave_launches(iters) + 1);
+    count_launch(wave_launches(iters, 1, b->field) + 1);
     b->info.waves++;
     b->info.max_iters = std::max(b->info.max_iters, iters);
     b->info.paths += waves[w].n;
@@ -1791,7 +1907,8 @@ int mupsi_gpu_scene_set_surrogate(mupsi_scene* scene, int32_t medium, mupsi_mlp*
   if (medium < 0 || medium >= scene->h.nmed) return fail(MUPSI_ERR_INVALID, "medium out of range");
   DMedium& md = scene->h.media[medium];
   if (mlp) {
-    if (md.mean_type != MUPSI_MEAN_MESH) return fail(MUPSI_ERR_INVALID, "the surrogate stands in for a mesh mean");
+    if (md.mean_type != MUPSI_MEAN_MESH || md.kind != MUPSI_MEDIUM_GP)
+      return fail(MUPSI_ERR_INVALID, "the surrogate stands in for a GP medium's mesh mean");
     if (!(band >= 0.0f) || !(scale >= 1.0f) || !(margin >= 0.0f) || !std::isfinite(band) || !std::isfinite(scale) ||
         !std::isfinite(margin))
       return fail(MUPSI_ERR_INVALID, "need band >= 0, scale >= 1, margin >= 0");
@@ -1825,6 +1942,7 @@ int mupsi_gpu_scene_set_mean_eval(mupsi_scene* scene, int32_t medium, int32_t mo
   if (medium < 0 || medium >= scene->h.nmed) return fail(MUPSI_ERR_INVALID, "medium out of range");
   if (mode != MUPSI_MEAN_EVAL_LAZY && mode != MUPSI_MEAN_EVAL_EVERY_STEP)
     return fail(MUPSI_ERR_INVALID, "unknown mean evaluation mode");
+  if (scene->h.media[medium].kind != MUPSI_MEDIUM_GP) return fail(MUPSI_ERR_INVALID, "not a GP medium");
   scene->h.media[medium].every_step = mode == MUPSI_MEAN_EVAL_EVERY_STEP;
   MUPSI_CUDA(cudaDeviceSynchronize());
   MUPSI_CUDA(cudaMemcpy(scene->d, &scene->h, sizeof(DScene), cudaMemcpyHostToDevice));
@@ -1865,6 +1983,72 @@ int mupsi_gpu_scene_set_sky_texture(mupsi_scene* scene, int32_t width, int32_t h
     scene->h.sky_w = width;
     scene->h.sky_h = height;
   }
+  MUPSI_CUDA(cudaMemcpy(scene->d, &scene->h, sizeof(DScene), cudaMemcpyHostToDevice));
+  return MUPSI_OK;
+}
+
+// The k_march variant: sphere means only among the GP media (field media are
+// marched by k_march_field, which handles every mean).
+static void update_medium_flags(DScene& S) {
+  S.sphere_only = 1;
+  S.field = 0;
+  for (int i = 0; i < S.nmed; ++i) {
+    if (S.media[i].kind != MUPSI_MEDIUM_GP)
+      S.field = 1;
+    else if (S.media[i].mean_type != MUPSI_MEAN_SPHERE)
+      S.sphere_only = 0;
+  }
+}
+
+int mupsi_gpu_scene_set_sdf_medium(mupsi_scene* scene, int32_t medium) {
+  clear_error();
+  if (!scene) return fail(MUPSI_ERR_INVALID, "null scene");
+  if (medium < 0 || medium >= scene->h.nmed) return fail(MUPSI_ERR_INVALID, "medium out of range");
+  if (scene->surr_mlp && scene->h.media[medium].surr) return fail(MUPSI_ERR_INVALID, "medium has a surrogate");
+  MUPSI_CUDA(cudaDeviceSynchronize());
+  DMedium& md = scene->h.media[medium];
+  md.kind = MUPSI_MEDIUM_SDF;
+  md.every_step = 0;
+  update_medium_flags(scene->h);
+  MUPSI_CUDA(cudaMemcpy(scene->d, &scene->h, sizeof(DScene), cudaMemcpyHostToDevice));
+  return MUPSI_OK;
+}
+
+int mupsi_gpu_scene_set_external_gp_medium(mupsi_scene* scene, int32_t medium, int32_t resolution,
+                                           const float bounds_min[3], const float bounds_max[3],
+                                           const float* mean_grid, const float* variance_grid, float noise_scale) {
+  clear_error();
+  if (!scene) return fail(MUPSI_ERR_INVALID, "null scene");
+  if (medium < 0 || medium >= scene->h.nmed) return fail(MUPSI_ERR_INVALID, "medium out of range");
+  if (scene->surr_mlp && scene->h.media[medium].surr) return fail(MUPSI_ERR_INVALID, "medium has a surrogate");
+  if (resolution < 2 || resolution > 1024) return fail(MUPSI_ERR_INVALID, "resolution must be in [2, 1024]");
+  if (!bounds_min || !bounds_max || !mean_grid) return fail(MUPSI_ERR_INVALID, "null argument");
+  if (!std::isfinite(noise_scale)) return fail(MUPSI_ERR_INVALID, "bad noise scale");
+  v3 bmin = ld3(bounds_min), bmax = ld3(bounds_max);
+  for (int a = 0; a < 3; ++a)
+    if (!std::isfinite(get(bmin, a)) || !std::isfinite(get(bmax, a)) || !(get(bmax, a) > get(bmin, a)))
+      return fail(MUPSI_ERR_INVALID, "need finite bounds_min < bounds_max");
+  MUPSI_CUDA(cudaDeviceSynchronize());
+  if (scene->grid_mem[medium]) {
+    cudaFree(scene->grid_mem[medium]);
+    scene->grid_mem[medium] = nullptr;
+  }
+  const size_t cells = (size_t)resolution * resolution * resolution;
+  float* mem = nullptr;
+  MUPSI_CUDA(cudaMalloc(&mem, cells * sizeof(float) * (variance_grid ? 2 : 1)));
+  scene->grid_mem[medium] = mem;
+  MUPSI_CUDA(cudaMemcpy(mem, mean_grid, cells * sizeof(float), cudaMemcpyHostToDevice));
+  if (variance_grid) MUPSI_CUDA(cudaMemcpy(mem + cells, variance_grid, cells * sizeof(float), cudaMemcpyHostToDevice));
+  DMedium& md = scene->h.media[medium];
+  md.kind = MUPSI_MEDIUM_EXTERNAL_GP;
+  md.every_step = 0;
+  // inv_cell_size_ = (res, res, res) / (bmax - bmin) (meanfunction.cpp:44)
+  const float r = (float)resolution;
+  const v3 inv = mk3(r / (bmax.x - bmin.x), r / (bmax.y - bmin.y), r / (bmax.z - bmin.z));
+  md.gmean = DGrid{mem, resolution, bmin, inv};
+  md.gvar = DGrid{variance_grid ? mem + cells : nullptr, resolution, bmin, inv};
+  md.noise_scale = noise_scale;
+  update_medium_flags(scene->h);
   MUPSI_CUDA(cudaMemcpy(scene->d, &scene->h, sizeof(DScene), cudaMemcpyHostToDevice));
   return MUPSI_OK;
 }

@@ -26,7 +26,15 @@ struct DPrim {
   const int32_t* face_uv;
   int tex_w, tex_h;
 };
+// GridMeanFunction (gp/meanfunction.h:45-55): res^3 float samples, x-major,
+// over [bmin, bmax]; inv = res / (bmax - bmin)
+struct DGrid {
+  const float* data;
+  int res;
+  v3 bmin, inv;
+};
 struct DMedium {
+  int kind;  // mupsi_medium_kind
   int mean_type;
   int mesh;
   v3 center;
@@ -41,6 +49,9 @@ struct DMedium {
   int surr_max;  // predictions per march
   int every_step;  // mesh mean queried exactly at every visited step (the plain form; no lazy mean)
   float surr_band, surr_scale, surr_add;
+  // ExternalGPMedium: mean and variance grids (gvar.data null: deterministic)
+  DGrid gmean, gvar;
+  float noise_scale;
 };
 
 // error bits raised by device code
@@ -71,6 +82,7 @@ struct DScene {
   unsigned long long* counters;  // nullable: [0] march steps visited, [1] psi evaluations, [2] marches
   int min_group;                 // smallest lane group per march
   int sphere_only;               // every mean is a sphere: the march kernel without BVH code
+  int field;                     // some medium is an SDF or external GP medium (k_march_field)
 };
 
 // ------------------------------------------------------------ mean functions
@@ -120,6 +132,191 @@ MD float4 medium_eval(const DScene* S, const DMedium& md, v3 p, uint32_t seed, c
   float4 nz = raw_noise(md.k, p, seed);
   float4 f = make_float4(mu.x + nz.x, mu.y + nz.y, mu.z + nz.z, mu.w + nz.w);
   return add_cond(md.k, c, p, f);
+}
+
+// ------------------------------------------------------------ field media
+// SDFMedium (sdfmedium.cpp:16-98) and ExternalGPMedium (externalgpmedium.cpp:
+// 9-130) march a scalar field by sphere tracing (step max(|f|, min_step)) and
+// refine a sign change by 16 bisections. Both take the mean functions above or
+// a GridMeanFunction; the conditioning state plays no part.
+
+// float -> int as the reference's x86 build converts: out of range and NaN give
+// INT_MIN (the GPU's own conversion saturates)
+MD int f2i_x86(float f) { return (f >= -2147483648.0f && f < 2147483648.0f) ? (int)f : (int)0x80000000u; }
+MD float clamp_std(float v, float lo, float hi) { return (v < lo) ? lo : ((hi < v) ? hi : v); }  // std::clamp
+
+// GridMeanFunction::eval (meanfunction.cpp:58-78): trilinear, clamped to the grid
+MD float grid_eval(const DGrid& g, v3 p) {
+  const float fx = (p.x - g.bmin.x) * g.inv.x - 0.5f;
+  const float fy = (p.y - g.bmin.y) * g.inv.y - 0.5f;
+  const float fz = (p.z - g.bmin.z) * g.inv.z - 0.5f;
+  const int i0 = max(0, min(g.res - 2, f2i_x86(floorf(fx))));
+  const int j0 = max(0, min(g.res - 2, f2i_x86(floorf(fy))));
+  const int k0 = max(0, min(g.res - 2, f2i_x86(floorf(fz))));
+  const float wx = clamp_std(fx - (float)i0, 0.0f, 1.0f);
+  const float wy = clamp_std(fy - (float)j0, 0.0f, 1.0f);
+  const float wz = clamp_std(fz - (float)k0, 0.0f, 1.0f);
+  const int64_t sy = g.res, sx = (int64_t)g.res * g.res;
+  const float* a = g.data + i0 * sx + j0 * sy + k0;  // (i0, j0, k0); +sx: i1, +sy: j1, +1: k1
+  const float c00 = __ldg(a) * (1.0f - wx) + __ldg(a + sx) * wx;
+  const float c01 = __ldg(a + 1) * (1.0f - wx) + __ldg(a + sx + 1) * wx;
+  const float c10 = __ldg(a + sy) * (1.0f - wx) + __ldg(a + sx + sy) * wx;
+  const float c11 = __ldg(a + sy + 1) * (1.0f - wx) + __ldg(a + sx + sy + 1) * wx;
+  const float c0 = c00 * (1.0f - wy) + c10 * wy;
+  const float c1 = c01 * (1.0f - wy) + c11 * wy;
+  return c0 * (1.0f - wz) + c1 * wz;
+}
+// GridMeanFunction::gradient (meanfunction.cpp:80-86): central differences, eps 1e-4
+MD v3 grid_gradient(const DGrid& g, v3 p) {
+  const float e = 1e-4f;
+  const float dx = grid_eval(g, mk3(p.x + e, p.y, p.z)) - grid_eval(g, mk3(p.x - e, p.y, p.z));
+  const float dy = grid_eval(g, mk3(p.x, p.y + e, p.z)) - grid_eval(g, mk3(p.x, p.y - e, p.z));
+  const float dz = grid_eval(g, mk3(p.x, p.y, p.z + e)) - grid_eval(g, mk3(p.x, p.y, p.z - e));
+  return mk3(dx, dy, dz) / (2.0f * e);
+}
+// hash11 (externalgpmedium.cpp:9-18): the coordinates' bit patterns folded
+// into the seed, finalised, mapped to [-1, 1]
+MD float hash11(v3 p, uint32_t seed) {
+  uint32_t h = seed;
+  h = h * 0x9e3779b1u + __float_as_uint(p.x);
+  h = h * 0x9e3779b1u + __float_as_uint(p.y);
+  h = h * 0x9e3779b1u + __float_as_uint(p.z);
+  h = (h ^ (h >> 16)) * 0x85ebca6bu;
+  h = (h ^ (h >> 13)) * 0xc2b2ae35u;
+  h = h ^ (h >> 16);
+  return (float)(h & 0xFFFFFFu) / 16777215.0f * 2.0f - 1.0f;
+}
+// ExternalGPMedium::evalWithGradient(p, seed).x (externalgpmedium.cpp:33-58)
+MD float ext_value(const DMedium& md, v3 p, uint32_t seed) {
+  const float mu = grid_eval(md.gmean, p);
+  float noise = 0.0f;
+  if (md.gvar.data && md.noise_scale > 0.0f) {
+    const float var = grid_eval(md.gvar, p);
+    if (var > 0.0f) noise = (md.noise_scale * sqrtf(var)) * hash11(p, seed);
+  }
+  return mu + noise;
+}
+// ExternalGPMedium::evalWithGradient(p, seed): value and gradient
+MD float4 ext_value_grad(const DMedium& md, v3 p, uint32_t seed) {
+  const float mu = grid_eval(md.gmean, p);
+  const v3 mg = grid_gradient(md.gmean, p);
+  float noise = 0.0f;
+  v3 ng = mk3(0.0f, 0.0f, 0.0f);
+  if (md.gvar.data && md.noise_scale > 0.0f) {
+    const float var = grid_eval(md.gvar, p);
+    if (var > 0.0f) {
+      const float amp = md.noise_scale * sqrtf(var);
+      noise = amp * hash11(p, seed);
+      const float e = 0.01f;
+      ng.x = amp * (hash11(mk3(p.x + e, p.y, p.z), seed) - hash11(mk3(p.x - e, p.y, p.z), seed)) / (2.0f * e);
+      ng.y = amp * (hash11(mk3(p.x, p.y + e, p.z), seed) - hash11(mk3(p.x, p.y - e, p.z), seed)) / (2.0f * e);
+      ng.z = amp * (hash11(mk3(p.x, p.y, p.z + e), seed) - hash11(mk3(p.x, p.y, p.z - e), seed)) / (2.0f * e);
+    }
+  }
+  return make_float4(mu + noise, mg.x + ng.x, mg.y + ng.y, mg.z + ng.z);
+}
+// value of a field medium: SDFMedium::eval is the mean function itself
+MD float field_value(const DScene* S, const DMedium& md, v3 p, uint32_t seed, bool& ovf) {
+  return md.kind == MUPSI_MEDIUM_SDF ? mean_value(S, md, p, ovf) : ext_value(md, p, seed);
+}
+MD float4 field_value_grad(const DScene* S, const DMedium& md, v3 p, uint32_t seed, bool& ovf) {
+  return md.kind == MUPSI_MEDIUM_SDF ? mean_value_grad(S, md, p, ovf) : ext_value_grad(md, p, seed);
+}
+
+// SDFMedium::sampleDistance (sdfmedium.cpp:16-63) / ExternalGPMedium::
+// sampleDistance (externalgpmedium.cpp:69-109). A hit's normal is the
+// normalised gradient there. Kept out of line: only field media reach it.
+__device__ __noinline__ void field_sample_distance(const DScene* S, const DMedium& md, v3 o, v3 d, float nt, float ft,
+                                                   uint32_t seed, mupsi_medium_sample& out, bool& ovf) {
+  ft = fmin_std(ft, 2000.0f);
+  out.exited = 1u;
+  out.t = 0.0f;
+  out.p[0] = out.p[1] = out.p[2] = 0.0f;
+  out.normal[0] = out.normal[1] = out.normal[2] = 0.0f;
+  float hit_t = 0.0f;
+  bool hit = false;
+  float t = nt;
+  if (md.kind == MUPSI_MEDIUM_SDF) {
+    float fc = field_value(S, md, o, seed, ovf);
+    for (int iter = 0; t < ft && iter < 512; ++iter) {
+      const float fp = fc, tp = t;
+      fc = field_value(S, md, o + d * t, seed, ovf);
+      if (fp * fc < 0.0f) {
+        float lo = tp, hi = t, flo = fp;
+        for (int b = 0; b < 16; ++b) {
+          const float mid = (lo + hi) * 0.5f;
+          const float fm = field_value(S, md, o + d * mid, seed, ovf);
+          if (flo * fm <= 0.0f) {
+            hi = mid;
+          } else {
+            lo = mid;
+            flo = fm;
+          }
+        }
+        hit_t = hi;
+        hit = true;
+        break;
+      }
+      t += fmax_std(fabsf(fc), 1e-3f);
+    }
+  } else {
+    float fp = field_value(S, md, o, seed, ovf);
+    for (int iter = 0; iter < 1024 && t < ft; ++iter) {
+      const float fc = field_value(S, md, o + d * t, seed, ovf);
+      if ((fc > 0.0f) != (fp > 0.0f) && fabsf(fp - fc) > 1e-6f) {
+        float lo = t - fmax_std(fabsf(fp), 0.005f), hi = t;
+        for (int b = 0; b < 16; ++b) {
+          const float mid = (lo + hi) * 0.5f;
+          const float fm = field_value(S, md, o + d * mid, seed, ovf);
+          if ((fm > 0.0f) == (fp > 0.0f))
+            lo = mid;
+          else
+            hi = mid;
+        }
+        hit_t = hi;
+        hit = true;
+        break;
+      }
+      const float step = fmax_std(fabsf(fc), 0.005f);
+      fp = fc;
+      t += step;
+    }
+  }
+  if (hit) {
+    const v3 p = o + d * hit_t;
+    const float4 f = field_value_grad(S, md, p, seed, ovf);
+    const v3 n = normalized(mk3(f.y, f.z, f.w));
+    out.exited = 0u;
+    out.t = hit_t;
+    st3(out.p, p);
+    st3(out.normal, n);
+  }
+}
+
+// SDFMedium::transmittance (sdfmedium.cpp:65-96) / ExternalGPMedium::
+// transmittance (externalgpmedium.cpp:111-130): 0 at the first sign change.
+__device__ __noinline__ float field_transmittance(const DScene* S, const DMedium& md, v3 o, v3 d, float nt, float ft,
+                                                  uint32_t seed, bool& ovf) {
+  ft = fmin_std(ft, 2000.0f);
+  float t = nt;
+  if (md.kind == MUPSI_MEDIUM_SDF) {
+    float fc = field_value(S, md, o, seed, ovf);
+    for (int iter = 0; t < ft && iter < 512; ++iter) {
+      const float fp = fc;
+      fc = field_value(S, md, o + d * t, seed, ovf);
+      if (fp * fc < 0.0f) return 0.0f;
+      t += fmax_std(fabsf(fc), 1e-3f);
+    }
+  } else {
+    float fp = field_value(S, md, o, seed, ovf);
+    for (int iter = 0; iter < 1024 && t < ft; ++iter) {
+      const float fc = field_value(S, md, o + d * t, seed, ovf);
+      if ((fc > 0.0f) != (fp > 0.0f) && fabsf(fp - fc) > 1e-6f) return 0.0f;
+      fp = fc;
+      t += fmax_std(fabsf(fc), 0.005f);
+    }
+  }
+  return 1.0f;
 }
 
 // ------------------------------------------------------------------ march

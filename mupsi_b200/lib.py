@@ -64,6 +64,9 @@ def _setup(L):
     L.mupsi_gpu_scene_set_occlusion.argtypes = [vp, i32]
     L.mupsi_gpu_scene_set_sky_texture.argtypes = [vp, i32, i32, vp]
     L.mupsi_gpu_scene_set_albedo_texture.argtypes = [vp, i32, i64, vp, vp, i32, i32, vp]
+    L.mupsi_gpu_scene_set_sdf_medium.argtypes = [vp, i32]
+    L.mupsi_gpu_scene_set_external_gp_medium.argtypes = [vp, i32, i32, vp, vp, vp, vp, C.c_float]
+    L.mupsi_gpu_transmittance.argtypes = [vp, i32, i64, vp, vp, vp, vp, C.c_int, vp]
     return L
 
 

@@ -9,6 +9,7 @@ import ctypes as C
 import json
 import math
 import os
+import warnings
 
 import numpy as np
 
@@ -141,10 +142,33 @@ class Scene:
 
     # -- construction helpers -------------------------------------------------
     def add_medium(self, mean_type="sphere", center=(0, 0, 0), radius=70.0, mesh=-1, sigma=1.0, length_scale=1.0,
-                   aniso=(1.0, 1.0, 1.0), points_per_cell=3):
-        self.media.append(dict(mean_type=_abi.MEAN_SPHERE if mean_type == "sphere" else _abi.MEAN_MESH,
+                   aniso=(1.0, 1.0, 1.0), points_per_cell=3, kind="gp"):
+        """A GPMedium (kind "gp") over a sphere or mesh mean with an SE kernel,
+        or an SDFMedium (kind "sdf": the mean itself is the field; the kernel
+        is unused)."""
+        if kind not in ("gp", "sdf"):
+            raise ValueError(f"unknown medium kind {kind!r}")
+        self.media.append(dict(kind=kind, mean_type=_abi.MEAN_SPHERE if mean_type == "sphere" else _abi.MEAN_MESH,
                                center=tuple(center), radius=float(radius), mesh=int(mesh), sigma=float(sigma),
                                length=float(length_scale), aniso=tuple(aniso), ppc=int(points_per_cell)))
+        return len(self.media) - 1
+
+    def add_external_gp_medium(self, resolution, bounds_min, bounds_max, mean_grid, variance_grid=None,
+                               noise_scale=1.0):
+        """An ExternalGPMedium (medium/externalgpmedium.h): GridMeanFunction mean
+        and variance grids of resolution^3 float32 samples, x-major
+        ((i * res + j) * res + k), over [bounds_min, bounds_max];
+        variance_grid None: no noise."""
+        res = int(resolution)
+        cells = res ** 3
+        mg = np.ascontiguousarray(mean_grid, np.float32).reshape(-1)
+        vg = None if variance_grid is None else np.ascontiguousarray(variance_grid, np.float32).reshape(-1)
+        if res < 2 or mg.size != cells or (vg is not None and vg.size != cells):
+            raise ValueError("grids need resolution^3 samples, resolution >= 2")
+        self.media.append(dict(kind="external_gp", mean_type=_abi.MEAN_SPHERE, center=(0.0, 0.0, 0.0), radius=1.0,
+                               mesh=-1, sigma=1.0, length=1.0, aniso=(1.0, 1.0, 1.0), ppc=3, res=res,
+                               bmin=tuple(float(v) for v in bounds_min), bmax=tuple(float(v) for v in bounds_max),
+                               mean_grid=mg, var_grid=vg, noise_scale=float(noise_scale)))
         return len(self.media) - 1
 
     def add_mesh(self, mesh):
@@ -199,6 +223,8 @@ class Scene:
         s.cam_fov = float(cam.get("fov", 45.0))
         s.gp_mode = _abi.GP_RENEWAL_PLUS if j.get("gp_mode", "single_realization") == "renewal_plus" \
             else _abi.GP_SINGLE_REALIZATION
+        # the medium of `int_medium` primitives: gp_medium, else sdf_medium, else
+        # external_gp_medium (controller.cpp:225-229)
         gpm_index = -1
         if "gp_medium" in j:
             g = j["gp_medium"]
@@ -215,9 +241,31 @@ class Scene:
                 gpm_index = s.add_medium("mesh", mesh=mi, **kw)
             else:
                 raise ValueError(f"unknown mean_type: {mt}")
-        for key in ("sdf_medium", "external_gp_medium"):
-            if key in j:
-                raise NotImplementedError(f"{key} is not part of the GPIS GPU path")
+        elif "sdf_medium" in j:  # controller.cpp:154-182
+            g = j["sdf_medium"]
+            mt = g.get("mean_type", "sphere")
+            if mt == "sphere":
+                gpm_index = s.add_medium("sphere", center=g["mean_center"], radius=g.get("mean_radius", 70.0),
+                                         kind="sdf")
+            elif mt == "mesh":
+                v, f, n = load_obj(_resolve(base_dir, g["file"]))
+                t = g.get("transform", {})
+                mi = s.add_mesh(Mesh(v, f, n, position=t.get("position", (0, 0, 0)), scale=t.get("scale", 1.0)))
+                gpm_index = s.add_medium("mesh", mesh=mi, kind="sdf")
+            else:
+                raise ValueError(f"unknown sdf_medium mean_type: {mt}")
+        elif "external_gp_medium" in j:  # controller.cpp:184-189
+            g = j["external_gp_medium"]
+            res = int(g.get("resolution", 48))
+            # grid files: the config's directory + the name, as a string
+            # (an absolute name too ends up under that directory)
+            cdir = base_dir.rstrip("/") + "/"
+            mean = load_grid(cdir + g["mean_file"], res)
+            var = None
+            if g.get("variance_file", ""):
+                var = load_grid(cdir + g["variance_file"], res)
+            gpm_index = s.add_external_gp_medium(res, g["bounds_min"], g["bounds_max"], mean, var,
+                                                 g.get("noise_scale", 1.0))
         if "skydrome" in j:
             s.sky_texture = load_texture_image(_resolve(base_dir, j["skydrome"]))
         if sky is not None:
@@ -273,12 +321,13 @@ class Scene:
         self._keep = [media, meshes, prims]
         return d
 
-    def to_json(self, obj_paths=None, sky_path=None, texture_paths=None):
+    def to_json(self, obj_paths=None, sky_path=None, texture_paths=None, grid_paths=None):
         """scene.json dict the reference's Controller::load accepts for this scene
         (meshes must have been written to `obj_paths` with their texcoords, a sky
         texture to `sky_path` and albedo textures to `texture_paths`, a dict
-        primitive index -> path, with save_image_raw). Returns (dict,
-        extra_meshes): primitives the schema cannot express (non-default
+        primitive index -> path, with save_image_raw; an external GP medium's
+        grids to `grid_paths` = (mean, variance or None), named relative to the
+        config's directory). Returns (dict, extra_meshes): primitives the schema cannot express (non-default
         albedo) are returned as (obj_path, albedo) pairs for a harness to add."""
         j = {"width": self.width, "height": self.height, "spp": self.spp, "max_bounce": self.max_bounce,
              "max_medium_bounce": self.max_medium_bounce,
@@ -292,16 +341,26 @@ class Scene:
             j["skydrome"] = sky_path
         if self.media:
             if len(self.media) > 1:
-                raise ValueError("scene.json holds one gp_medium")
+                raise ValueError("scene.json holds one medium")
             m = self.media[0]
-            j["kernel"] = {"sigma": m["sigma"], "length_scale": m["length"], "aniso": list(m["aniso"]),
-                           "points_per_cell": m["ppc"]}
-            if m["mean_type"] == _abi.MEAN_SPHERE:
-                j["gp_medium"] = {"mean_type": "sphere", "mean_center": list(m["center"]), "mean_radius": m["radius"]}
+            kind = m.get("kind", "gp")
+            if kind == "external_gp":
+                eg = {"resolution": m["res"], "bounds_min": list(m["bmin"]), "bounds_max": list(m["bmax"]),
+                      "noise_scale": m["noise_scale"], "mean_file": grid_paths[0]}
+                if m["var_grid"] is not None:
+                    eg["variance_file"] = grid_paths[1]
+                j["external_gp_medium"] = eg
             else:
-                mm = self.meshes[m["mesh"]]
-                j["gp_medium"] = {"mean_type": "mesh", "file": obj_paths[m["mesh"]],
-                                  "transform": {"position": list(mm.position), "scale": mm.scale}}
+                key = "gp_medium" if kind == "gp" else "sdf_medium"
+                if kind == "gp":
+                    j["kernel"] = {"sigma": m["sigma"], "length_scale": m["length"], "aniso": list(m["aniso"]),
+                                   "points_per_cell": m["ppc"]}
+                if m["mean_type"] == _abi.MEAN_SPHERE:
+                    j[key] = {"mean_type": "sphere", "mean_center": list(m["center"]), "mean_radius": m["radius"]}
+                else:
+                    mm = self.meshes[m["mesh"]]
+                    j[key] = {"mean_type": "mesh", "file": obj_paths[m["mesh"]],
+                              "transform": {"position": list(mm.position), "scale": mm.scale}}
         names = {_abi.BSDF_LAMBERTIAN: "lambertian", _abi.BSDF_NULL: "null", _abi.BSDF_SPECULAR: "specular"}
         for pi, p in enumerate(self.primitives):
             if p["type"] == _abi.PRIM_SPHERE:
@@ -325,6 +384,23 @@ class Scene:
                             pj["transform"] = {"position": list(mm.position), "scale": mm.scale}
                     j["primitives"].append(pj)
         return j, extra
+
+
+def load_grid(path, res):
+    """A GridMeanFunction file (meanfunction.cpp:41-56): res^3 float32, x-major.
+    As the reference, a short or missing file leaves the remaining samples 0
+    (with a warning here)."""
+    cells = res ** 3
+    out = np.zeros(cells, np.float32)
+    try:
+        with open(path, "rb") as fh:
+            data = np.frombuffer(fh.read(cells * 4), np.float32)
+    except OSError:
+        data = np.zeros(0, np.float32)
+    if data.size < cells:
+        warnings.warn(f"GridMeanFunction {path}: {data.size} of {cells} samples; the rest are 0")
+    out[:data.size] = data
+    return out
 
 
 def load_texture_image(path):
@@ -514,6 +590,56 @@ def textured_floor_scene(texture, with_texcoords=True, width=24, height=24, spp=
     fm = sc.add_mesh(Mesh(fv, ff, texcoords=tc, face_texcoords=ftc))
     sc.add_mesh_primitive(fm, texture=texture)
     return sc
+
+
+def external_gp_grids(res=16, seed=0, center=(0.0, 0.0, -500.0), radius=70.0, half=130.0):
+    """Seeded GridMeanFunction samples for an ExternalGPMedium over the cube of
+    half-width `half` around `center`: mean = distance to the sphere of
+    `radius` plus a smooth seeded ripple of amplitude 6, variance ~ U(0.2, 2).
+    Returns (bounds_min, bounds_max, mean, variance), grids (res, res, res)."""
+    rng = np.random.default_rng(seed)
+    c = np.asarray(center, np.float64)
+    bmin, bmax = c - half, c + half
+    ax = [bmin[a] + (np.arange(res) + 0.5) * (2 * half / res) for a in range(3)]
+    X, Y, Z = np.meshgrid(*ax, indexing="ij")
+    ph = rng.uniform(0, 2 * np.pi, 3)
+    mean = (np.sqrt((X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2) - radius
+            + 6.0 * np.sin(X / 23.0 + ph[0]) * np.sin(Y / 19.0 + ph[1]) * np.sin(Z / 29.0 + ph[2]))
+    var = rng.uniform(0.2, 2.0, (res, res, res))
+    return (tuple(np.float32(bmin).tolist()), tuple(np.float32(bmax).tolist()), mean.astype(np.float32),
+            var.astype(np.float32))
+
+
+def field_scene(kind, width=24, height=24, spp=2, seed=0):
+    """Configuration 0's layout (null sphere of radius 130 at (0, 0, -500),
+    constant sky 1.0, 10 bounces) seen from (0, 0, -250) along -z, so that
+    every pixel enters the null sphere, with a field medium inside it, plus an emissive Lambertian sphere so that
+    next-event estimation crosses the medium's transmittance:
+    "sdf_sphere": SDFMedium over the sphere mean of radius 70;
+    "sdf_mesh": SDFMedium over a displaced icosphere (level 2, radius 60);
+    "external_gp": ExternalGPMedium over external_gp_grids(16, seed), noise scale 1;
+    "external_gp_mean": the same without the variance grid (no noise)."""
+    s = Scene()
+    s.width, s.height, s.spp = width, height, spp
+    s.max_bounce = 10
+    s.max_medium_bounce = 10
+    s.gp_mode = _abi.GP_RENEWAL_PLUS
+    s.sky = (1.0, 1.0, 1.0)
+    s.cam_pos = (0.0, 0.0, -250.0)
+    c = (0.0, 0.0, -500.0)
+    if kind == "sdf_sphere":
+        m = s.add_medium("sphere", center=c, radius=70.0, kind="sdf")
+    elif kind == "sdf_mesh":
+        v, f = displaced_icosphere(2, radius=60.0, center=c, seed=seed)
+        m = s.add_medium("mesh", mesh=s.add_mesh(Mesh(v, f)), kind="sdf")
+    elif kind in ("external_gp", "external_gp_mean"):
+        bmin, bmax, mean, var = external_gp_grids(16, seed, c)
+        m = s.add_external_gp_medium(16, bmin, bmax, mean, var if kind == "external_gp" else None, 1.0)
+    else:
+        raise ValueError(f"unknown field scene {kind!r}")
+    s.add_sphere(c, 130.0, bsdf=_abi.BSDF_NULL, int_medium=m)
+    s.add_sphere((40.0, 160.0, -380.0), 45.0, emission=(6.0, 5.0, 4.0))
+    return s
 
 
 def config_mesh_scene(level=6, width=512, height=512, spp=64, seed=0):

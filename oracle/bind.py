@@ -78,6 +78,10 @@ class _Port:
         L.mo_medium_eval.argtypes = [C.c_void_p, C.c_int, C.c_int64, _f32, _u32, C.c_void_p, _f32]
         L.mo_sample_distance.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.c_void_p, _u32, C.c_void_p, C.c_void_p]
         L.mo_sample_condition.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.c_void_p, _u32, C.c_void_p]
+        L.mo_transmittance.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.c_void_p, _u32, C.c_void_p, _f32]
+        L.mo_scene_set_sdf_medium.argtypes = [C.c_void_p, C.c_int]
+        L.mo_scene_set_external_gp_medium.argtypes = [C.c_void_p, C.c_int, C.c_int, _f32, _f32, _f32, C.c_void_p,
+                                                      C.c_float]
         L.mo_trace.argtypes = [C.c_void_p, C.c_int64, _i32, _i32, _i32, _f32]
         L.mo_trace_work.argtypes = [C.c_void_p, C.c_int64, _i32, _i32, _i32, _i64]
         L.mo_scene_set_sky_texture.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
@@ -219,6 +223,12 @@ class PortOracle:
     def scene_from(self, sc):
         """scene_create(sc.desc()) plus the scene's sky and albedo textures."""
         h = self.scene_create(sc.desc())
+        for i, m in enumerate(sc.media):
+            if m.get("kind") == "sdf":
+                self.scene_set_sdf(h, i)
+            elif m.get("kind") == "external_gp":
+                self.scene_set_external_gp(h, i, m["res"], m["bmin"], m["bmax"], m["mean_grid"], m["var_grid"],
+                                           m["noise_scale"])
         if getattr(sc, "sky_texture", None) is not None:
             self.scene_set_sky(h, sc.sky_texture)
         for i, p in enumerate(sc.primitives):
@@ -284,6 +294,24 @@ class PortOracle:
         res[:, 0] = out.view(np.uint32)[:, 0].astype(np.float32)
         return res
 
+    def transmittance(self, h, medium, rays, seed, cond=None):
+        rays = ray_array(rays)
+        out = np.zeros(len(rays), np.float32)
+        ca = cond_array(cond)
+        self.L.mo_transmittance(h, medium, len(rays), rays.ctypes.data, _u(seed),
+                                None if ca is None else ca.ctypes.data, out)
+        return out
+
+    def scene_set_sdf(self, h, medium):
+        if self.L.mo_scene_set_sdf_medium(h, medium) != 0:
+            raise ValueError("bad medium")
+
+    def scene_set_external_gp(self, h, medium, res, bmin, bmax, mean, var=None, noise_scale=1.0):
+        v = None if var is None else _f(var).reshape(-1)
+        if self.L.mo_scene_set_external_gp_medium(h, medium, res, _f(bmin), _f(bmax), _f(mean).reshape(-1),
+                                                  None if v is None else v.ctypes.data, noise_scale) != 0:
+            raise ValueError("bad external GP medium")
+
     def sample_condition(self, h, medium, samples, seed):
         """samples: (n, 7) [exited, p xyz, normal xyz] -> (n, 8) [C, u, g, active]"""
         samples = np.asarray(samples, np.float32)
@@ -338,6 +366,14 @@ class RefOracle:
         L.ref_sample_condition.argtypes = [C.c_void_p, C.c_long, _f32, _u32, C.c_int, _f32]
         L.ref_bvh_build.restype = C.c_void_p
         L.ref_bvh_build.argtypes = [C.c_long, _f32, C.c_long, _i32]
+        L.ref_field_create.restype = C.c_void_p
+        L.ref_field_create.argtypes = [C.c_int, C.c_int, _f32, C.c_float, C.c_char_p, C.c_void_p, C.c_float, C.c_int,
+                                       _f32, _f32, C.c_char_p, C.c_char_p, C.c_float]
+        L.ref_field_free.argtypes = [C.c_void_p]
+        L.ref_field_eval.argtypes = [C.c_void_p, C.c_long, _f32, _u32, _f32]
+        L.ref_field_sample_distance.argtypes = [C.c_void_p, C.c_long, _f32, _u32, _f32]
+        L.ref_field_transmittance.argtypes = [C.c_void_p, C.c_long, _f32, _u32, _f32]
+        L.ref_grid_eval.argtypes = [C.c_char_p, C.c_int, _f32, _f32, C.c_long, _f32, _f32]
         L.ref_bvh_free.argtypes = [C.c_void_p]
         L.ref_bvh_node_count.restype = C.c_long
         L.ref_bvh_node_count.argtypes = [C.c_void_p]
@@ -404,6 +440,51 @@ class RefOracle:
 
     def medium_free(self, h):
         self.L.ref_medium_free(h)
+
+    def sdf_create(self, mean_type, center=(0, 0, 0), radius=70.0, obj_path=None, mesh_pos=None, mesh_scale=1.0):
+        """SDFMedium over a SphereMeanFunction (0) or MeshMeanFunction (1)."""
+        mp = _f(mesh_pos) if mesh_pos is not None else None
+        h = self.L.ref_field_create(1, mean_type, _f(center), radius, obj_path.encode() if obj_path else None,
+                                    mp.ctypes.data if mp is not None else None, mesh_scale, 0, _f([0, 0, 0]),
+                                    _f([1, 1, 1]), None, None, 0.0)
+        if not h:
+            raise RuntimeError("reference SDF medium could not be created")
+        return h
+
+    def external_gp_create(self, res, bmin, bmax, mean_path, var_path=None, noise_scale=1.0):
+        """ExternalGPMedium over GridMeanFunction files (float32, x-major)."""
+        h = self.L.ref_field_create(2, 0, _f([0, 0, 0]), 0.0, None, None, 1.0, res, _f(bmin), _f(bmax),
+                                    mean_path.encode(), var_path.encode() if var_path else None, noise_scale)
+        if not h:
+            raise RuntimeError("reference external GP medium could not be created")
+        return h
+
+    def field_free(self, h):
+        self.L.ref_field_free(h)
+
+    def field_eval(self, h, p, seed):
+        p = _f(p)
+        out = np.zeros((len(p), 4), np.float32)
+        self.L.ref_field_eval(h, len(p), p, _u(seed), out)
+        return out
+
+    def field_sample_distance(self, h, rays, seed):
+        rays = _f(rays)
+        out = np.zeros((len(rays), 8), np.float32)
+        self.L.ref_field_sample_distance(h, len(rays), rays, _u(seed), out)
+        return out
+
+    def field_transmittance(self, h, rays, seed):
+        rays = _f(rays)
+        out = np.zeros(len(rays), np.float32)
+        self.L.ref_field_transmittance(h, len(rays), rays, _u(seed), out)
+        return out
+
+    def grid_eval(self, path, res, bmin, bmax, p):
+        p = _f(p)
+        out = np.zeros((len(p), 4), np.float32)
+        self.L.ref_grid_eval(path.encode(), res, _f(bmin), _f(bmax), len(p), p, out)
+        return out
 
     def mean(self, h, p):
         p = _f(p)

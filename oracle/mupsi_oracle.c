@@ -50,6 +50,11 @@ static inline float fmax_std(float a, float b) { return (a < b) ? b : a; } /* st
 static inline float vmaxc(v3 a) { return fmax_std(a.x, fmax_std(a.y, a.z)); }
 static inline float vget(v3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
 static inline v3 vload(const float* p) { return V3(p[0], p[1], p[2]); }
+static inline void vstore(float* p, v3 a) {
+  p[0] = a.x;
+  p[1] = a.y;
+  p[2] = a.z;
+}
 
 /* 4x4 matrices, column-major like Eigen; products reduce over k by halves. */
 typedef struct {
@@ -536,9 +541,19 @@ typedef struct {
   int32_t* face_uv;
 } oprim;
 
+/* GridMeanFunction (meanfunction.h:45-55): res^3 samples, x-major */
+typedef struct {
+  float* data;
+  int res;
+  v3 bmin, inv;
+} ogrid;
+
 typedef struct {
   mupsi_medium_desc d;
   kparams k;
+  int kind; /* mupsi_medium_kind */
+  ogrid gmean, gvar; /* ExternalGPMedium grids (gvar.data NULL: no noise) */
+  float noise_scale;
 } omedium;
 
 struct mo_scene {
@@ -661,6 +676,10 @@ void mo_scene_free(mo_scene* s) {
   }
   free(s->prims);
   free(s->lights);
+  for (int i = 0; i < s->nmed; ++i) {
+    free(s->media[i].gmean.data);
+    free(s->media[i].gvar.data);
+  }
   free(s->media);
   free(s->sky_tex);
   free(s);
@@ -1077,13 +1096,98 @@ static f4 medium_eval(const mo_scene* s, const omedium* md, v3 p, uint32_t seed,
   return add_cond(&md->k, f, p, c);
 }
 
+/* ------------------------------------------- field media evaluation -- */
+static float clamp_std(float v, float lo, float hi) { return (v < lo) ? lo : ((hi < v) ? hi : v); }
+static int imin(int a, int b) { return a < b ? a : b; }
+static int imax(int a, int b) { return a < b ? b : a; }
+/* (int)f as x86's cvttss2si: out of range / NaN -> INT_MIN (C leaves it undefined) */
+static int f2i(float f) { return (f >= -2147483648.0f && f < 2147483648.0f) ? (int)f : INT32_MIN; }
+
+/* GridMeanFunction::eval (meanfunction.cpp:58-78) */
+static float grid_eval(const ogrid* g, v3 p) {
+  float fx = (p.x - g->bmin.x) * g->inv.x - 0.5f;
+  float fy = (p.y - g->bmin.y) * g->inv.y - 0.5f;
+  float fz = (p.z - g->bmin.z) * g->inv.z - 0.5f;
+  int i0 = imax(0, imin(g->res - 2, f2i(floorf(fx))));
+  int j0 = imax(0, imin(g->res - 2, f2i(floorf(fy))));
+  int k0 = imax(0, imin(g->res - 2, f2i(floorf(fz))));
+  int i1 = i0 + 1, j1 = j0 + 1, k1 = k0 + 1;
+  float wx = clamp_std(fx - (float)i0, 0.0f, 1.0f);
+  float wy = clamp_std(fy - (float)j0, 0.0f, 1.0f);
+  float wz = clamp_std(fz - (float)k0, 0.0f, 1.0f);
+  size_t sy = (size_t)g->res, sx = (size_t)g->res * g->res;
+#define AT(i, j, k) g->data[(size_t)(i) * sx + (size_t)(j) * sy + (size_t)(k)]
+  float c00 = AT(i0, j0, k0) * (1 - wx) + AT(i1, j0, k0) * wx;
+  float c01 = AT(i0, j0, k1) * (1 - wx) + AT(i1, j0, k1) * wx;
+  float c10 = AT(i0, j1, k0) * (1 - wx) + AT(i1, j1, k0) * wx;
+  float c11 = AT(i0, j1, k1) * (1 - wx) + AT(i1, j1, k1) * wx;
+#undef AT
+  float c0 = c00 * (1 - wy) + c10 * wy;
+  float c1 = c01 * (1 - wy) + c11 * wy;
+  return c0 * (1 - wz) + c1 * wz;
+}
+/* GridMeanFunction::gradient (meanfunction.cpp:80-86) */
+static v3 grid_gradient(const ogrid* g, v3 p) {
+  float eps = 1e-4f;
+  float dx = grid_eval(g, V3(p.x + eps, p.y, p.z)) - grid_eval(g, V3(p.x - eps, p.y, p.z));
+  float dy = grid_eval(g, V3(p.x, p.y + eps, p.z)) - grid_eval(g, V3(p.x, p.y - eps, p.z));
+  float dz = grid_eval(g, V3(p.x, p.y, p.z + eps)) - grid_eval(g, V3(p.x, p.y, p.z - eps));
+  return vdiv(V3(dx, dy, dz), 2.0f * eps);
+}
+/* hash11 (externalgpmedium.cpp:9-18) */
+static float hash11(v3 p, uint32_t seed) {
+  uint32_t h = seed, b;
+  memcpy(&b, &p.x, 4);
+  h = h * 0x9e3779b1u + b;
+  memcpy(&b, &p.y, 4);
+  h = h * 0x9e3779b1u + b;
+  memcpy(&b, &p.z, 4);
+  h = h * 0x9e3779b1u + b;
+  h = (h ^ (h >> 16)) * 0x85ebca6bu;
+  h = (h ^ (h >> 13)) * 0xc2b2ae35u;
+  h = h ^ (h >> 16);
+  return (float)(h & 0xFFFFFFu) / (float)0xFFFFFFu * 2.0f - 1.0f;
+}
+/* ExternalGPMedium::evalWithGradient(p, seed) (externalgpmedium.cpp:33-58) */
+static f4 ext_eval(const omedium* md, v3 p, uint32_t seed) {
+  float mu = grid_eval(&md->gmean, p);
+  v3 mg = grid_gradient(&md->gmean, p);
+  float noise = 0.0f;
+  v3 ng = V3(0.0f, 0.0f, 0.0f);
+  if (md->gvar.data && md->noise_scale > 0.0f) {
+    float var = grid_eval(&md->gvar, p);
+    if (var > 0.0f) {
+      float amp = md->noise_scale * sqrtf(var);
+      noise = amp * hash11(p, seed);
+      float eps = 0.01f;
+      ng.x = amp * (hash11(V3(p.x + eps, p.y, p.z), seed) - hash11(V3(p.x - eps, p.y, p.z), seed)) / (2.0f * eps);
+      ng.y = amp * (hash11(V3(p.x, p.y + eps, p.z), seed) - hash11(V3(p.x, p.y - eps, p.z), seed)) / (2.0f * eps);
+      ng.z = amp * (hash11(V3(p.x, p.y, p.z + eps), seed) - hash11(V3(p.x, p.y, p.z - eps), seed)) / (2.0f * eps);
+    }
+  }
+  f4 f = {mu + noise, mg.x + ng.x, mg.y + ng.y, mg.z + ng.z};
+  return f;
+}
+/* SDFMedium::evalWithGradient (sdfmedium.cpp:10-14) / ExternalGPMedium */
+static f4 field_eval(const mo_scene* s, const omedium* md, v3 p, uint32_t seed) {
+  if (md->kind == MUPSI_MEDIUM_SDF) {
+    v3 g = mean_grad(s, md, p);
+    f4 f = {mean_eval(s, md, p), g.x, g.y, g.z};
+    return f;
+  }
+  return ext_eval(md, p, seed);
+}
+static float field_value(const mo_scene* s, const omedium* md, v3 p, uint32_t seed) {
+  return md->kind == MUPSI_MEDIUM_SDF ? mean_eval(s, md, p) : ext_eval(md, p, seed).v;
+}
 void mo_mean(const mo_scene* s, int medium, int64_t n, const float* p, float* out) {
   const omedium* md = &s->media[medium];
 #pragma omp parallel for schedule(dynamic, 64)
   for (int64_t i = 0; i < n; ++i) {
     v3 P = vload(p + 3 * i);
-    out[4 * i] = mean_eval(s, md, P);
-    v3 g = mean_grad(s, md, P);
+    int grid = md->kind == MUPSI_MEDIUM_EXTERNAL_GP;
+    out[4 * i] = grid ? grid_eval(&md->gmean, P) : mean_eval(s, md, P);
+    v3 g = grid ? grid_gradient(&md->gmean, P) : mean_grad(s, md, P);
     out[4 * i + 1] = g.x;
     out[4 * i + 2] = g.y;
     out[4 * i + 3] = g.z;
@@ -1094,7 +1198,8 @@ void mo_medium_eval(const mo_scene* s, int medium, int64_t n, const float* p, co
   const omedium* md = &s->media[medium];
 #pragma omp parallel for schedule(dynamic, 64)
   for (int64_t i = 0; i < n; ++i) {
-    f4 f = medium_eval(s, md, vload(p + 3 * i), seed[i], cond ? cond + i : NULL);
+    f4 f = md->kind == MUPSI_MEDIUM_GP ? medium_eval(s, md, vload(p + 3 * i), seed[i], cond ? cond + i : NULL)
+                                       : field_eval(s, md, vload(p + 3 * i), seed[i]);
     out[4 * i] = f.v;
     out[4 * i + 1] = f.gx;
     out[4 * i + 2] = f.gy;
@@ -1172,6 +1277,155 @@ static void sample_condition(const mo_scene* s, const omedium* md, const mupsi_m
   }
 }
 
+/* ------------------------------------------------------- field media -- */
+int mo_scene_set_sdf_medium(mo_scene* s, int medium) {
+  if (medium < 0 || medium >= s->nmed) return -1;
+  s->media[medium].kind = MUPSI_MEDIUM_SDF;
+  return 0;
+}
+int mo_scene_set_external_gp_medium(mo_scene* s, int medium, int res, const float* bmin, const float* bmax,
+                                    const float* mean, const float* var, float noise_scale) {
+  if (medium < 0 || medium >= s->nmed || res < 2 || !mean) return -1;
+  omedium* md = &s->media[medium];
+  size_t cells = (size_t)res * res * res;
+  free(md->gmean.data);
+  free(md->gvar.data);
+  md->gmean.data = (float*)malloc(cells * sizeof(float));
+  memcpy(md->gmean.data, mean, cells * sizeof(float));
+  md->gvar.data = NULL;
+  if (var) {
+    md->gvar.data = (float*)malloc(cells * sizeof(float));
+    memcpy(md->gvar.data, var, cells * sizeof(float));
+  }
+  /* inv_cell_size_ = Vector3f(res, res, res).cwiseQuotient(bmax - bmin) (meanfunction.cpp:44) */
+  v3 lo = vload(bmin), hi = vload(bmax);
+  v3 inv = V3((float)res / (hi.x - lo.x), (float)res / (hi.y - lo.y), (float)res / (hi.z - lo.z));
+  md->gmean.res = md->gvar.res = res;
+  md->gmean.bmin = md->gvar.bmin = lo;
+  md->gmean.inv = md->gvar.inv = inv;
+  md->noise_scale = noise_scale;
+  md->kind = MUPSI_MEDIUM_EXTERNAL_GP;
+  return 0;
+}
+
+static float max_std(float a, float b) { return (a < b) ? b : a; }
+
+/* SDFMedium::sampleDistance (sdfmedium.cpp:16-63) */
+static void sdf_sample_distance(const mo_scene* s, const omedium* md, const oray* r, mupsi_medium_sample* out) {
+  float nt = r->nt, ft = fmin_std(r->ft, 2000.0f);
+  const float minStep = 1e-3f;
+  const int maxIter = 512;
+  float t = nt;
+  float f_c = field_value(s, md, r->o, 0);
+  int iter = 0;
+  while (t < ft && iter < maxIter) {
+    v3 p = vadd(r->o, vmul(r->d, t));
+    float f_prev = f_c, t_prev = t;
+    f_c = field_value(s, md, p, 0);
+    if (f_prev * f_c < 0.0f) {
+      float lo = t_prev, hi = t, f_lo = f_prev;
+      for (int b = 0; b < 16; b++) {
+        float mid = (lo + hi) * 0.5f;
+        float f_mid = field_value(s, md, vadd(r->o, vmul(r->d, mid)), 0);
+        if (f_lo * f_mid <= 0.0f) {
+          hi = mid;
+        } else {
+          lo = mid;
+          f_lo = f_mid;
+        }
+      }
+      v3 hp = vadd(r->o, vmul(r->d, hi));
+      f4 f = field_eval(s, md, hp, 0);
+      v3 n = vnormalized(V3(f.gx, f.gy, f.gz));
+      out->exited = 0;
+      out->t = hi;
+      vstore(out->p, hp);
+      vstore(out->normal, n);
+      return;
+    }
+    float step = max_std(fabsf(f_c), minStep);
+    t += step;
+    iter++;
+  }
+  out->exited = 1;
+}
+/* ExternalGPMedium::sampleDistance (externalgpmedium.cpp:69-109) */
+static void ext_sample_distance(const omedium* md, const oray* r, uint32_t seed, mupsi_medium_sample* out) {
+  float nt = r->nt, ft = fmin_std(r->ft, 2000.0f);
+  const float min_step = 0.005f;
+  const int max_iter = 1024;
+  float t = nt;
+  float f_prev = ext_eval(md, r->o, seed).v;
+  for (int iter = 0; iter < max_iter && t < ft; ++iter) {
+    v3 p = vadd(r->o, vmul(r->d, t));
+    float f_c = ext_eval(md, p, seed).v;
+    if ((f_c > 0.0f) != (f_prev > 0.0f) && fabsf(f_prev - f_c) > 1e-6f) {
+      float lo = t - max_std(fabsf(f_prev), min_step);
+      float hi = t;
+      for (int b = 0; b < 16; ++b) {
+        float mid = (lo + hi) * 0.5f;
+        float f_mid = ext_eval(md, vadd(r->o, vmul(r->d, mid)), seed).v;
+        if ((f_mid > 0.0f) == (f_prev > 0.0f))
+          lo = mid;
+        else
+          hi = mid;
+      }
+      v3 hp = vadd(r->o, vmul(r->d, hi));
+      f4 f = ext_eval(md, hp, seed);
+      v3 n = vnormalized(V3(f.gx, f.gy, f.gz));
+      out->exited = 0;
+      out->t = hi;
+      vstore(out->p, hp);
+      vstore(out->normal, n);
+      return;
+    }
+    float step = max_std(fabsf(f_c), min_step);
+    f_prev = f_c;
+    t += step;
+  }
+  out->exited = 1;
+}
+/* SDFMedium::transmittance (sdfmedium.cpp:65-96) / ExternalGPMedium::transmittance
+ * (externalgpmedium.cpp:111-130) */
+static float field_transmittance(const mo_scene* s, const omedium* md, const oray* r, uint32_t seed) {
+  float nt = r->nt, ft = fmin_std(r->ft, 2000.0f);
+  float t = nt;
+  if (md->kind == MUPSI_MEDIUM_SDF) {
+    float f_c = field_value(s, md, r->o, 0);
+    for (int iter = 0; t < ft && iter < 512; iter++) {
+      v3 p = vadd(r->o, vmul(r->d, t));
+      float f_prev = f_c;
+      f_c = field_value(s, md, p, 0);
+      if (f_prev * f_c < 0.0f) return 0.0f;
+      t += max_std(fabsf(f_c), 1e-3f);
+    }
+    return 1.0f;
+  }
+  float f_prev = ext_eval(md, r->o, seed).v;
+  for (int iter = 0; iter < 1024 && t < ft; ++iter) {
+    v3 p = vadd(r->o, vmul(r->d, t));
+    float f_c = ext_eval(md, p, seed).v;
+    if ((f_c > 0.0f) != (f_prev > 0.0f) && fabsf(f_prev - f_c) > 1e-6f) return 0.0f;
+    f_prev = f_c;
+    t += max_std(fabsf(f_c), 0.005f);
+  }
+  return 1.0f;
+}
+/* Medium::sampleDistance / transmittance by medium kind */
+static void any_sample_distance(const mo_scene* s, const omedium* md, const oray* r, uint32_t seed,
+                                const mupsi_cond* c, mupsi_medium_sample* out, int64_t* work) {
+  if (md->kind == MUPSI_MEDIUM_SDF)
+    sdf_sample_distance(s, md, r, out);
+  else if (md->kind == MUPSI_MEDIUM_EXTERNAL_GP)
+    ext_sample_distance(md, r, seed, out);
+  else
+    sample_distance(s, md, r, seed, c, out, work);
+}
+static float any_transmittance(const mo_scene* s, const omedium* md, const oray* r, uint32_t seed,
+                               const mupsi_cond* c) {
+  return md->kind == MUPSI_MEDIUM_GP ? transmittance(s, md, r, seed, c) : field_transmittance(s, md, r, seed);
+}
+
 void mo_sample_distance(const mo_scene* s, int medium, int64_t n, const mupsi_ray* rays, const uint32_t* seed,
                         const mupsi_cond* cond, mupsi_medium_sample* out) {
   const omedium* md = &s->media[medium];
@@ -1179,7 +1433,16 @@ void mo_sample_distance(const mo_scene* s, int medium, int64_t n, const mupsi_ra
   for (int64_t i = 0; i < n; ++i) {
     oray r = load_ray(&rays[i]);
     memset(&out[i], 0, sizeof out[i]);
-    sample_distance(s, md, &r, seed[i], cond ? cond + i : NULL, &out[i], NULL);
+    any_sample_distance(s, md, &r, seed[i], cond ? cond + i : NULL, &out[i], NULL);
+  }
+}
+void mo_transmittance(const mo_scene* s, int medium, int64_t n, const mupsi_ray* rays, const uint32_t* seed,
+                      const mupsi_cond* cond, float* out) {
+  const omedium* md = &s->media[medium];
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int64_t i = 0; i < n; ++i) {
+    oray r = load_ray(&rays[i]);
+    out[i] = any_transmittance(s, md, &r, seed[i], cond ? cond + i : NULL);
   }
 }
 void mo_sample_condition(const mo_scene* s, int medium, int64_t n, const mupsi_medium_sample* samples,
@@ -1493,7 +1756,7 @@ static v3 trace_sample(const mo_scene* s, int x, int y, int k, int64_t* work) {
       const omedium* md = &s->media[medium];
       uint32_t ms = mo_make_seed5((uint32_t)x, (uint32_t)y, (uint32_t)k, seed, (uint32_t)bounce);
       csampler cs = constant_sampler(single ? seed : ms);
-      sample_distance(s, md, &ray, cs.i, &cond, &smp, work);
+      any_sample_distance(s, md, &ray, cs.i, &cond, &smp, work);
       if (!smp.exited) {
         /* makeSurfaceEventFromMedium (medium.cpp:8-26) + handleVolume (trace.cpp:77-116) */
         v3 P = vload(smp.p), N = vload(smp.normal), wo = vneg(ray.d);
@@ -1502,7 +1765,7 @@ static v3 trace_sample(const mo_scene* s, int x, int y, int k, int64_t* work) {
           oray sr = mkray(vadd(P, vmul(N, eps)), ls.d);
           float bias = ls.dist - eps * fabsf(vdot(ls.d, N));
           sr.ft = bias * 0.99f;
-          float tr = transmittance(s, md, &sr, cs.i, &cond);
+          float tr = any_transmittance(s, md, &sr, cs.i, &cond);
           v3 f = bsdf_weight(MUPSI_BSDF_LAMBERTIAN, med_albedo, ls.d, wo, N);
           emission = vadd(emission, vmul(smul(tr, cmul(thr, cmul(f, ls.weight))), fabsf(vdot(ls.d, N))));
         }
@@ -1514,7 +1777,7 @@ static v3 trace_sample(const mo_scene* s, int x, int y, int k, int64_t* work) {
         thr = vdiv(thr, surv);
         uint32_t ns = mo_make_seed5((uint32_t)x, (uint32_t)y, (uint32_t)k, seed, (uint32_t)(bounce + 1));
         csampler ncs = constant_sampler(single ? seed : ns);
-        sample_condition(s, md, &smp, ncs.i, !single, &cond);
+        if (md->kind == MUPSI_MEDIUM_GP) sample_condition(s, md, &smp, ncs.i, !single, &cond); /* trace.cpp:144-147 */
         ray = mkray(vadd(P, vmul(N, eps)), wi);
         ray.nt = neart;
         bounce++;

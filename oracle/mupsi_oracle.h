@@ -73,6 +73,14 @@ void mo_mean(const mo_scene* s, int medium, int64_t n, const float* p, float* ou
 void mo_medium_eval(const mo_scene* s, int medium, int64_t n, const float* p, const uint32_t* seed,
                     const mupsi_cond* cond, float* out);
 /* gpmedium.cpp:46-103 */
+/* SDFMedium / ExternalGPMedium on medium `medium` (0 ok, -1 bad arguments);
+ * grids res^3 floats, x-major; var may be NULL. */
+int mo_scene_set_sdf_medium(mo_scene* s, int medium);
+int mo_scene_set_external_gp_medium(mo_scene* s, int medium, int res, const float* bmin, const float* bmax,
+                                    const float* mean, const float* var, float noise_scale);
+/* Medium::transmittance of n rays: out[n] in {0, 1} */
+void mo_transmittance(const mo_scene* s, int medium, int64_t n, const mupsi_ray* rays, const uint32_t* seed,
+                      const mupsi_cond* cond, float* out);
 void mo_sample_distance(const mo_scene* s, int medium, int64_t n, const mupsi_ray* rays, const uint32_t* seed,
                         const mupsi_cond* cond, mupsi_medium_sample* out);
 /* gpmedium.cpp:133-161 */

@@ -41,8 +41,10 @@
 #include "gp/meanfunction.h"
 #include "math/random.h"
 #include "math/sampler.h"
+#include "medium/externalgpmedium.h"
 #include "medium/gpmedium.h"
 #include "medium/medium.h"
+#include "medium/sdfmedium.h"
 #include "primitives/mesh.h"
 #include "primitives/skydrome.h"
 #include "primitives/sphere.h"
@@ -78,6 +80,11 @@ struct ScenePrimitives {
 template struct MemberAccess<ControllerScene, &Controller::scene_>;
 template struct MemberAccess<ControllerSpp, &Controller::spp_>;
 template struct MemberAccess<ScenePrimitives, &Scene::primitives_>;
+struct ExternalEval {
+  typedef Vector4f (ExternalGPMedium::*type)(const Vector3f&, uint32_t) const;
+  friend type member_of(ExternalEval);
+};
+template struct MemberAccess<ExternalEval, &ExternalGPMedium::evalWithGradient>;
 
 namespace {
 std::shared_ptr<Scene>& scene_of(Controller& c) { return c.*member_of(ControllerScene()); }
@@ -102,6 +109,15 @@ struct RefMedium {
   std::shared_ptr<SparseSEKernel> kernel;
   std::shared_ptr<SparseGPNoiseGenerator> noise;
   std::shared_ptr<GPMedium> medium;
+};
+
+// An SDFMedium or ExternalGPMedium with what it owns.
+struct RefField {
+  std::shared_ptr<Mesh> mesh;
+  std::shared_ptr<MeanFunction> mean;
+  std::shared_ptr<SDFMedium> sdf;
+  std::shared_ptr<ExternalGPMedium> ext;
+  Medium* medium() const { return sdf ? static_cast<Medium*>(sdf.get()) : static_cast<Medium*>(ext.get()); }
 };
 
 struct RefScene {
@@ -286,6 +302,107 @@ void ref_sample_condition(void* h, long n, const float* hit, const uint32_t* see
     }
     o[3] = st.u_tilde;
     o[7] = st.active ? 1.0f : 0.0f;
+  }
+}
+
+// ---- field media: SDFMedium, ExternalGPMedium, GridMeanFunction ----------------------
+// kind 1: SDFMedium over a sphere (mean_type 0) or OBJ mesh (mean_type 1) mean;
+// kind 2: ExternalGPMedium over GridMeanFunction files (var_path nullable).
+void* ref_field_create(int kind, int mean_type, const float* center, float radius, const char* obj_path,
+                       const float* mesh_pos, float mesh_scale, int res, const float* bmin, const float* bmax,
+                       const char* mean_path, const char* var_path, float noise_scale) {
+  auto* f = new RefField();
+  if (kind == 1) {
+    if (mean_type == 0) {
+      f->mean = std::make_shared<SphereMeanFunction>(Vector3f(center[0], center[1], center[2]), radius);
+    } else {
+      f->mesh = std::make_shared<Mesh>();
+      if (!f->mesh->fetchFrom(obj_path)) {
+        delete f;
+        return nullptr;
+      }
+      if (mesh_pos)
+        f->mesh->setTransform(
+            Affine3f(Translation3f(Vector3f(mesh_pos[0], mesh_pos[1], mesh_pos[2])) * Scaling(mesh_scale)).matrix());
+      f->mean = std::make_shared<MeshMeanFunction>(f->mesh);
+    }
+    f->sdf = std::make_shared<SDFMedium>(f->mean);
+  } else {
+    Vector3f lo(bmin[0], bmin[1], bmin[2]), hi(bmax[0], bmax[1], bmax[2]);
+    auto mg = std::make_shared<GridMeanFunction>(mean_path, res, lo, hi);
+    std::shared_ptr<GridMeanFunction> vg;
+    if (var_path) vg = std::make_shared<GridMeanFunction>(var_path, res, lo, hi);
+    f->ext = std::make_shared<ExternalGPMedium>(mg, vg, noise_scale);
+  }
+  return f;
+}
+void ref_field_free(void* h) { delete static_cast<RefField*>(h); }
+
+// evalWithGradient(p[, seed]) (sdfmedium.cpp:10-14, externalgpmedium.cpp:33-58): out[n*4]
+void ref_field_eval(void* h, long n, const float* p, const uint32_t* seed, float* out) {
+  auto* f = static_cast<RefField*>(h);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (long i = 0; i < n; ++i) {
+    Vector3f P(p[3 * i], p[3 * i + 1], p[3 * i + 2]);
+    Vector4f r = f->sdf ? f->sdf->evalWithGradient(P) : ((*f->ext).*member_of(ExternalEval()))(P, seed[i]);
+    for (int c = 0; c < 4; ++c) out[4 * i + c] = r[c];
+  }
+}
+
+// sampleDistance for n rays (ray[n*8] as ref_sample_distance; seed = medium_sampler.nextI()):
+// out[n*8] = (exited, t, p xyz, normal xyz)
+void ref_field_sample_distance(void* h, long n, const float* ray, const uint32_t* seed, float* out) {
+  auto* f = static_cast<RefField*>(h);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (long i = 0; i < n; ++i) {
+    const float* r = ray + 8 * i;
+    Ray R(Vector3f(r[0], r[1], r[2]), Vector3f(r[3], r[4], r[5]));
+    R.setNearT(r[6]);
+    R.setFarT(r[7]);
+    GPConditioningState st;
+    MediumSample s;
+    s.conditioning = &st;
+    s.t = 0.0f;
+    s.p = Vector3f::Zero();
+    s.normal = Vector3f::Zero();
+    FixedSeedSampler ms(seed[i]);
+    f->medium()->sampleDistance(R, s, ms);
+    float* o = out + 8 * i;
+    o[0] = s.exited ? 1.0f : 0.0f;
+    o[1] = s.t;
+    for (int c = 0; c < 3; ++c) {
+      o[2 + c] = s.p[c];
+      o[5 + c] = s.normal[c];
+    }
+  }
+}
+
+// transmittance for n rays: out[n] (the x component)
+void ref_field_transmittance(void* h, long n, const float* ray, const uint32_t* seed, float* out) {
+  auto* f = static_cast<RefField*>(h);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (long i = 0; i < n; ++i) {
+    const float* r = ray + 8 * i;
+    Ray R(Vector3f(r[0], r[1], r[2]), Vector3f(r[3], r[4], r[5]));
+    R.setNearT(r[6]);
+    R.setFarT(r[7]);
+    GPConditioningState st;
+    MediumSample s;
+    s.conditioning = &st;
+    FixedSeedSampler ms(seed[i]);
+    out[i] = f->medium()->transmittance(R, s, ms).x();
+  }
+}
+
+// GridMeanFunction(path, res, bmin, bmax)::eval + gradient: out[n*4]
+void ref_grid_eval(const char* path, int res, const float* bmin, const float* bmax, long n, const float* p,
+                   float* out) {
+  GridMeanFunction g(path, res, Vector3f(bmin[0], bmin[1], bmin[2]), Vector3f(bmax[0], bmax[1], bmax[2]));
+  for (long i = 0; i < n; ++i) {
+    Vector3f P(p[3 * i], p[3 * i + 1], p[3 * i + 2]);
+    out[4 * i] = g.eval(P);
+    Vector3f gr = g.gradient(P);
+    for (int c = 0; c < 3; ++c) out[4 * i + 1 + c] = gr[c];
   }
 }
 

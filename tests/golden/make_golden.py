@@ -95,6 +95,104 @@ def trace_tex(R, td):
     np.savez_compressed(os.path.join(OUT, "trace_tex.npz"), **out)
 
 
+FIELD_KINDS = ("sdf_sphere", "sdf_mesh", "external_gp", "external_gp_mean")
+
+
+def _field_files(sc, td, name):
+    """Write what the reference loads for a field scene: the SDF mesh as OBJ,
+    the external GP grids as raw float32. Returns (obj_paths, grid_paths, ref medium kwargs)."""
+    m = sc.media[0]
+    obj_paths, grid_paths = [], None
+    for i, mesh in enumerate(sc.meshes):
+        op = os.path.join(td, f"{name}_{i}.obj")
+        S.save_obj(op, mesh.vertices, mesh.faces)
+        obj_paths.append(op)
+    if m["kind"] == "external_gp":
+        mp = f"{name}_mean.bin"
+        m["mean_grid"].tofile(os.path.join(td, mp))
+        vp = None
+        if m["var_grid"] is not None:
+            vp = f"{name}_var.bin"
+            m["var_grid"].tofile(os.path.join(td, vp))
+        grid_paths = (mp, vp)
+    return obj_paths, grid_paths
+
+
+def _field_rays(rng, n_out=256, n_in=64):
+    """Rays from the camera towards the medium (jittered), rays starting inside
+    the null sphere in random directions, and shadow-ray-like finite ones."""
+    d = np.stack([rng.normal(0, 0.12, n_out), rng.normal(0, 0.12, n_out), -np.ones(n_out)], 1)
+    o = np.zeros((n_out, 3))
+    o2 = np.float64([0, 0, -500]) + rng.uniform(-100, 100, (n_in, 3))
+    d2 = rng.normal(0, 1, (n_in, 3))
+    o = np.concatenate([o, o2])
+    d = np.concatenate([d, d2])
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.zeros((len(o), 8), np.float32)
+    rays[:, 0:3] = o
+    rays[:, 3:6] = d
+    rays[:, 6] = 1e-3
+    rays[:, 7] = 3e38
+    rays[n_out + n_in // 2:, 7] = rng.uniform(20, 200, n_in - n_in // 2)  # finite farT
+    return rays
+
+
+def field_media(R, td):
+    """SDFMedium / ExternalGPMedium / GridMeanFunction per point and per ray,
+    from the reference's own classes (ref_field_* in oracle/ref_harness.cpp)."""
+    rng = np.random.default_rng(21)
+    out = {}
+    for kind in FIELD_KINDS:
+        sc = S.field_scene(kind)
+        obj_paths, grid_paths = _field_files(sc, td, kind)
+        m = sc.media[0]
+        if kind == "sdf_sphere":
+            h = R.sdf_create(0, center=m["center"], radius=m["radius"])
+        elif kind == "sdf_mesh":
+            h = R.sdf_create(1, obj_path=obj_paths[0])
+        else:
+            h = R.external_gp_create(m["res"], m["bmin"], m["bmax"], os.path.join(td, grid_paths[0]),
+                                     os.path.join(td, grid_paths[1]) if grid_paths[1] else None, m["noise_scale"])
+        rays = _field_rays(rng)
+        seed = rng.integers(0, 2 ** 32, len(rays), dtype=np.uint64).astype(np.uint32)
+        p = (np.float32([0, 0, -500]) + rng.uniform(-140, 140, (256, 3))).astype(np.float32)
+        pseed = rng.integers(0, 2 ** 32, len(p), dtype=np.uint64).astype(np.uint32)
+        sd = R.field_sample_distance(h, rays, seed)
+        assert 0.2 < (sd[:, 0] == 0).mean() < 0.9, kind
+        out[kind + "_rays"] = rays
+        out[kind + "_seed"] = seed
+        out[kind + "_sd"] = sd
+        out[kind + "_tr"] = R.field_transmittance(h, rays, seed)
+        out[kind + "_p"] = p
+        out[kind + "_pseed"] = pseed
+        out[kind + "_eval"] = R.field_eval(h, p, pseed)
+        if kind.startswith("external"):
+            out[kind + "_grid"] = R.grid_eval(os.path.join(td, grid_paths[0]), m["res"], m["bmin"], m["bmax"], p)
+        R.field_free(h)
+    np.savez_compressed(os.path.join(OUT, "field_media.npz"), **out)
+
+
+def trace_field(R, td):
+    """Full traces of the field scenes through Controller::load's sdf_medium /
+    external_gp_medium keys: 24x24, 2 passes."""
+    xs, ys, ks = np.meshgrid(np.arange(24), np.arange(24), np.arange(2), indexing="ij")
+    xs, ys, ks = xs.ravel().astype(np.int32), ys.ravel().astype(np.int32), ks.ravel().astype(np.int32)
+    out = dict(x=xs, y=ys, k=ks)
+    for kind in FIELD_KINDS:
+        sc = S.field_scene(kind)
+        obj_paths, grid_paths = _field_files(sc, td, kind)
+        j, extra = sc.to_json(obj_paths=obj_paths, grid_paths=grid_paths)
+        assert not extra
+        jp = os.path.join(td, kind + ".json")
+        json.dump(j, open(jp, "w"))
+        rh = R.scene_load(jp, sky=1.0)
+        rad = R.trace(rh, xs, ys, ks)
+        R.scene_free(rh)
+        assert len(np.unique(rad[:, 0])) > 50, kind
+        out[kind] = rad
+    np.savez_compressed(os.path.join(OUT, "trace_field.npz"), **out)
+
+
 def main():
     if len(sys.argv) > 1:
         with tempfile.TemporaryDirectory() as td:
@@ -210,6 +308,8 @@ def main():
     np.savez_compressed(os.path.join(OUT, "trace_mesh.npz"), x=xs, y=ys, k=ks, radiance=rad)
     trace_sky(R, td)
     trace_tex(R, td)
+    field_media(R, td)
+    trace_field(R, td)
     print("fixtures written to", OUT)
 
 

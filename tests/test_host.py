@@ -89,8 +89,15 @@ def test_scene_json_defaults_and_errors(tmp_path):
     assert s.primitives[0]["radius"] == 100.0 and s.sky is None
     with pytest.raises(ValueError):
         S.Scene.from_json({"camera": j["camera"]})
-    with pytest.raises(NotImplementedError):
+    with pytest.raises(KeyError):  # a sphere SDF needs its mean_center
         S.Scene.from_json(dict(j, sdf_medium={}))
+    prim = {"type": "sphere", "center": [0, 0, -5], "int_medium": True}
+    s = S.Scene.from_json(dict(j, sdf_medium={"mean_center": [0, 0, -5], "mean_radius": 2.0}, primitives=[prim]))
+    assert s.media[0]["kind"] == "sdf" and s.primitives[0]["int_medium"] == 0
+    # gp_medium wins over sdf_medium for int_medium primitives (controller.cpp:225-229)
+    s = S.Scene.from_json(dict(j, sdf_medium={"mean_center": [0, 0, -5]},
+                               gp_medium={"mean_center": [0, 0, -5]}, primitives=[prim]))
+    assert len(s.media) == 1 and s.media[0]["kind"] == "gp"
 
 
 def test_obj_roundtrip(tmp_path):
