@@ -387,6 +387,23 @@ int mupsi_gpu_scene_set_surrogate(mupsi_scene* scene, int32_t medium, mupsi_mlp*
  * of the descriptor. width = height = 0 removes it. */
 int mupsi_gpu_scene_set_sky_texture(mupsi_scene* scene, int32_t width, int32_t height, const float* rgb);
 
+/* The scene's image size (Camera width / height). */
+int mupsi_gpu_scene_get_size(const mupsi_scene* scene, int32_t* width, int32_t* height);
+
+/* GPSettings::gpMode for the scene's next renders (Controller::setGpMode,
+ * controller.cpp:385-391). */
+int mupsi_gpu_scene_set_gp_mode(mupsi_scene* scene, int32_t mode);
+
+/* PathTracerSettings::skip_medium (rendering/trace.h:22, trace.cpp:142): with
+ * skip != 0 paths pass through every medium without marching it (surfaces
+ * only), as Controller::startProgressive(targetSpp, skipMedium = true). */
+int mupsi_gpu_scene_set_skip_medium(mupsi_scene* scene, int32_t skip);
+
+/* Replace the SparseSEKernel of GP medium `medium` (Controller::applyGpMedium,
+ * controller.cpp:395-425, rebuilds the GPMedium with the UI's sigma, length
+ * scale and points per cell). */
+int mupsi_gpu_scene_set_kernel(mupsi_scene* scene, int32_t medium, const mupsi_kernel* kernel);
+
 /* Turn medium `medium` into an SDFMedium (controller.cpp:154-182,
  * sdfmedium.cpp:16-98): its descriptor's mean function (sphere or mesh) is the
  * field itself, sphere traced from the ray's nearT (steps max(|f|, 1e-3), at
@@ -484,6 +501,42 @@ typedef struct mupsi_batch_info {
   int64_t paths;             /* path samples traced */
 } mupsi_batch_info;
 int mupsi_gpu_batch_info(const mupsi_batch* batch, mupsi_batch_info* out);
+
+/* ---- headless progressive display (controller/controller.cpp:266-375) ----
+ * Controller's render control over one scene: a host thread renders frames
+ * of passes (mupsi_gpu_render, on the display's own stream) and after each
+ * frame swaps a pinned back buffer holding the averaged image with the front
+ * buffer under a mutex (framebufferFront_ / framebufferBack_, displayMtx_);
+ * the copy functions read the front buffer, so they always see a complete
+ * frame. While a display renders, the scene must not be used by other calls. */
+typedef struct mupsi_display mupsi_display;
+/* Front and back buffers (black) for the scene's image size. */
+int mupsi_gpu_display_create(mupsi_scene* scene, mupsi_display** out);
+/* Stops a running render and frees the buffers. */
+void mupsi_gpu_display_destroy(mupsi_display* d);
+/* Controller::startProgressive: stop any running render, then render passes
+ * [0, target_spp) in frames of passes_per_frame passes (1: a frame after every
+ * pass, as the reference; 0: frames of about 2^20 paths), publishing each. */
+int mupsi_gpu_display_start_progressive(mupsi_display* d, int32_t target_spp, int32_t passes_per_frame);
+/* Controller::start: all spp passes, published once at the end. */
+int mupsi_gpu_display_start(mupsi_display* d, int32_t spp);
+/* Controller::cancel (the render thread stops between waves; an unfinished
+ * frame is not published) and Controller::stop (cancel + join). stop returns
+ * the render thread's status (its message in mupsi_gpu_last_error). */
+void mupsi_gpu_display_cancel(mupsi_display* d);
+int mupsi_gpu_display_stop(mupsi_display* d);
+/* 1 while the render thread runs. */
+int32_t mupsi_gpu_display_running(const mupsi_display* d);
+/* isSppPassDone / ackSppPass / getCurrentSpp: a frame was published since the
+ * last ack; the passes in the front buffer. */
+int32_t mupsi_gpu_display_spp_pass_done(const mupsi_display* d);
+void mupsi_gpu_display_ack_spp_pass(mupsi_display* d);
+int32_t mupsi_gpu_display_current_spp(const mupsi_display* d);
+/* copyDisplayRawTo / copyDisplayTo: the front buffer, dst[(y * w + x) * 3 + c]
+ * (row y = camera y), raw or Reinhard tonemapped v / (1 + v)
+ * (framebuffer.cpp:37-45). width / height must be the scene's. */
+int mupsi_gpu_display_copy_raw(mupsi_display* d, float* dst, int32_t width, int32_t height);
+int mupsi_gpu_display_copy_tonemapped(mupsi_display* d, float* dst, int32_t width, int32_t height);
 
 #ifdef __cplusplus
 }

@@ -53,6 +53,27 @@ def _stream(stream):
     return None
 
 
+def _need(a, shape, name):
+    """An input the library reads `shape` elements of (a None input is absent)."""
+    if a is not None and tuple(a.shape) != tuple(shape):
+        raise ValueError(f"{name} must have shape {tuple(shape)}, got {tuple(a.shape)}")
+
+
+def check_buf(a, shape, dtype=np.float32, name="out"):
+    """A caller's output buffer must hold exactly `shape` elements of `dtype`
+    (the library writes that many through the pointer). Returns a."""
+    n = int(np.prod(shape))
+    if _is_dev(a):
+        tdt = {np.float32: torch.float32, np.float64: torch.float64, np.int32: torch.int32,
+               np.uint32: torch.int32}[dtype]
+        ok = a.dtype == tdt and a.numel() == n
+    else:
+        ok = isinstance(a, np.ndarray) and a.dtype == np.dtype(dtype) and a.size == n
+    if not ok:
+        raise ValueError(f"{name} must hold {tuple(shape)} {np.dtype(dtype).name} values")
+    return a
+
+
 def _empty(like_dev, shape, dtype):
     if like_dev:
         tdt = {np.float32: torch.float32, np.uint32: torch.int32, np.uint8: torch.uint8}[dtype]
@@ -107,9 +128,11 @@ class SparseGPNoiseGenerator:
         seed = _host(seed, np.uint32)
         n = p.shape[0]
         c = cond_records(cond)
+        _need(p, (n, 3), "p"), _need(seed, (n,), "seed"), _need(c, (n, 8), "cond")
         mem = _mem(p, seed, c, out)
         if out is None:
             out = _empty(mem == _abi.MEM_DEVICE, (n, 4), np.float32)
+        check_buf(out, (n, 4))
         check(load().mupsi_gpu_psi(C.byref(self._k), n, _ptr(p), _ptr(seed), _ptr(c), _ptr(out), mem,
                                    _stream(stream)))
         return out
@@ -119,9 +142,11 @@ class SparseGPNoiseGenerator:
         seed = _host(seed, np.uint32)
         n = p.shape[0]
         c = cond_records(cond)
+        _need(p, (n, 3), "p"), _need(seed, (n,), "seed"), _need(c, (n, 8), "cond")
         mem = _mem(p, seed, c, out)
         if out is None:
             out = _empty(mem == _abi.MEM_DEVICE, (n,), np.float32)
+        check_buf(out, (n,))
         check(load().mupsi_gpu_psi_value(C.byref(self._k), n, _ptr(p), _ptr(seed), _ptr(c), _ptr(out), mem,
                                          _stream(stream)))
         return out
@@ -170,6 +195,7 @@ class DeviceMesh:
         """BVH::intersect: rays (n, 8) [o, d, nearT, farT] -> (tri u32 (0xFFFFFFFF miss), (t, u, v))."""
         rays = _host(rays, np.float32)
         n = rays.shape[0]
+        _need(rays, (n, 8), "rays")
         mem = _mem(rays)
         dev = mem == _abi.MEM_DEVICE
         tri, tuv = _empty(dev, (n,), np.uint32), _empty(dev, (n, 3), np.float32)
@@ -179,6 +205,7 @@ class DeviceMesh:
     def occluded(self, rays, stream=None):
         rays = _host(rays, np.float32)
         n = rays.shape[0]
+        _need(rays, (n, 8), "rays")
         mem = _mem(rays)
         out = _empty(mem == _abi.MEM_DEVICE, (n,), np.uint8)
         check(load().mupsi_gpu_bvh_occluded(self.h, n, _ptr(rays), _ptr(out), mem, _stream(stream)))
@@ -188,6 +215,7 @@ class DeviceMesh:
         """BVH::closest: p (n, 3) -> (tri, (dist, q xyz))"""
         p = _host(p, np.float32)
         n = p.shape[0]
+        _need(p, (n, 3), "p")
         mem = _mem(p)
         dev = mem == _abi.MEM_DEVICE
         tri, dq = _empty(dev, (n,), np.uint32), _empty(dev, (n, 4), np.float32)
@@ -198,6 +226,7 @@ class DeviceMesh:
         """Mesh::inside and Mesh::distToPoint: -> (inside u8, tri, (dist, q xyz))"""
         p = _host(p, np.float32)
         n = p.shape[0]
+        _need(p, (n, 3), "p")
         mem = _mem(p)
         dev = mem == _abi.MEM_DEVICE
         ins, tri, dq = _empty(dev, (n,), np.uint8), _empty(dev, (n,), np.uint32), _empty(dev, (n, 4), np.float32)
@@ -282,6 +311,7 @@ class GpuScene:
     def mean(self, medium, p, stream=None):
         """MeanFunction eval + gradient -> (n, 4)"""
         p = _host(p, np.float32)
+        _need(p, (p.shape[0], 3), "p")
         mem = _mem(p)
         out = _empty(mem == _abi.MEM_DEVICE, (p.shape[0], 4), np.float32)
         check(load().mupsi_gpu_mean(self.h, medium, p.shape[0], _ptr(p), _ptr(out), mem, _stream(stream)))
@@ -292,6 +322,7 @@ class GpuScene:
         p = _host(p, np.float32)
         seed = _host(seed, np.uint32)
         c = cond_records(cond)
+        _need(p, (p.shape[0], 3), "p"), _need(seed, (p.shape[0],), "seed"), _need(c, (p.shape[0], 8), "cond")
         mem = _mem(p, seed, c)
         out = _empty(mem == _abi.MEM_DEVICE, (p.shape[0], 4), np.float32)
         check(load().mupsi_gpu_medium_eval(self.h, medium, p.shape[0], _ptr(p), _ptr(seed), _ptr(c), _ptr(out), mem,
@@ -303,6 +334,8 @@ class GpuScene:
         rays = _host(rays, np.float32)
         seed = _host(seed, np.uint32)
         c = cond_records(cond)
+        n = rays.shape[0]
+        _need(rays, (n, 8), "rays"), _need(seed, (n,), "seed"), _need(c, (n, 8), "cond")
         mem = _mem(rays, seed, c)
         out = _empty(mem == _abi.MEM_DEVICE, (rays.shape[0], 8), np.float32)
         check(load().mupsi_gpu_sample_distance(self.h, medium, rays.shape[0], _ptr(rays), _ptr(seed), _ptr(c),
@@ -320,6 +353,8 @@ class GpuScene:
         rays = _host(rays, np.float32)
         seed = _host(seed, np.uint32)
         c = cond_records(cond)
+        n = rays.shape[0]
+        _need(rays, (n, 8), "rays"), _need(seed, (n,), "seed"), _need(c, (n, 8), "cond")
         mem = _mem(rays, seed, c)
         out = _empty(mem == _abi.MEM_DEVICE, (rays.shape[0],), np.float32)
         check(load().mupsi_gpu_transmittance(self.h, medium, rays.shape[0], _ptr(rays), _ptr(seed), _ptr(c),
@@ -331,6 +366,7 @@ class GpuScene:
         samples = np.asarray(samples, np.float32)
         seed = np.ascontiguousarray(seed, np.uint32)
         n = samples.shape[0]
+        _need(samples, (n, 7), "samples"), _need(seed, (n,), "seed")
         ms = np.zeros((n, 8), np.float32)
         ms.view(np.uint32)[:, 0] = samples[:, 0].astype(np.uint32)
         ms[:, 2:5] = samples[:, 1:4]
@@ -349,6 +385,11 @@ class GpuScene:
         for a in (x, y, k, out):
             if not _is_dev(a):
                 raise ValueError("trace_noalloc takes CUDA tensors only")
+        n = x.shape[0]
+        for a, nm in ((y, "y"), (k, "k")):
+            check_buf(a, (n,), np.int32, nm)
+        check_buf(x, (n,), np.int32, "x")
+        check_buf(out, (n, 3))
         check(load().mupsi_gpu_trace_samples_noalloc(self.h, x.shape[0], _ptr(x), _ptr(y), _ptr(k), _ptr(out),
                                                      _stream(stream)))
         return out
@@ -360,6 +401,25 @@ class GpuScene:
             return
         img = np.ascontiguousarray(img, np.float32)
         check(load().mupsi_gpu_scene_set_sky_texture(self.h, img.shape[1], img.shape[0], img.ctypes.data))
+
+    def size(self):
+        """(width, height) of the scene's image."""
+        w, h = C.c_int32(), C.c_int32()
+        check(load().mupsi_gpu_scene_get_size(self.h, C.byref(w), C.byref(h)))
+        return w.value, h.value
+
+    def set_gp_mode(self, mode):
+        """GPSettings::gpMode: _abi.GP_SINGLE_REALIZATION or _abi.GP_RENEWAL_PLUS."""
+        check(load().mupsi_gpu_scene_set_gp_mode(self.h, int(mode)))
+
+    def set_skip_medium(self, skip):
+        """PathTracerSettings::skip_medium: pass through media without marching."""
+        check(load().mupsi_gpu_scene_set_skip_medium(self.h, 1 if skip else 0))
+
+    def set_kernel(self, medium, kernel):
+        """Replace a GP medium's SparseSEKernel (an SparseSEKernel with its
+        impulse density: kernel.struct(points_per_cell))."""
+        check(load().mupsi_gpu_scene_set_kernel(self.h, medium, C.byref(kernel)))
 
     def set_sdf_medium(self, medium):
         """Make medium `medium` an SDFMedium over its mean function."""
@@ -425,6 +485,7 @@ class GpuScene:
         x, y, k = (_host(a, np.int32) for a in (x, y, k))
         mem = _mem(x, y, k)
         n = x.shape[0]
+        _need(x, (n,), "x"), _need(y, (n,), "y"), _need(k, (n,), "k")
         if mem == _abi.MEM_DEVICE:
             out = torch.empty((n, 3), dtype=torch.float32, device="cuda")
         else:
@@ -456,6 +517,7 @@ class GpuRenderer:
         dev = out is not None and _is_dev(out)
         if out is None:
             out = np.empty((h, w, 3), np.float32)
+        check_buf(out, (h, w, 3))
         mom = np.zeros((h, w, 6), np.float64) if moments else None
         cb = _abi.ON_SPP(lambda k, user: on_spp(k)) if on_spp else _abi.ON_SPP()
         args = _abi.RenderArgs(spp_begin, target_spp, C.pointer(self.cancel_flag), cb, None, _ptr(out),
@@ -466,6 +528,76 @@ class GpuRenderer:
             return None
         check(code)
         return (out, mom) if moments else out
+
+
+class GpuDisplay:
+    """Headless double-buffered progressive display over one GpuScene
+    (Controller's render control, controller/controller.cpp:266-375): a native
+    render thread publishes frames; copy_raw / copy_tonemapped read the
+    latest complete one."""
+
+    def __init__(self, scene):
+        self.scene = scene if isinstance(scene, GpuScene) else GpuScene(scene)
+        self.width, self.height = self.scene.size()
+        h = C.c_void_p()
+        check(load().mupsi_gpu_display_create(self.scene.h, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            load().mupsi_gpu_display_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def start_progressive(self, target_spp, passes_per_frame=1):
+        check(load().mupsi_gpu_display_start_progressive(self.h, int(target_spp), int(passes_per_frame)))
+
+    def start(self, spp):
+        check(load().mupsi_gpu_display_start(self.h, int(spp)))
+
+    def cancel(self):
+        load().mupsi_gpu_display_cancel(self.h)
+
+    def stop(self):
+        check(load().mupsi_gpu_display_stop(self.h))
+
+    def running(self):
+        return bool(load().mupsi_gpu_display_running(self.h))
+
+    def is_spp_pass_done(self):
+        return bool(load().mupsi_gpu_display_spp_pass_done(self.h))
+
+    def ack_spp_pass(self):
+        load().mupsi_gpu_display_ack_spp_pass(self.h)
+
+    def current_spp(self):
+        return int(load().mupsi_gpu_display_current_spp(self.h))
+
+    def _dst(self, out):
+        if out is None:
+            return np.empty((self.height, self.width, 3), np.float32)
+        if not (isinstance(out, np.ndarray) and out.dtype == np.float32 and out.ndim == 3 and out.shape[2] == 3
+                and out.flags.c_contiguous):
+            raise ValueError("out must be a C-contiguous (h, w, 3) float32 array")
+        return out
+
+    def copy_raw(self, out=None):
+        """The front frame (h, w, 3) float32, un-tonemapped (copyDisplayRawTo).
+        The library checks out's size against the scene's."""
+        out = self._dst(out)
+        check(load().mupsi_gpu_display_copy_raw(self.h, out.ctypes.data, out.shape[1], out.shape[0]))
+        return out
+
+    def copy_tonemapped(self, out=None):
+        """The front frame Reinhard tonemapped v / (1 + v) (copyDisplayTo)."""
+        out = self._dst(out)
+        check(load().mupsi_gpu_display_copy_tonemapped(self.h, out.ctypes.data, out.shape[1], out.shape[0]))
+        return out
 
 
 class GpuBatch:
@@ -509,6 +641,11 @@ class GpuBatch:
             raise ValueError("one spp per scene")
         if out is None:
             out = [np.empty((sc.scene.height, sc.scene.width, 3), np.float32) for sc in self.scenes]
+        if len(out) != n:
+            raise ValueError("one output per scene")
+        for o, sc in zip(out, self.scenes):
+            if o is not None:
+                check_buf(o, (sc.scene.height, sc.scene.width, 3))
         dev = _mem(*out) == _abi.MEM_DEVICE
         sp = (C.c_int32 * n)(*[int(v) for v in spp])
         ptrs = (C.c_void_p * n)(*[_ptr(o) for o in out])

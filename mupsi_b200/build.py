@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmupsi_gpu.so")
-SOURCES = ["core.cu", "render.cu", "mlp.cu", "host_bvh.cpp"]
+SOURCES = ["core.cu", "render.cu", "mlp.cu", "host_bvh.cpp", "display.cpp"]
 HEADERS = ["core.cuh", "dmath.cuh", "geom.cuh", "gp.cuh", "host.h", "scene.cuh", "tc.cuh"]
 ROOT_HEADER = os.path.join(HERE, "..", "include", "mupsi_gpu.h")
 
@@ -58,7 +58,7 @@ def build(force=False, verbose=False):
         if verbose and out.strip():
             print(out)
     tmp = LIB + ".tmp"
-    cmd = [nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart"]
+    cmd = [nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart", "-lpthread"]
     r = subprocess.run(cmd, capture_output=True, text=True, env=env)
     if r.returncode != 0:
         raise RuntimeError("link failed:\n" + r.stdout + r.stderr)

@@ -414,7 +414,7 @@ __global__ void __launch_bounds__(128) k_shade(const DScene* const* __restrict__
     int bounce = meta_bounce(meta.w);
     bool has_hit = false, exited = true, dead = false;
     Cond cond = load_cond(P, i);
-    if (medium >= 0) {
+    if (medium >= 0 && !S->skip_medium) {  // the medium branch (trace.cpp:142)
       float4 hb = P.hb[i];
       if (__float_as_uint(hb.w) == 0u) {
         // makeSurfaceEventFromMedium (medium.cpp:8-26) + handleVolume (trace.cpp:77-116)
@@ -497,7 +497,7 @@ __global__ void __launch_bounds__(128) k_shade(const DScene* const* __restrict__
       store_cond(P, i, cond);
       P.meta[i] = make_int4(meta.x, meta.y, meta.z, pack_meta(bounce, inst));
       push(qa_next, ca_next, i);
-      if (medium >= 0) push(qm_next, cm_next, i);
+      if (medium >= 0 && !S->skip_medium) push(qm_next, cm_next, i);
     } else {
       P.rad[3 * (int64_t)i] = em.x;
       P.rad[3 * (int64_t)i + 1] = em.y;
@@ -1983,6 +1983,44 @@ int mupsi_gpu_scene_set_sky_texture(mupsi_scene* scene, int32_t width, int32_t h
     scene->h.sky_w = width;
     scene->h.sky_h = height;
   }
+  MUPSI_CUDA(cudaMemcpy(scene->d, &scene->h, sizeof(DScene), cudaMemcpyHostToDevice));
+  return MUPSI_OK;
+}
+
+int mupsi_gpu_scene_get_size(const mupsi_scene* scene, int32_t* width, int32_t* height) {
+  clear_error();
+  if (!scene || !width || !height) return fail(MUPSI_ERR_INVALID, "null argument");
+  *width = scene->width;
+  *height = scene->height;
+  return MUPSI_OK;
+}
+
+int mupsi_gpu_scene_set_gp_mode(mupsi_scene* scene, int32_t mode) {
+  clear_error();
+  if (!scene) return fail(MUPSI_ERR_INVALID, "null scene");
+  if (mode != MUPSI_GP_SINGLE_REALIZATION && mode != MUPSI_GP_RENEWAL_PLUS) return fail(MUPSI_ERR_INVALID, "bad gp_mode");
+  MUPSI_CUDA(cudaDeviceSynchronize());
+  scene->h.gp_mode = mode;
+  MUPSI_CUDA(cudaMemcpy(scene->d, &scene->h, sizeof(DScene), cudaMemcpyHostToDevice));
+  return MUPSI_OK;
+}
+
+int mupsi_gpu_scene_set_skip_medium(mupsi_scene* scene, int32_t skip) {
+  clear_error();
+  if (!scene) return fail(MUPSI_ERR_INVALID, "null scene");
+  MUPSI_CUDA(cudaDeviceSynchronize());
+  scene->h.skip_medium = skip ? 1 : 0;
+  MUPSI_CUDA(cudaMemcpy(scene->d, &scene->h, sizeof(DScene), cudaMemcpyHostToDevice));
+  return MUPSI_OK;
+}
+
+int mupsi_gpu_scene_set_kernel(mupsi_scene* scene, int32_t medium, const mupsi_kernel* kernel) {
+  clear_error();
+  if (!scene || !kernel) return fail(MUPSI_ERR_INVALID, "null argument");
+  if (medium < 0 || medium >= scene->h.nmed) return fail(MUPSI_ERR_INVALID, "medium out of range");
+  if (int e = check_kernel(kernel)) return e;
+  MUPSI_CUDA(cudaDeviceSynchronize());
+  scene->h.media[medium].k = make_kparams(*kernel);
   MUPSI_CUDA(cudaMemcpy(scene->d, &scene->h, sizeof(DScene), cudaMemcpyHostToDevice));
   return MUPSI_OK;
 }

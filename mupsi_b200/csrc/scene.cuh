@@ -83,6 +83,7 @@ struct DScene {
   int min_group;                 // smallest lane group per march
   int sphere_only;               // every mean is a sphere: the march kernel without BVH code
   int field;                     // some medium is an SDF or external GP medium (k_march_field)
+  int skip_medium;               // PathTracerSettings::skip_medium: media are passed through unmarched
 };
 
 // ------------------------------------------------------------ mean functions

@@ -67,6 +67,25 @@ def _setup(L):
     L.mupsi_gpu_scene_set_sdf_medium.argtypes = [vp, i32]
     L.mupsi_gpu_scene_set_external_gp_medium.argtypes = [vp, i32, i32, vp, vp, vp, vp, C.c_float]
     L.mupsi_gpu_transmittance.argtypes = [vp, i32, i64, vp, vp, vp, vp, C.c_int, vp]
+    L.mupsi_gpu_scene_get_size.argtypes = [vp, C.POINTER(i32), C.POINTER(i32)]
+    L.mupsi_gpu_scene_set_skip_medium.argtypes = [vp, i32]
+    L.mupsi_gpu_scene_set_gp_mode.argtypes = [vp, i32]
+    L.mupsi_gpu_scene_set_kernel.argtypes = [vp, i32, C.POINTER(_abi.Kernel)]
+    L.mupsi_gpu_display_create.argtypes = [vp, C.POINTER(vp)]
+    L.mupsi_gpu_display_destroy.argtypes = [vp]
+    L.mupsi_gpu_display_destroy.restype = None
+    L.mupsi_gpu_display_start_progressive.argtypes = [vp, i32, i32]
+    L.mupsi_gpu_display_start.argtypes = [vp, i32]
+    L.mupsi_gpu_display_cancel.argtypes = [vp]
+    L.mupsi_gpu_display_cancel.restype = None
+    L.mupsi_gpu_display_stop.argtypes = [vp]
+    for f in ("running", "spp_pass_done", "current_spp"):
+        getattr(L, "mupsi_gpu_display_" + f).argtypes = [vp]
+        getattr(L, "mupsi_gpu_display_" + f).restype = i32
+    L.mupsi_gpu_display_ack_spp_pass.argtypes = [vp]
+    L.mupsi_gpu_display_ack_spp_pass.restype = None
+    L.mupsi_gpu_display_copy_raw.argtypes = [vp, vp, i32, i32]
+    L.mupsi_gpu_display_copy_tonemapped.argtypes = [vp, vp, i32, i32]
     return L
 
 

@@ -14,6 +14,7 @@ import ctypes as C
 import numpy as np
 
 from . import _abi
+from .api import check_buf
 from .lib import check, load
 
 PARAMS = 18753
@@ -118,6 +119,8 @@ class SurrogateMean:
         """mu_hat at points p (n, 3): numpy (host) or CUDA tensor (device)."""
         dev = _dev(p)
         n = p.shape[0]
+        if tuple(p.shape) != (n, 3):
+            raise ValueError("p must be (n, 3)")
         if out is None:
             if dev:
                 import torch
@@ -126,6 +129,7 @@ class SurrogateMean:
                 out = np.empty(n, np.float32)
         if not dev:
             p = np.ascontiguousarray(p, np.float32)
+        check_buf(out, (n,))
         check(load().mupsi_gpu_mlp_infer(self.h, n, _ptr(p), _ptr(out), _abi.MEM_DEVICE if dev else _abi.MEM_HOST,
                                          _stream()))
         return out
@@ -136,6 +140,7 @@ class SurrogateMean:
         if not dev:
             p = np.ascontiguousarray(p, np.float32)
             target = np.ascontiguousarray(target, np.float32)
+        _points_targets(p, target)
         g = np.zeros(PARAMS, np.float32)
         loss = np.zeros(1, np.float32)
         check(load().mupsi_gpu_mlp_grad(self.h, p.shape[0], _ptr(p), _ptr(target), g.ctypes.data, loss.ctypes.data,
@@ -149,11 +154,19 @@ class SurrogateMean:
         if not dev:
             p = np.ascontiguousarray(p, np.float32)
             target = np.ascontiguousarray(target, np.float32)
+        _points_targets(p, target)
         a = TrainArgs(steps, batch, lr, lr_final, betas[0], betas[1], eps, seed)
         losses = np.zeros(steps, np.float32)
         check(load().mupsi_gpu_mlp_train(self.h, p.shape[0], _ptr(p), _ptr(target), C.addressof(a),
                                          losses.ctypes.data, _abi.MEM_DEVICE if dev else _abi.MEM_HOST, _stream()))
         return losses
+
+
+def _points_targets(p, target):
+    """The library reads n points (n, 3) and n targets (n,)."""
+    n = p.shape[0]
+    if tuple(p.shape) != (n, 3) or tuple(target.shape) != (n,):
+        raise ValueError("need points (n, 3) and targets (n,)")
 
 
 def training_points(vertices, faces, n, box_lo, box_hi, seed=0, normal_sigma=2.0):

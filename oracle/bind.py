@@ -80,6 +80,7 @@ class _Port:
         L.mo_sample_condition.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.c_void_p, _u32, C.c_void_p]
         L.mo_transmittance.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.c_void_p, _u32, C.c_void_p, _f32]
         L.mo_scene_set_sdf_medium.argtypes = [C.c_void_p, C.c_int]
+        L.mo_scene_set_skip_medium.argtypes = [C.c_void_p, C.c_int]
         L.mo_scene_set_external_gp_medium.argtypes = [C.c_void_p, C.c_int, C.c_int, _f32, _f32, _f32, C.c_void_p,
                                                       C.c_float]
         L.mo_trace.argtypes = [C.c_void_p, C.c_int64, _i32, _i32, _i32, _f32]
@@ -302,6 +303,9 @@ class PortOracle:
                                 None if ca is None else ca.ctypes.data, out)
         return out
 
+    def scene_set_skip_medium(self, h, skip):
+        self.L.mo_scene_set_skip_medium(h, 1 if skip else 0)
+
     def scene_set_sdf(self, h, medium):
         if self.L.mo_scene_set_sdf_medium(h, medium) != 0:
             raise ValueError("bad medium")
@@ -374,6 +378,7 @@ class RefOracle:
         L.ref_field_sample_distance.argtypes = [C.c_void_p, C.c_long, _f32, _u32, _f32]
         L.ref_field_transmittance.argtypes = [C.c_void_p, C.c_long, _f32, _u32, _f32]
         L.ref_grid_eval.argtypes = [C.c_char_p, C.c_int, _f32, _f32, C.c_long, _f32, _f32]
+        L.ref_set_skip_medium.argtypes = [C.c_int]
         L.ref_bvh_free.argtypes = [C.c_void_p]
         L.ref_bvh_node_count.restype = C.c_long
         L.ref_bvh_node_count.argtypes = [C.c_void_p]
@@ -552,6 +557,10 @@ class RefOracle:
         dq = np.zeros((n, 4), np.float32)
         self.L.ref_mesh_queries(medium_h, n, p, ins, tri, dq)
         return ins, tri, dq
+
+    def set_skip_medium(self, skip):
+        """g_pathTracerSettings.skip_medium for the scenes prepared from now on."""
+        self.L.ref_set_skip_medium(1 if skip else 0)
 
     def scene_load(self, json_path, sky=1.0, extra_meshes=()):
         h = self.L.ref_scene_load(json_path.encode(), -1.0 if sky is None else float(sky))

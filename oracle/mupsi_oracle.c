@@ -570,6 +570,7 @@ struct mo_scene {
   /* Skydrome(BitmapTexture) (skydrome.cpp, texture.cpp): RGB, row 0 at the top */
   float* sky_tex;
   int sky_w, sky_h;
+  int skip_medium; /* PathTracerSettings::skip_medium (trace.h:22) */
 };
 
 /* Mesh::computeFaceNormals (mesh.cpp:140-154) */
@@ -1278,6 +1279,7 @@ static void sample_condition(const mo_scene* s, const omedium* md, const mupsi_m
 }
 
 /* ------------------------------------------------------- field media -- */
+void mo_scene_set_skip_medium(mo_scene* s, int skip) { s->skip_medium = skip != 0; }
 int mo_scene_set_sdf_medium(mo_scene* s, int medium) {
   if (medium < 0 || medium >= s->nmed) return -1;
   s->media[medium].kind = MUPSI_MEDIUM_SDF;
@@ -1752,7 +1754,7 @@ static v3 trace_sample(const mo_scene* s, int x, int y, int k, int64_t* work) {
   do {
     has_hit = 0;
     int exited = 1;
-    if (medium >= 0) {
+    if (medium >= 0 && !s->skip_medium) { /* trace.cpp:142 */
       const omedium* md = &s->media[medium];
       uint32_t ms = mo_make_seed5((uint32_t)x, (uint32_t)y, (uint32_t)k, seed, (uint32_t)bounce);
       csampler cs = constant_sampler(single ? seed : ms);

@@ -76,6 +76,8 @@ void mo_medium_eval(const mo_scene* s, int medium, int64_t n, const float* p, co
 /* SDFMedium / ExternalGPMedium on medium `medium` (0 ok, -1 bad arguments);
  * grids res^3 floats, x-major; var may be NULL. */
 int mo_scene_set_sdf_medium(mo_scene* s, int medium);
+/* PathTracerSettings::skip_medium */
+void mo_scene_set_skip_medium(mo_scene* s, int skip);
 int mo_scene_set_external_gp_medium(mo_scene* s, int medium, int res, const float* bmin, const float* bmax,
                                     const float* mean, const float* var, float noise_scale);
 /* Medium::transmittance of n rays: out[n] in {0, 1} */

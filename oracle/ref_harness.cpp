@@ -524,6 +524,9 @@ int ref_scene_add_mesh(void* h, const char* obj_path, float albedo) {
   scene_of(s->ctrl)->addPrimitive(m);
   return 0;
 }
+// PathTracerSettings::skip_medium of the render contexts snapshotted from now on
+// (Controller::startProgressive sets the global the same way, controller.cpp:302).
+void ref_set_skip_medium(int skip) { g_pathTracerSettings.skip_medium = skip != 0; }
 // Snapshot the render context and prepare primitives (renderer.cpp:10-16).
 void ref_scene_prepare(void* h) {
   auto* s = static_cast<RefScene*>(h);

@@ -193,6 +193,31 @@ def trace_field(R, td):
     np.savez_compressed(os.path.join(OUT, "trace_field.npz"), **out)
 
 
+def trace_skip(R, td):
+    """PathTracerSettings::skip_medium (trace.cpp:142) on the 16x16 mesh scene:
+    the reference renders with the global set, as Controller::startProgressive
+    (targetSpp, true) leaves it."""
+    sc = S.config_mesh_scene(level=2, width=16, height=16, spp=2, seed=5)
+    objs = []
+    for i, m in enumerate(sc.meshes):
+        p = os.path.join(td, f"skip{i}.obj")
+        S.save_obj(p, m.vertices, m.faces)
+        objs.append(p)
+    j, extra = sc.to_json(objs)
+    jp = os.path.join(td, "skip.json")
+    json.dump(j, open(jp, "w"))
+    R.set_skip_medium(True)
+    try:
+        rh = R.scene_load(jp, sky=1.0, extra_meshes=extra)
+    finally:
+        R.set_skip_medium(False)
+    xs, ys, ks = np.meshgrid(np.arange(16), np.arange(16), np.arange(2), indexing="ij")
+    xs, ys, ks = xs.ravel().astype(np.int32), ys.ravel().astype(np.int32), ks.ravel().astype(np.int32)
+    rad = R.trace(rh, xs, ys, ks)
+    R.scene_free(rh)
+    np.savez_compressed(os.path.join(OUT, "trace_skip.npz"), x=xs, y=ys, k=ks, radiance=rad)
+
+
 def main():
     if len(sys.argv) > 1:
         with tempfile.TemporaryDirectory() as td:
@@ -310,6 +335,7 @@ def main():
     trace_tex(R, td)
     field_media(R, td)
     trace_field(R, td)
+    trace_skip(R, td)
     print("fixtures written to", OUT)
 
 

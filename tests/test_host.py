@@ -152,3 +152,18 @@ def test_tuning_file_is_valid():
     t = json.load(open(TUNING_FILE))["tuning"]
     for k, v in t.items():
         assert v in CANDIDATES[k]
+
+
+def test_buffer_checks_reject_short_buffers():
+    """The wrappers refuse buffers the library would over-read or over-write."""
+    from mupsi_b200 import api
+    api._need(np.zeros((4, 3), np.float32), (4, 3), "p")
+    with pytest.raises(ValueError):
+        api._need(np.zeros((4, 2), np.float32), (4, 3), "p")
+    with pytest.raises(ValueError):
+        api._need(np.zeros(3, np.uint32), (4,), "seed")
+    api.check_buf(np.zeros((2, 3, 3), np.float32), (2, 3, 3))
+    with pytest.raises(ValueError):
+        api.check_buf(np.zeros((8, 8, 3), np.float32), (64, 64, 3))
+    with pytest.raises(ValueError):
+        api.check_buf(np.zeros((2, 3, 3), np.float64), (2, 3, 3))
