@@ -538,6 +538,24 @@ int32_t mupsi_gpu_display_current_spp(const mupsi_display* d);
 int mupsi_gpu_display_copy_raw(mupsi_display* d, float* dst, int32_t width, int32_t height);
 int mupsi_gpu_display_copy_tonemapped(mupsi_display* d, float* dst, int32_t width, int32_t height);
 
+/* ---- OBJ files (primitives/mesh.cpp:20-136, Mesh::fetchFrom) ----
+ * Host-side reader with the reference's parsing rules and number extraction:
+ * v, vn, vt, triangular f in the v, v/vt, v//vn, v/vt/vn forms, 1-based or
+ * negative indices (a missing vt index is texcoord 0), other faces skipped.
+ * Arrays are malloc'd; release with mupsi_obj_free. face_texcoords is NULL
+ * when the file has no vt lines. MUPSI_ERR_INVALID for an unreadable file,
+ * no geometry, or an index out of range. */
+typedef struct {
+  int64_t num_vertices, num_faces, num_normals, num_texcoords;
+  float* vertices;         /* [num_vertices*3] */
+  int32_t* faces;          /* [num_faces*3], 0-based */
+  float* normals;          /* [num_normals*3] (the reference indexes them by vertex id) */
+  float* texcoords;        /* [num_texcoords*2] */
+  int32_t* face_texcoords; /* [num_faces*3] */
+} mupsi_obj;
+int mupsi_obj_load(const char* path, mupsi_obj* out);
+void mupsi_obj_free(mupsi_obj* obj);
+
 #ifdef __cplusplus
 }
 #endif

@@ -151,6 +151,14 @@ class RenderStats(C.Structure):
     ]
 
 
+class Obj(C.Structure):
+    """mupsi_obj"""
+    _fields_ = [("num_vertices", C.c_int64), ("num_faces", C.c_int64), ("num_normals", C.c_int64),
+                ("num_texcoords", C.c_int64), ("vertices", C.POINTER(C.c_float)), ("faces", C.POINTER(C.c_int32)),
+                ("normals", C.POINTER(C.c_float)), ("texcoords", C.POINTER(C.c_float)),
+                ("face_texcoords", C.POINTER(C.c_int32))]
+
+
 class Tuning(C.Structure):
     _fields_ = [
         ("march_block", C.c_int32),

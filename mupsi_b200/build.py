@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmupsi_gpu.so")
-SOURCES = ["core.cu", "render.cu", "mlp.cu", "host_bvh.cpp", "display.cpp"]
+SOURCES = ["core.cu", "render.cu", "mlp.cu", "host_bvh.cpp", "host_obj.cpp", "display.cpp"]
 HEADERS = ["core.cuh", "dmath.cuh", "geom.cuh", "gp.cuh", "host.h", "scene.cuh", "tc.cuh"]
 ROOT_HEADER = os.path.join(HERE, "..", "include", "mupsi_gpu.h")
 

@@ -68,6 +68,9 @@ def _setup(L):
     L.mupsi_gpu_scene_set_external_gp_medium.argtypes = [vp, i32, i32, vp, vp, vp, vp, C.c_float]
     L.mupsi_gpu_transmittance.argtypes = [vp, i32, i64, vp, vp, vp, vp, C.c_int, vp]
     L.mupsi_gpu_scene_get_size.argtypes = [vp, C.POINTER(i32), C.POINTER(i32)]
+    L.mupsi_obj_load.argtypes = [C.c_char_p, C.POINTER(_abi.Obj)]
+    L.mupsi_obj_free.argtypes = [C.POINTER(_abi.Obj)]
+    L.mupsi_obj_free.restype = None
     L.mupsi_gpu_scene_set_skip_medium.argtypes = [vp, i32]
     L.mupsi_gpu_scene_set_gp_mode.argtypes = [vp, i32]
     L.mupsi_gpu_scene_set_kernel.argtypes = [vp, i32, C.POINTER(_abi.Kernel)]

@@ -25,8 +25,16 @@ class Mesh:
                  face_texcoords=None):
         self.vertices = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
         self.faces = np.ascontiguousarray(faces, dtype=np.int32).reshape(-1, 3)
-        self.vertex_normals = (None if vertex_normals is None else
-                               np.ascontiguousarray(vertex_normals, dtype=np.float32).reshape(-1, 3))
+        self.vertex_normals = None
+        if vertex_normals is not None:
+            # Mesh::interpolateNormal indexes normals_ by vertex id (mesh.cpp:163-166):
+            # the first len(vertices) normals are the ones read; with fewer normals
+            # than vertices the reference reads past its array, so they are dropped
+            vn = np.ascontiguousarray(vertex_normals, dtype=np.float32).reshape(-1, 3)
+            if len(vn) >= len(self.vertices):
+                self.vertex_normals = np.ascontiguousarray(vn[:len(self.vertices)])
+            else:
+                warnings.warn(f"{len(vn)} normals for {len(self.vertices)} vertices: using face normals")
         self.position = tuple(float(v) for v in position)
         self.scale = float(scale)
         # OBJ texture coordinates (vt) and per-face indices into them; None:
@@ -49,55 +57,28 @@ class Mesh:
 
 
 def load_obj(path, texcoords=False):
-    """OBJ reader following Mesh::fetchFrom (primitives/mesh.cpp:20-136): v, vn,
-    vt, triangular f in v, v/vt, v//vn, v/vt/vn forms, 1-based or negative indices;
-    faces with other vertex counts are skipped. Returns (vertices, faces,
-    normals), plus (texcoords, face_texcoords) with texcoords=True: None, None
-    for a file without vt lines (interpolateTexcoord then yields the
-    barycentrics, mesh.cpp:175-177); a face corner without a vt index takes
-    texcoord 0, as normIdx maps index 0 there."""
-    verts, normals, faces, tcs, ftcs = [], [], [], [], []
-
-    def norm_idx(i, count):
-        return i - 1 if i > 0 else (count + i if i < 0 else 0)
-
-    with open(path) as fh:
-        for line in fh:
-            line = line.rstrip("\r\n")
-            if not line or line[0] == "#":
-                continue
-            parts = line.split()
-            if not parts:
-                continue
-            t = parts[0]
-            if t == "v":
-                verts.append([float(v) for v in parts[1:4]])
-            elif t == "vn":
-                normals.append([float(v) for v in parts[1:4]])
-            elif t == "vt":
-                tcs.append([float(v) for v in parts[1:3]])
-            elif t == "f":
-                idx, tidx = [], []
-                for spec in parts[1:]:
-                    fields = spec.split("/")
-                    vi = int(fields[0])
-                    ti = int(fields[1]) if len(fields) > 1 and fields[1] else 0
-                    idx.append(norm_idx(vi, len(verts)))
-                    tidx.append(norm_idx(ti, len(tcs)))
-                if len(idx) == 3:
-                    faces.append(idx)
-                    ftcs.append(tidx)
-    if not verts or not faces:
-        raise ValueError(f"{path}: no valid geometry")
-    out = (np.array(verts, np.float32), np.array(faces, np.int32), (np.array(normals, np.float32) if normals else None))
-    if not texcoords:
+    """OBJ file through the library's reader (mupsi_obj_load), which follows
+    Mesh::fetchFrom (primitives/mesh.cpp:20-136) down to its number parsing.
+    Returns (vertices, faces, normals or None), plus (texcoords,
+    face_texcoords) with texcoords=True: None, None for a file without vt
+    lines (interpolateTexcoord then yields the barycentrics, mesh.cpp:175-177)."""
+    from .lib import check, load
+    L = load()
+    o = _abi.Obj()
+    check(L.mupsi_obj_load(os.fsencode(path), C.byref(o)))
+    try:
+        def arr(ptr, n, cols, dt):
+            if n == 0:
+                return None
+            return np.ctypeslib.as_array(ptr, shape=(n * cols,)).astype(dt).reshape(n, cols)
+        out = (arr(o.vertices, o.num_vertices, 3, np.float32), arr(o.faces, o.num_faces, 3, np.int32),
+               arr(o.normals, o.num_normals, 3, np.float32))
+        if texcoords:
+            out = out + (arr(o.texcoords, o.num_texcoords, 2, np.float32),
+                         arr(o.face_texcoords, o.num_faces if o.num_texcoords else 0, 3, np.int32))
         return out
-    if not tcs:
-        return out + (None, None)
-    ft = np.array(ftcs, np.int32)
-    if ft.min() < 0 or ft.max() >= len(tcs):
-        raise ValueError(f"{path}: texcoord index out of range")
-    return out + (np.array(tcs, np.float32), ft)
+    finally:
+        L.mupsi_obj_free(C.byref(o))
 
 
 def save_obj(path, vertices, faces, texcoords=None, face_texcoords=None):

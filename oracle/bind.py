@@ -379,6 +379,10 @@ class RefOracle:
         L.ref_field_transmittance.argtypes = [C.c_void_p, C.c_long, _f32, _u32, _f32]
         L.ref_grid_eval.argtypes = [C.c_char_p, C.c_int, _f32, _f32, C.c_long, _f32, _f32]
         L.ref_set_skip_medium.argtypes = [C.c_int]
+        L.ref_obj_load.restype = C.c_void_p
+        L.ref_obj_load.argtypes = [C.c_char_p, C.c_void_p]
+        L.ref_obj_arrays.argtypes = [C.c_void_p, _f32, _i32, _f32, _f32, _i32]
+        L.ref_obj_free.argtypes = [C.c_void_p]
         L.ref_bvh_free.argtypes = [C.c_void_p]
         L.ref_bvh_node_count.restype = C.c_long
         L.ref_bvh_node_count.argtypes = [C.c_void_p]
@@ -557,6 +561,19 @@ class RefOracle:
         dq = np.zeros((n, 4), np.float32)
         self.L.ref_mesh_queries(medium_h, n, p, ins, tri, dq)
         return ins, tri, dq
+
+    def obj_load(self, path):
+        """Mesh::fetchFrom: (vertices, faces, normals, texcoords, face_texcoords) or None."""
+        sizes = np.zeros(4, np.int64)
+        h = self.L.ref_obj_load(path.encode(), sizes.ctypes.data)
+        if not h:
+            return None
+        nv, nf, nn, nt = (int(x) for x in sizes)
+        v, f = np.zeros((nv, 3), np.float32), np.zeros((nf, 3), np.int32)
+        n, t, ft = np.zeros((nn, 3), np.float32), np.zeros((nt, 2), np.float32), np.zeros((nf, 3), np.int32)
+        self.L.ref_obj_arrays(h, v, f, n, t, ft)
+        self.L.ref_obj_free(h)
+        return v, f, n, t, ft
 
     def set_skip_medium(self, skip):
         """g_pathTracerSettings.skip_medium for the scenes prepared from now on."""

@@ -406,6 +406,37 @@ void ref_grid_eval(const char* path, int res, const float* bmin, const float* bm
   }
 }
 
+// ---- Mesh::fetchFrom ---------------------------------------------------------------
+// Loads an OBJ with the reference's reader; sizes[4] = (vertices, faces, normals,
+// texcoords); nullptr if fetchFrom fails.
+void* ref_obj_load(const char* path, long* sizes) {
+  auto* m = new Mesh();
+  if (!m->fetchFrom(path)) {
+    delete m;
+    return nullptr;
+  }
+  sizes[0] = (long)m->vertices_.size();
+  sizes[1] = (long)m->faces_.size();
+  sizes[2] = (long)m->normals_.size();
+  sizes[3] = (long)m->texcoords_.size();
+  return m;
+}
+void ref_obj_arrays(void* h, float* v, int32_t* f, float* n, float* t, int32_t* ft) {
+  auto* m = static_cast<Mesh*>(h);
+  for (size_t i = 0; i < m->vertices_.size(); ++i)
+    for (int c = 0; c < 3; ++c) v[3 * i + c] = m->vertices_[i][c];
+  for (size_t i = 0; i < m->faces_.size(); ++i)
+    for (int c = 0; c < 3; ++c) {
+      f[3 * i + c] = m->faces_[i][c];
+      ft[3 * i + c] = m->faceTexIndices_[i][c];
+    }
+  for (size_t i = 0; i < m->normals_.size(); ++i)
+    for (int c = 0; c < 3; ++c) n[3 * i + c] = m->normals_[i][c];
+  for (size_t i = 0; i < m->texcoords_.size(); ++i)
+    for (int c = 0; c < 2; ++c) t[2 * i + c] = m->texcoords_[i][c];
+}
+void ref_obj_free(void* h) { delete static_cast<Mesh*>(h); }
+
 // ---- bvh/ ---------------------------------------------------------------------------
 struct RefBvh {
   std::vector<Vector3f> v;

@@ -218,6 +218,40 @@ def trace_skip(R, td):
     np.savez_compressed(os.path.join(OUT, "trace_skip.npz"), x=xs, y=ys, k=ks, radiance=rad)
 
 
+OBJ_TEXT = """# tricky numbers and records for Mesh::fetchFrom
+v 0.1 0.2 0.3
+v 1.00000005960464477539 -2.5e-3 3.4028235e38
+v 1e-45 -0 123456789.123456789
+v .5 -.25 7
+vn 0 0 1
+vn 0.577350269 0.577350269 0.577350269
+vt 0.333333343267 0.666666686535 0.9
+vt -1.5 2.5
+vt 0.1 0.7
+o object
+g group
+s 1
+usemtl m
+f 1/1/1 2/2/2 3/3/1
+f 2//1 3//2 4//1
+f -1/-1 -2/-2 -3/-3
+f 1 2 3 4
+f 1 2
+f 4/3 1 2/1\r
+"""
+
+
+def obj_parse(R, td):
+    """Mesh::fetchFrom on an OBJ with long decimals, exponents, relative and
+    missing indices, CR line ends and skipped records and faces."""
+    p = os.path.join(td, "tricky.obj")
+    with open(p, "w", newline="") as fh:
+        fh.write(OBJ_TEXT.replace("\\r", "\r"))
+    v, f, n, t, ft = R.obj_load(p)
+    np.savez_compressed(os.path.join(OUT, "obj_parse.npz"), text=np.frombuffer(open(p, "rb").read(), np.uint8),
+                        vertices=v, faces=f, normals=n, texcoords=t, face_texcoords=ft)
+
+
 def main():
     if len(sys.argv) > 1:
         with tempfile.TemporaryDirectory() as td:
@@ -336,6 +370,7 @@ def main():
     field_media(R, td)
     trace_field(R, td)
     trace_skip(R, td)
+    obj_parse(R, td)
     print("fixtures written to", OUT)
 
 

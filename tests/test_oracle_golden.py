@@ -198,3 +198,23 @@ def test_texture_json_round_trip(tmp_path):
     with pytest.raises(OSError):  # float pixels only under .hdr / .exr names
         S.save_image_raw(str(tmp_path / "f.png"), tex8.astype(np.float32))
         S.load_texture_image(str(tmp_path / "f.png"))
+
+
+def test_obj_loader_matches_fetch_from(golden, tmp_path):
+    """mupsi_obj_load against Mesh::fetchFrom on the same bytes (long
+    decimals, a denormal, -0, relative and missing indices, CR line ends,
+    skipped records and faces): identical arrays, bit for bit."""
+    g = golden("obj_parse.npz")
+    p = tmp_path / "tricky.obj"
+    p.write_bytes(bytes(g["text"]))
+    v, f, n, t, ft = S.load_obj(str(p), texcoords=True)
+    assert np.array_equal(bits(v), bits(g["vertices"]))
+    assert np.array_equal(f, g["faces"]) and np.array_equal(ft, g["face_texcoords"])
+    assert np.array_equal(bits(n), bits(g["normals"])) and np.array_equal(bits(t), bits(g["texcoords"]))
+    with pytest.warns(UserWarning):  # 2 normals for 4 vertices: the reference would read past them
+        m = S.Mesh(v, f, n)
+    assert m.vertex_normals is None
+    bad = tmp_path / "bad.obj"
+    bad.write_text("v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 9\n")
+    with pytest.raises(Exception):
+        S.load_obj(str(bad))
