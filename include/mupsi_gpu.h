@@ -457,6 +457,9 @@ typedef struct mupsi_tuning {
   int32_t min_group;   /* smallest lane group sharing one ray's psi sums: 4, 8, 16 or 32 */
   int32_t shade_block; /* threads per block of the shading kernel: a multiple of 32 in [32, 128] */
   int32_t wave_paths;  /* paths in flight per wave (the queue tile); 0 = 8 Mi */
+  int32_t block_rays;  /* sphere-mean marches: one ray per block, its next 2 x warps psi steps at
+                          once, while the queue holds at most block_rays rays per persistent
+                          block (late bounces); 0 = never. 0..16 */
 } mupsi_tuning;
 int mupsi_gpu_set_tuning(const mupsi_tuning* t);
 int mupsi_gpu_get_tuning(mupsi_tuning* out);

@@ -165,6 +165,7 @@ class Tuning(C.Structure):
         ("min_group", C.c_int32),
         ("shade_block", C.c_int32),
         ("wave_paths", C.c_int32),
+        ("block_rays", C.c_int32),
     ]
 
 

@@ -236,7 +236,7 @@ class DeviceMesh:
 
 
 TUNING_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning.json")
-_TUNING_KEYS = ("march_block", "min_group", "shade_block", "wave_paths")
+_TUNING_KEYS = ("march_block", "min_group", "shade_block", "wave_paths", "block_rays")
 _tuning_applied = False
 
 
@@ -248,7 +248,7 @@ def get_tuning():
 
 
 def set_tuning(**kw):
-    """Change some launch shapes (march_block, min_group, shade_block, wave_paths)."""
+    """Change some launch shapes (march_block, min_group, shade_block, wave_paths, block_rays)."""
     cur = get_tuning()
     for k, v in kw.items():
         if k not in _TUNING_KEYS:

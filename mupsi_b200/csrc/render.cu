@@ -202,16 +202,127 @@ __global__ void k_raygen(const DScene* const* __restrict__ scenes, Paths P, Wave
 // Launch-wide settings of the march and shade kernels.
 struct WaveCfg {
   int min_group;                 // smallest lane group per march
+  int block_rays;                // block-per-ray marches while n <= block_rays * blocks (sphere means)
   int* err;                      // device error word (ERR_* bits)
   unsigned long long* counters;  // nullable work counters
 };
+
+// Short queues of sphere-mean marches (the late bounces): one ray per block.
+// Which steps of such a march need psi is settled without psi (the mean and
+// the per-point bound decide every step, and a psi step without a hit moves
+// the march on by exactly one step), so the block scans ahead for the next
+// 2 x warps of them, each half-warp evaluates psi at one (the 16-slot sum
+// order is the same for any group, so these are the values the one-group
+// march computes), and the first sign change in step order is the hit. The
+// origin, whose psi fixes the sign every step is compared with, goes first
+// alone. Bounded by the march's own step and guard limits.
+__device__ void march_block_rays(const DScene* const* __restrict__ scenes, Paths& P, uint32_t n,
+                                 const uint32_t* __restrict__ q, uint32_t* cursor, const WaveCfg& cfg) {
+  constexpr int kMaxCand = 64;
+  __shared__ uint32_t s_j;
+  __shared__ float s_t[kMaxCand];
+  __shared__ int s_k[kMaxCand];
+  __shared__ int s_hit[kMaxCand];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int ncand_max = min(kMaxCand, 2 * (int)(blockDim.x >> 5));
+  const int cand = 2 * warp + (lane >> 4);  // the candidate this half-warp evaluates
+  Group half;
+  half.G = 16;
+  half.sub = lane & 15;
+  half.mask = (lane >> 4) ? 0xffff0000u : 0x0000ffffu;
+  Group full;
+  full.G = 32;
+  full.sub = lane;
+  full.mask = 0xffffffffu;
+  bool ovf = false;
+  unsigned long long steps = 0, psis = 0, marches = 0, imps = 0;
+  for (;;) {
+    __syncthreads();  // every thread has read the previous s_j
+    if (threadIdx.x == 0) s_j = atomicAdd(cursor, 1u);
+    __syncthreads();
+    const uint32_t j = s_j;
+    if (j >= n) break;
+    const uint32_t idx = q[j];
+    const float4 o = P.o[idx], d = P.d[idx];
+    const int4 meta = P.meta[idx];
+    const int med = __float_as_int(d.w);
+    const DScene* S = scenes[meta_inst(meta.w)];
+    const DMedium& md = S->media[med];
+    if (md.kind != MUPSI_MEDIUM_GP) continue;  // k_march_field marches it
+    March m;
+    march_begin(S, m, mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), o.w, 3.402823466e+38f, med,
+                medium_seed(S, meta.x, meta.y, meta.z, meta_bounce(meta.w)), load_cond(P, idx));
+    m.may_request = false;
+    marches++;
+    {  // the origin (every warp alike)
+      v3 p;
+      if (m.init && march_cheap<MEAN_SPHERE_ONLY>(S, m, p, ovf, &full))
+        march_psi<MEAN_SPHERE_ONLY, true>(S, m, p, full, ovf);
+      m.spec_valid = false;
+    }
+    while (m.status == 0) {
+      int nc = 0;
+      v3 myp = m.o;
+      float mymu = 0.0f;
+      while (nc < ncand_max) {  // the next steps that need psi, assuming none of them is a hit
+        v3 p;
+        if (!march_cheap<MEAN_SPHERE_ONLY>(S, m, p, ovf, nullptr)) break;  // settled without psi (hit or exit)
+        if (cand == nc) {
+          myp = p;
+          mymu = m.pend_mu;
+        }
+        if (threadIdx.x == 0) {
+          s_t[nc] = m.t;
+          s_k[nc] = m.k;
+        }
+        ++nc;
+        march_advance(S, m, -INFINITY);
+        if (m.status != 0) break;
+      }
+      if (cand < nc) {
+        const float qv = (md.k.sigma * psi_sums_group<false, true>(md.k, myp, m.seed, half).x) / md.k.sqrt_var;
+        float f = mymu + qv;
+        if (m.c.active) f += cond_value(md.k, m.c, myp);
+        const bool hit = (f > 0.0f) != m.fprev_pos && (m.fprev_big || (double)fabsf(m.fprev - f) > 1e-6);
+        if (half.sub == 0) s_hit[cand] = hit ? 1 : 0;
+      }
+      __syncthreads();
+      for (int c = 0; c < nc; ++c)
+        if (s_hit[c]) {  // the first candidate with a sign change: the march's hit
+          m.t = s_t[c];
+          m.k = s_k[c];
+          m.status = 1;
+          break;
+        }
+      psis += (unsigned long long)nc;
+      imps += (unsigned long long)nc * 27ull * (unsigned long long)md.k.ppc;
+      __syncthreads();  // s_t / s_k / s_hit are written again next round
+    }
+    if (warp == 0) {
+      mupsi_medium_sample r;
+      march_result<MEAN_SPHERE_ONLY, true>(S, m, r, ovf, full);
+      if (lane == 0) {
+        P.ha[idx] = make_float4(r.t, r.p[0], r.p[1], r.p[2]);
+        P.hb[idx] = make_float4(r.normal[0], r.normal[1], r.normal[2], __uint_as_float(r.exited));
+      }
+    }
+    steps += m.n_steps;
+  }
+  if (ovf) atomicOr(cfg.err, ERR_BVH_STACK);
+  if (cfg.counters && threadIdx.x == 0) {
+    atomicAdd(&cfg.counters[0], steps);
+    atomicAdd(&cfg.counters[1], psis);
+    atomicAdd(&cfg.counters[2], marches);
+    atomicAdd(&cfg.counters[3], imps);
+  }
+}
 
 // Persistent march over the medium queue of iteration `it`. Each ray is
 // marched by a group of G lanes that share its psi sums: G = 4 while the queue
 // fills the resident threads, larger (up to 32) as the queue shrinks, so the
 // late bounces' few long marches finish up to 8x sooner than on one lane.
 template <int MK>
-__global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? 6 : 1) k_march(const DScene* const* __restrict__ scenes, Paths P, int it, int round,
+__global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? 6 : 3) k_march(const DScene* const* __restrict__ scenes, Paths P, int it, int round,
                                                WaveCfg cfg) {
   // round 0 marches the iteration's medium queue; round r >= 1 resumes the
   // marches suspended in round r - 1 with their surrogate predictions
@@ -222,6 +333,12 @@ __global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? 6 : 1) k_march(c
   const uint32_t* q = P.q[it & 1];
   uint32_t* cursor = resume ? P.rcursors + it * R + round : P.cursors + it;
   const bool can_suspend = round + 1 < R;
+  if constexpr (MK == MEAN_SPHERE_ONLY) {
+    if ((uint64_t)n <= (uint64_t)gridDim.x * (uint64_t)cfg.block_rays) {
+      march_block_rays(scenes, P, n, q, cursor, cfg);
+      return;
+    }
+  }
   const unsigned lane = threadIdx.x & 31;
   const uint64_t resident = (uint64_t)gridDim.x * blockDim.x;
   Group grp;
@@ -697,6 +814,8 @@ struct mupsi_scene {
   int width = 0, height = 0, max_bounce = 0;
   // progressive framebuffer: running sum and passes so far
   float* sum = nullptr;
+  float* avg = nullptr;  // device staging of the averaged image for host output (kept: an
+                         // allocation per render would be released and mapped again each time)
   int passes_done = 0;
   int next_pass = -1;  // pass after the last one accumulated
   PathBuf pb;  // wave buffers (grow-only)
@@ -786,6 +905,7 @@ mupsi_scene::~mupsi_scene() {
     for (void* p : grid_mem)
       if (p) cudaFree(p);
     if (sum) cudaFree(sum);
+    if (avg) cudaFree(avg);
     if (pb.mem) pool_give(pb.mem, pb.bytes);
     if (err) cudaFree(err);
     if (counters) cudaFree(counters);
@@ -1011,7 +1131,7 @@ int ensure_paths(mupsi_scene* s, int64_t cap) {
 
 // Launch shapes of the wave kernels (mupsi_gpu_set_tuning; chosen by the
 // project's autotuner, mupsi_b200/autotune.py).
-mupsi_tuning g_tuning = {128, 4, 128, 0};
+mupsi_tuning g_tuning = {128, 4, 128, 0, 1};
 
 // Persistent march grid: resident blocks per SM x SMs.
 struct MarchLaunch {
@@ -1099,6 +1219,7 @@ WaveExec scene_exec(mupsi_scene* s) {
   w.sphere_only = s->h.sphere_only != 0;
   w.field = s->h.field != 0;
   w.cfg.min_group = g_tuning.min_group;
+  w.cfg.block_rays = g_tuning.block_rays;
   w.cfg.err = s->err;
   w.cfg.counters = s->profile ? s->counters : nullptr;
   w.mlp = s->surr_mlp;
@@ -1321,6 +1442,7 @@ void batch_wave_launches(mupsi_batch* b, int iters) {
   w.sphere_only = b->sphere_only;
   w.field = b->field;
   w.cfg.min_group = g_tuning.min_group;
+  w.cfg.block_rays = g_tuning.block_rays;
   w.cfg.err = b->err;
   w.cfg.counters = nullptr;
   WaveSrc src;
@@ -1332,7 +1454,8 @@ void batch_wave_launches(mupsi_batch* b, int iters) {
 }
 
 bool same_tuning(const mupsi_tuning& a, const mupsi_tuning& c) {
-  return a.march_block == c.march_block && a.min_group == c.min_group && a.shade_block == c.shade_block;
+  return a.march_block == c.march_block && a.min_group == c.min_group && a.shade_block == c.shade_block &&
+         a.block_rays == c.block_rays;
 }
 
 // The graph of a wave with `iters` bounce iterations, captured on first use.
@@ -1587,12 +1710,10 @@ int mupsi_gpu_render(mupsi_scene* scene, const mupsi_render_args* a) {
       k_average<<<grid_n(wh * 3), 128, 0, st>>>(scene->sum, wh * 3, inv, a->rgb_out);
       count_launch();
     } else {
-      float* tmp = nullptr;
-      MUPSI_CUDA(cudaMallocAsync((void**)&tmp, wh * 12, st));
-      k_average<<<grid_n(wh * 3), 128, 0, st>>>(scene->sum, wh * 3, inv, tmp);
+      if (!scene->avg) MUPSI_CUDA(cudaMalloc((void**)&scene->avg, wh * 12));
+      k_average<<<grid_n(wh * 3), 128, 0, st>>>(scene->sum, wh * 3, inv, scene->avg);
       count_launch();
-      MUPSI_CUDA(cudaMemcpyAsync(a->rgb_out, tmp, wh * 12, cudaMemcpyDeviceToHost, st));
-      MUPSI_CUDA(cudaFreeAsync(tmp, st));
+      MUPSI_CUDA(cudaMemcpyAsync(a->rgb_out, scene->avg, wh * 12, cudaMemcpyDeviceToHost, st));
     }
   }
   if (dmom) {
@@ -1697,6 +1818,7 @@ int mupsi_gpu_set_tuning(const mupsi_tuning* t) {
   if (t->shade_block < 32 || t->shade_block > 128 || t->shade_block % 32)
     return fail(MUPSI_ERR_INVALID, "shade_block must be a multiple of 32 in [32, 128]");
   if (t->wave_paths < 0 || t->wave_paths > (1 << 28)) return fail(MUPSI_ERR_INVALID, "wave_paths out of range");
+  if (t->block_rays < 0 || t->block_rays > 16) return fail(MUPSI_ERR_INVALID, "block_rays must be in [0, 16]");
   g_tuning = *t;
   return MUPSI_OK;
 }
@@ -1879,12 +2001,10 @@ int mupsi_gpu_batch_render(mupsi_batch* b, const mupsi_batch_args* a) {
         k_average<<<grid_n(wh * 3), 128, 0, bs>>>(s->sum, wh * 3, inv, a->rgb_out[i]);
         count_launch();
       } else {
-        float* tmp = nullptr;
-        MUPSI_CUDA(cudaMallocAsync((void**)&tmp, wh * 12, bs));
-        k_average<<<grid_n(wh * 3), 128, 0, bs>>>(s->sum, wh * 3, inv, tmp);
+        if (!s->avg) MUPSI_CUDA(cudaMalloc((void**)&s->avg, wh * 12));
+        k_average<<<grid_n(wh * 3), 128, 0, bs>>>(s->sum, wh * 3, inv, s->avg);
         count_launch();
-        MUPSI_CUDA(cudaMemcpyAsync(a->rgb_out[i], tmp, wh * 12, cudaMemcpyDeviceToHost, bs));
-        MUPSI_CUDA(cudaFreeAsync(tmp, bs));
+        MUPSI_CUDA(cudaMemcpyAsync(a->rgb_out[i], s->avg, wh * 12, cudaMemcpyDeviceToHost, bs));
       }
     }
   }

@@ -74,12 +74,28 @@ def test_results_do_not_depend_on_launch_shape(gpu, tuning_restored, scene):
     xs, ys, ks = (a.ravel().astype(np.int32) for a in np.meshgrid(np.arange(20), np.arange(20), np.arange(3),
                                                                  indexing="ij"))
     base = None
-    for mb, mg, sb in [(128, 4, 128), (64, 16, 64), (96, 8, 32), (128, 32, 96), (32, 4, 128)]:
-        set_tuning(march_block=mb, min_group=mg, shade_block=sb)
+    # block_rays: 0 keeps every march on lane groups; >= 1 marches these small
+    # queues one ray per block with speculated psi steps (sphere means)
+    for mb, mg, sb, br in [(128, 4, 128, 0), (64, 16, 64, 1), (96, 8, 32, 16), (128, 32, 96, 2), (32, 4, 128, 1)]:
+        set_tuning(march_block=mb, min_group=mg, shade_block=sb, block_rays=br)
         rad = gs.trace(xs, ys, ks)
         if base is None:
             base = rad
-        assert np.array_equal(bits(rad), bits(base)), (mb, mg, sb)
+        assert np.array_equal(bits(rad), bits(base)), (mb, mg, sb, br)
+
+
+def test_block_rays_render_matches(gpu, tuning_restored):
+    """A full 96x96x6 configuration-0 render with the block-per-ray march for
+    every short queue (block_rays 16) and for none (0): identical images."""
+    sc = S.config0_scene(96, 96, 6)
+    imgs = []
+    for br in (0, 16, 1):
+        set_tuning(block_rays=br)
+        r = GpuRenderer()
+        r.prepare_render(GpuScene(sc))
+        imgs.append(r.start_render_progressive(6))
+    assert np.array_equal(bits(imgs[0]), bits(imgs[1])) and np.array_equal(bits(imgs[0]), bits(imgs[2]))
+    assert (imgs[0][..., 0] < 1).sum() > 100
 
 
 def test_batch_completion_order_and_device_output(gpu, tuning_restored):
@@ -119,3 +135,5 @@ def test_batch_zero_spp_and_errors(gpu):
         set_tuning(min_group=2)
     with pytest.raises(MupsiError):
         set_tuning(march_block=256)
+    with pytest.raises(MupsiError):
+        set_tuning(block_rays=17)
