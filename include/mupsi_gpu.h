@@ -459,7 +459,7 @@ typedef struct mupsi_tuning {
   int32_t wave_paths;  /* paths in flight per wave (the queue tile); 0 = 8 Mi */
   int32_t block_rays;  /* sphere-mean marches: one ray per block, its next 2 x warps psi steps at
                           once, while the queue holds at most block_rays rays per persistent
-                          block (late bounces); 0 = never. 0..16 */
+                          block (late bounces); 0 = never. 0..256 */
 } mupsi_tuning;
 int mupsi_gpu_set_tuning(const mupsi_tuning* t);
 int mupsi_gpu_get_tuning(mupsi_tuning* out);

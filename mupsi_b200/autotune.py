@@ -27,9 +27,9 @@ CANDIDATES = {
     "min_group": [4, 8, 16, 32],
     "shade_block": [64, 128],
     "wave_paths": [1 << 21, 1 << 22, 1 << 23, 1 << 24],
-    "block_rays": [0, 1, 2, 4],
+    "block_rays": [0, 4, 8, 16],
 }
-DEFAULT = {"march_block": 128, "min_group": 4, "shade_block": 128, "wave_paths": 1 << 23, "block_rays": 1}
+DEFAULT = {"march_block": 128, "min_group": 4, "shade_block": 128, "wave_paths": 1 << 23, "block_rays": 8}
 
 
 def coordinate_descent(measure, candidates=CANDIDATES, start=DEFAULT, passes=2):

@@ -216,15 +216,37 @@ struct WaveCfg {
 // march computes), and the first sign change in step order is the hit. The
 // origin, whose psi fixes the sign every step is compared with, goes first
 // alone. Bounded by the march's own step and guard limits.
+// Window positions below `stop` in warp w's lanes.
+__device__ __forceinline__ unsigned below(int stop, int w) {
+  const int b = stop - 32 * w;
+  return b >= 32 ? 0xffffffffu : (b <= 0 ? 0u : ((1u << b) - 1u));
+}
+// Window position of the r-th (from 0) step needing psi below `stop`.
+__device__ __forceinline__ int nth_need(const unsigned* need, int nw, int stop, int r) {
+  for (int w = 0; w < nw; ++w) {
+    unsigned msk = need[w] & below(stop, w);
+    const int c = __popc(msk);
+    if (r < c) {
+      for (int i = 0; i < r; ++i) msk &= msk - 1u;
+      return 32 * w + __ffs(msk) - 1;
+    }
+    r -= c;
+  }
+  return 0;  // not reached: r < the count of such steps
+}
+
 __device__ void march_block_rays(const DScene* const* __restrict__ scenes, Paths& P, uint32_t n,
                                  const uint32_t* __restrict__ q, uint32_t* cursor, const WaveCfg& cfg) {
-  constexpr int kMaxCand = 64;
+  constexpr int kMaxWarps = 4, kWindow = 32 * kMaxWarps;
   __shared__ uint32_t s_j;
-  __shared__ float s_t[kMaxCand];
-  __shared__ int s_k[kMaxCand];
-  __shared__ int s_hit[kMaxCand];
+  __shared__ float s_tw[kWindow], s_mw[kWindow];
+  __shared__ int s_cls[kWindow];
+  __shared__ int s_hit[2 * kMaxWarps];
+  __shared__ unsigned s_need[kMaxWarps], s_end[kMaxWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int ncand_max = min(kMaxCand, 2 * (int)(blockDim.x >> 5));
+  const int nw = min(kMaxWarps, (int)(blockDim.x >> 5));
+  const int W = 32 * nw;  // window of steps classified per round
+  const int ncand_max = 2 * nw;
   const int cand = 2 * warp + (lane >> 4);  // the candidate this half-warp evaluates
   Group half;
   half.G = 16;
@@ -261,25 +283,54 @@ __device__ void march_block_rays(const DScene* const* __restrict__ scenes, Paths
       m.spec_valid = false;
     }
     while (m.status == 0) {
-      int nc = 0;
-      v3 myp = m.o;
-      float mymu = 0.0f;
-      while (nc < ncand_max) {  // the next steps that need psi, assuming none of them is a hit
-        v3 p;
-        if (!march_cheap<MEAN_SPHERE_ONLY>(S, m, p, ovf, nullptr)) break;  // settled without psi (hit or exit)
-        if (cand == nc) {
-          myp = p;
-          mymu = m.pend_mu;
+      // candidate 0: the march's next psi step; jumps, certain hits and the
+      // end are settled on the way exactly as the one-group march settles them
+      v3 p0;
+      if (!march_cheap<MEAN_SPHERE_ONLY>(S, m, p0, ovf, nullptr)) break;
+      const int k0 = m.k;
+      const float mu0 = m.pend_mu;
+      // the next W steps (table marches), one per thread: 0 sign settled and
+      // kept, 1 needs psi, 2 sign settled and changed (hit), 3 past the end
+      int stop = W, total = 0, take = 0;
+      if (m.use_tab) {
+        const int i = (int)threadIdx.x, kk = k0 + 1 + i;
+        int cls = 3;
+        if (i < W && kk < S->tab_steps) {
+          const float tw = __ldg(S->tab + kk);
+          const v3 pw = m.o + m.d * tw;
+          const float mw = mean_value<MEAN_SPHERE_ONLY>(S, md, pw, ovf);
+          const float lb = fabsf(mw);
+          if (lb * 0.999999f > m.B || lb * 0.999999f > noise_bound_at(md.k, m.c, pw))
+            cls = ((mw > 0.0f) != m.fprev_pos) ? 2 : 0;
+          else
+            cls = 1;
+          s_tw[i] = tw;
+          s_mw[i] = mw;
         }
-        if (threadIdx.x == 0) {
-          s_t[nc] = m.t;
-          s_k[nc] = m.k;
+        const unsigned need = __ballot_sync(0xffffffffu, cls == 1), end = __ballot_sync(0xffffffffu, cls >= 2);
+        if (i < W && cls >= 2) s_cls[i] = cls;
+        if (lane == 0 && warp < kMaxWarps) {
+          s_need[warp] = need;
+          s_end[warp] = end;
         }
-        ++nc;
-        march_advance(S, m, -INFINITY);
-        if (m.status != 0) break;
+        __syncthreads();
+        for (int w = 0; w < nw; ++w)
+          if (s_end[w]) {
+            stop = 32 * w + __ffs(s_end[w]) - 1;
+            break;
+          }
+        for (int w = 0; w < nw; ++w) total += __popc(s_need[w] & below(stop, w));
+        take = min(total, ncand_max - 1);
       }
+      const int nc = 1 + take;
       if (cand < nc) {
+        v3 myp = p0;
+        float mymu = mu0;
+        if (cand > 0) {
+          const int pos = nth_need(s_need, nw, stop, cand - 1);
+          myp = m.o + m.d * s_tw[pos];
+          mymu = s_mw[pos];
+        }
         const float qv = (md.k.sigma * psi_sums_group<false, true>(md.k, myp, m.seed, half).x) / md.k.sqrt_var;
         float f = mymu + qv;
         if (m.c.active) f += cond_value(md.k, m.c, myp);
@@ -287,16 +338,41 @@ __device__ void march_block_rays(const DScene* const* __restrict__ scenes, Paths
         if (half.sub == 0) s_hit[cand] = hit ? 1 : 0;
       }
       __syncthreads();
+      int first = -1;
       for (int c = 0; c < nc; ++c)
-        if (s_hit[c]) {  // the first candidate with a sign change: the march's hit
-          m.t = s_t[c];
-          m.k = s_k[c];
-          m.status = 1;
+        if (s_hit[c]) {
+          first = c;
           break;
         }
+      if (first == 0) {  // at candidate 0's step, where march_cheap left the march
+        m.status = 1;
+      } else if (first > 0) {
+        const int pos = nth_need(s_need, nw, stop, first - 1);
+        m.k = k0 + 1 + pos;
+        m.t = s_tw[pos];
+        m.status = 1;
+      } else if (!m.use_tab) {
+        march_advance(S, m, -INFINITY);  // one step on, as after a psi step without a hit
+      } else if (take < total) {  // more psi steps in the window than candidates: resume after the last one
+        m.k = k0 + 2 + nth_need(s_need, nw, stop, take - 1);
+        m.t = __ldg(S->tab + m.k);
+      } else if (stop < W) {  // the window's first settled change of sign, or the end
+        m.k = k0 + 1 + stop;
+        if (s_cls[stop] == 2) {
+          m.t = s_tw[stop];
+          m.status = 1;
+        } else {
+          m.t = __ldg(S->tab + m.k);
+          m.status = 2;
+        }
+      } else {
+        m.k = k0 + 1 + W;
+        m.t = __ldg(S->tab + m.k);
+      }
+      m.n_steps += (uint32_t)min(stop, W);
       psis += (unsigned long long)nc;
       imps += (unsigned long long)nc * 27ull * (unsigned long long)md.k.ppc;
-      __syncthreads();  // s_t / s_k / s_hit are written again next round
+      __syncthreads();  // the shared candidate state is written again next round
     }
     if (warp == 0) {
       mupsi_medium_sample r;
@@ -1131,7 +1207,7 @@ int ensure_paths(mupsi_scene* s, int64_t cap) {
 
 // Launch shapes of the wave kernels (mupsi_gpu_set_tuning; chosen by the
 // project's autotuner, mupsi_b200/autotune.py).
-mupsi_tuning g_tuning = {128, 4, 128, 0, 1};
+mupsi_tuning g_tuning = {128, 4, 128, 0, 8};
 
 // Persistent march grid: resident blocks per SM x SMs.
 struct MarchLaunch {
@@ -1818,7 +1894,7 @@ int mupsi_gpu_set_tuning(const mupsi_tuning* t) {
   if (t->shade_block < 32 || t->shade_block > 128 || t->shade_block % 32)
     return fail(MUPSI_ERR_INVALID, "shade_block must be a multiple of 32 in [32, 128]");
   if (t->wave_paths < 0 || t->wave_paths > (1 << 28)) return fail(MUPSI_ERR_INVALID, "wave_paths out of range");
-  if (t->block_rays < 0 || t->block_rays > 16) return fail(MUPSI_ERR_INVALID, "block_rays must be in [0, 16]");
+  if (t->block_rays < 0 || t->block_rays > 256) return fail(MUPSI_ERR_INVALID, "block_rays must be in [0, 256]");
   g_tuning = *t;
   return MUPSI_OK;
 }

@@ -136,4 +136,4 @@ def test_batch_zero_spp_and_errors(gpu):
     with pytest.raises(MupsiError):
         set_tuning(march_block=256)
     with pytest.raises(MupsiError):
-        set_tuning(block_rays=17)
+        set_tuning(block_rays=257)
