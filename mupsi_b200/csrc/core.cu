@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "core.cuh"
@@ -198,12 +199,73 @@ static int psi_common(bool grad, const mupsi_kernel* kernel, int64_t n, const fl
   return MUPSI_OK;
 }
 
+// ------------------------------------------------------- buffer cache
+namespace {
+struct CachedBuf {
+  int dev;
+  size_t cls;
+  void* p;
+};
+std::mutex g_buf_mu;
+std::vector<CachedBuf> g_buf_free;
+std::unordered_map<void*, CachedBuf> g_buf_live;
+size_t g_buf_cached = 0;
+constexpr size_t kBufMax = size_t(16) << 20, kBufCap = size_t(256) << 20;
+}  // namespace
+
+cudaError_t dev_take(void** out, size_t bytes) {
+  if (bytes > kBufMax) return cudaMalloc(out, bytes);  // not cached: cudaFree'd by dev_give
+  size_t cls = 256;
+  while (cls < bytes) cls <<= 1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  {
+    std::lock_guard<std::mutex> lock(g_buf_mu);
+    for (size_t i = 0; i < g_buf_free.size(); ++i)
+      if (g_buf_free[i].dev == dev && g_buf_free[i].cls == cls) {
+        const CachedBuf b = g_buf_free[i];
+        g_buf_free[i] = g_buf_free.back();
+        g_buf_free.pop_back();
+        g_buf_cached -= cls;
+        g_buf_live[b.p] = b;
+        *out = b.p;
+        return cudaSuccess;
+      }
+  }
+  void* p = nullptr;
+  const cudaError_t e = cudaMalloc(&p, cls);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(g_buf_mu);
+  g_buf_live[p] = CachedBuf{dev, cls, p};
+  *out = p;
+  return cudaSuccess;
+}
+
+void dev_give(void* p) {
+  if (!p) return;
+  {
+    std::lock_guard<std::mutex> lock(g_buf_mu);
+    auto it = g_buf_live.find(p);
+    if (it != g_buf_live.end()) {
+      const CachedBuf b = it->second;
+      g_buf_live.erase(it);
+      if (g_buf_cached + b.cls <= kBufCap) {
+        g_buf_free.push_back(b);
+        g_buf_cached += b.cls;
+        return;
+      }
+    }
+  }
+  cudaFree(p);
+}
+
 // ------------------------------------------------------------ meshes / BVH
 struct MeshStore {
   DMesh d;
   std::vector<void*> allocs;
   ~MeshStore() {
-    for (void* p : allocs) cudaFree(p);
+    cudaDeviceSynchronize();  // nothing in flight reads the buffers handed back
+    for (void* p : allocs) dev_give(p);
   }
 };
 
@@ -214,7 +276,7 @@ static cudaError_t upload(std::vector<void*>& allocs, const T* src, size_t count
     return cudaSuccess;
   }
   void* p = nullptr;
-  cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+  cudaError_t e = dev_take(&p, count * sizeof(T));
   if (e != cudaSuccess) return e;
   allocs.push_back(p);
   e = cudaMemcpy(p, src, count * sizeof(T), cudaMemcpyHostToDevice);

@@ -18,6 +18,15 @@ cudaStream_t resolve_stream(void* s);
 int num_sms();
 int make_device_mesh(const mupsi_mesh_desc& md, DMesh& d, std::vector<void*>& allocs);
 
+// Device buffers that live as long as a scene or mesh: released ones stay in a
+// per-device cache (power-of-two size classes from 256 B, buffers up to 16 MB,
+// 256 MB in all) and are handed out again, so a host that creates and
+// releases a scene per frame pays no cudaMalloc / cudaFree (each may
+// synchronise the device) after the first. dev_give's caller has
+// synchronised: no work in flight uses the buffer.
+cudaError_t dev_take(void** out, size_t bytes);
+void dev_give(void* p);
+
 // A buffer of one batch call: aliases the caller's pointer for device memory,
 // otherwise a stream-ordered device allocation with the copy in (in()) or the
 // copy back (finish()); the caller synchronises the stream before returning.

@@ -971,20 +971,21 @@ void pool_give(void* p, size_t bytes) {
 
 mupsi_scene::~mupsi_scene() {
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
-    for (void* p : allocs) cudaFree(p);
-    if (d) cudaFree(d);
-    if (d_list) cudaFree(d_list);
-    if (d_chunk) cudaFree(d_chunk);
+    cudaDeviceSynchronize();  // nothing in flight reads the buffers handed back
+    for (void* p : allocs) dev_give(p);
+    dev_give(d);
+    dev_give(d_list);
+    dev_give(d_chunk);
     if (sky_mem) cudaFree(sky_mem);
     for (void* p : tex_mem)
       if (p) cudaFree(p);
     for (void* p : grid_mem)
       if (p) cudaFree(p);
-    if (sum) cudaFree(sum);
-    if (avg) cudaFree(avg);
+    dev_give(sum);
+    dev_give(avg);
     if (pb.mem) pool_give(pb.mem, pb.bytes);
-    if (err) cudaFree(err);
-    if (counters) cudaFree(counters);
+    dev_give(err);
+    dev_give(counters);
 }
 
 namespace {
@@ -1104,7 +1105,7 @@ int build_scene(const mupsi_scene_desc* desc, mupsi_scene* s) {
     tab.push_back(t);
     const float* dtab = nullptr;
     void* p = nullptr;
-    MUPSI_CUDA(cudaMalloc(&p, tab.size() * sizeof(float)));
+    MUPSI_CUDA(dev_take(&p, tab.size() * sizeof(float)));
     s->allocs.push_back(p);
     MUPSI_CUDA(cudaMemcpy(p, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice));
     dtab = (const float*)p;
@@ -1114,21 +1115,21 @@ int build_scene(const mupsi_scene_desc* desc, mupsi_scene* s) {
     S.tab_ft = ft;
     S.tab_dt = dt;
   }
-  MUPSI_CUDA(cudaMalloc(&s->err, sizeof(int)));
+  MUPSI_CUDA(dev_take((void**)&s->err, sizeof(int)));
   MUPSI_CUDA(cudaMemset(s->err, 0, sizeof(int)));
   S.err = s->err;
-  MUPSI_CUDA(cudaMalloc(&s->counters, 8 * sizeof(unsigned long long)));
+  MUPSI_CUDA(dev_take((void**)&s->counters, 8 * sizeof(unsigned long long)));
   MUPSI_CUDA(cudaMemset(s->counters, 0, 8 * sizeof(unsigned long long)));
   S.counters = nullptr;
-  MUPSI_CUDA(cudaMalloc(&s->d, sizeof(DScene)));
+  MUPSI_CUDA(dev_take((void**)&s->d, sizeof(DScene)));
   MUPSI_CUDA(cudaMemcpy(s->d, &S, sizeof(DScene), cudaMemcpyHostToDevice));
-  MUPSI_CUDA(cudaMalloc(&s->d_list, sizeof(DScene*)));
+  MUPSI_CUDA(dev_take((void**)&s->d_list, sizeof(DScene*)));
   MUPSI_CUDA(cudaMemcpy(s->d_list, &s->d, sizeof(DScene*), cudaMemcpyHostToDevice));
-  MUPSI_CUDA(cudaMalloc(&s->d_chunk, sizeof(WaveChunk)));
+  MUPSI_CUDA(dev_take((void**)&s->d_chunk, sizeof(WaveChunk)));
   s->width = desc->width;
   s->height = desc->height;
   s->max_bounce = desc->max_bounce;
-  MUPSI_CUDA(cudaMalloc(&s->sum, (size_t)3 * desc->width * desc->height * sizeof(float)));
+  MUPSI_CUDA(dev_take((void**)&s->sum, (size_t)3 * desc->width * desc->height * sizeof(float)));
   MUPSI_CUDA(cudaMemset(s->sum, 0, (size_t)3 * desc->width * desc->height * sizeof(float)));
   return MUPSI_OK;
 }
@@ -1786,7 +1787,7 @@ int mupsi_gpu_render(mupsi_scene* scene, const mupsi_render_args* a) {
       k_average<<<grid_n(wh * 3), 128, 0, st>>>(scene->sum, wh * 3, inv, a->rgb_out);
       count_launch();
     } else {
-      if (!scene->avg) MUPSI_CUDA(cudaMalloc((void**)&scene->avg, wh * 12));
+      if (!scene->avg) MUPSI_CUDA(dev_take((void**)&scene->avg, wh * 12));
       k_average<<<grid_n(wh * 3), 128, 0, st>>>(scene->sum, wh * 3, inv, scene->avg);
       count_launch();
       MUPSI_CUDA(cudaMemcpyAsync(a->rgb_out, scene->avg, wh * 12, cudaMemcpyDeviceToHost, st));
@@ -2077,7 +2078,7 @@ int mupsi_gpu_batch_render(mupsi_batch* b, const mupsi_batch_args* a) {
         k_average<<<grid_n(wh * 3), 128, 0, bs>>>(s->sum, wh * 3, inv, a->rgb_out[i]);
         count_launch();
       } else {
-        if (!s->avg) MUPSI_CUDA(cudaMalloc((void**)&s->avg, wh * 12));
+        if (!s->avg) MUPSI_CUDA(dev_take((void**)&s->avg, wh * 12));
         k_average<<<grid_n(wh * 3), 128, 0, bs>>>(s->sum, wh * 3, inv, s->avg);
         count_launch();
         MUPSI_CUDA(cudaMemcpyAsync(a->rgb_out[i], s->avg, wh * 12, cudaMemcpyDeviceToHost, bs));
