@@ -3,7 +3,8 @@
     python -m mupsi_b200.autotune [--out mupsi_b200/tuning.json] [--spp-div 4] [--passes 2]
 
 Tunes the persistent march's block size, the smallest lane group per ray, the
-shading block size and the paths per wave (the queue tile) by coordinate
+shading block size, the paths per wave (the queue tile) and the queue size
+per block below which sphere-mean rays are marched one per block by coordinate
 descent on two workloads: a batched render of the seeded uneven instances of
 scene.batch_scenes (pass counts divided by --spp-div to keep a trial short)
 and the 256x256x20 configuration-0 render. Both are timed on the device with
