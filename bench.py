@@ -343,16 +343,19 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
-EXTRAS = ("config1", "config2", "config4", "config3")
+EXTRAS = ("config1", "config2", "config4", "config3", "next")
 
 
 def run_extras(args, only=None):
     """The other configurations on the same GPU, device-timed with CUDA events:
     1 (psi microbench), 2 (level-6 mesh mean render), 4 (batched instances) and
-    3 (level-8 mesh, exact mean against the surrogate). `only` runs one of them."""
+    3 (level-8 mesh, exact mean against the surrogate), and the scene features
+    beyond the configurations (image skydrome, textured mesh, SDF and external
+    GP media, the progressive display). `only` runs one of them."""
     out = {}
     legs = {"config1": ("config1_psi", run_psi_sweep), "config2": ("config2_mesh", run_mesh),
-            "config4": ("config4_batch", run_batch), "config3": ("config3_surrogate", run_surrogate)}
+            "config4": ("config4_batch", run_batch), "config3": ("config3_surrogate", run_surrogate),
+            "next": ("scene_features", run_scene_features)}
     for name in EXTRAS:
         if only is None or only == name:
             key, fn = legs[name]
@@ -400,6 +403,120 @@ def run_psi_sweep():
                 sweep[f"L{L}_aniso{az:g}_ppc{ppc}"] = {"ms": round(ms, 3), "Gqueries_s": round(n / ms / 1e6, 3)}
     return {"queries_per_point": n, "points": 18, "total_ms": round(total_ms, 2),
             "Gimpulse_evals_s": round(imps / total_ms / 1e6, 1), "sweep": sweep}
+
+
+def _reference_scene(engine, sc, td, name):
+    """Write what the reference's Controller::load reads for scene `sc` (OBJ
+    files with texcoords, raw images, GridMeanFunction grids, scene.json) and
+    load it into the reference timing build."""
+    from mupsi_b200 import scene as S
+    objs = []
+    for i, m in enumerate(sc.meshes):
+        op = os.path.join(td, f"{name}_{i}.obj")
+        S.save_obj(op, m.vertices, m.faces, m.texcoords, m.face_texcoords)
+        objs.append(op)
+    sky_path = None
+    if sc.sky_texture is not None:
+        sky_path = os.path.join(td, f"{name}_sky.hdr")
+        S.save_image_raw(sky_path, sc.sky_texture)
+    tex = {}
+    for i, pr in enumerate(sc.primitives):
+        if pr.get("texture") is not None:
+            tex[i] = os.path.join(td, f"{name}_tex{i}.hdr")
+            S.save_image_raw(tex[i], pr["texture"])
+    grids = None
+    m0 = sc.media[0] if sc.media else {}
+    if m0.get("kind") == "external_gp":
+        m0["mean_grid"].tofile(os.path.join(td, f"{name}_mean.bin"))
+        vp = None
+        if m0["var_grid"] is not None:
+            vp = f"{name}_var.bin"
+            m0["var_grid"].tofile(os.path.join(td, vp))
+        grids = (f"{name}_mean.bin", vp)
+    j, extra = sc.to_json(obj_paths=objs, sky_path=sky_path, texture_paths=tex, grid_paths=grids)
+    jp = os.path.join(td, f"{name}.json")
+    with open(jp, "w") as fh:
+        json.dump(j, fh)
+    return engine.scene_load(jp, sky=None if sky_path else 1.0, extra_meshes=extra)
+
+
+def run_scene_features(cpu_seconds=2.0):
+    """The scene features beyond configurations 0-4 at 256x256x20 (the
+    configuration-0 camera and bounce limit): GPU device time of a full render
+    (median of 3 after a warm-up) and the reference's timing build on a strided
+    pixel subset of the same scene; and the progressive display publishing a
+    frame after every pass of the configuration-0 scene."""
+    import torch
+    from mupsi_b200 import scene as S
+    from mupsi_b200.api import GpuDisplay, GpuRenderer, GpuScene
+
+    rng = np.random.default_rng(31)
+    sky = rng.uniform(0.2, 3.0, (128, 256, 3)).astype(np.float32)
+    tex = rng.uniform(0.05, 0.95, (64, 64, 3)).astype(np.float32)
+    scenes = {}
+    s0 = S.config0_scene(W, H, SPP)
+    s0.sky_texture = sky
+    scenes["sky_texture"] = s0
+    scenes["albedo_texture"] = S.textured_floor_scene(tex, True, W, H, SPP)
+    for kind in ("sdf_sphere", "sdf_mesh", "external_gp"):
+        scenes[kind] = S.field_scene(kind, W, H, SPP)
+    kind, eng = _cpu_engine()
+    td = tempfile.mkdtemp()
+    out = {}
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for name, sc in scenes.items():
+        gs = GpuScene(sc)
+        r = GpuRenderer()
+        r.prepare_render(gs)
+        fb = torch.empty((H, W, 3), device="cuda")
+        r.start_render_progressive(SPP, out=fb)
+        ts = []
+        for _ in range(3):
+            flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            r.start_render_progressive(SPP, out=fb)
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        gs.close()
+        ms = float(np.median(ts))
+        entry = {"gpu_ms": round(ms, 3), "gpu_samples_per_s": SAMPLES_PER_STEP / (ms / 1000.0)}
+        if kind == "reference":
+            h = _reference_scene(eng, sc, td, name)
+            xs, ys, ks, _ = _cpu_samples(SPP * 256)  # 256 pixels on the image's diagonal: a fair rate estimate
+            t = time.perf_counter()
+            eng.trace(h, xs, ys, ks)
+            rate0 = len(xs) / (time.perf_counter() - t)
+            xs, ys, ks, stride = _cpu_samples(int(max(SPP * 64, rate0 * cpu_seconds)), offset=1)
+            t = time.perf_counter()
+            eng.trace(h, xs, ys, ks)
+            cpu = len(xs) / (time.perf_counter() - t)
+            eng.scene_free(h)
+            entry.update({"cpu_reference_samples_per_s": cpu, "cpu_sample": f"{len(xs)} samples, every {stride}th "
+                          f"pixel x {SPP} passes, {eng.num_threads()} threads", "gpu_over_cpu": entry["gpu_samples_per_s"] / cpu})
+        out[name] = entry
+    # progressive display: a frame (pinned front/back swap) after every pass
+    d = GpuDisplay(S.config0_scene(W, H, 64))
+    d.start_progressive(2, 1)
+    while d.running():
+        time.sleep(0.001)
+    d.stop()
+    frames = 0
+    t0 = time.perf_counter()
+    d.start_progressive(64, 1)
+    while d.running() or d.is_spp_pass_done():
+        if d.is_spp_pass_done():
+            d.ack_spp_pass()
+            frames += 1
+        time.sleep(0.0002)
+    d.stop()
+    wall = time.perf_counter() - t0
+    out["progressive_display"] = {"workload": "configuration 0, 256x256, 64 passes, a frame after every pass",
+                                  "wall_s": round(wall, 4), "passes_per_s": 64 / wall,
+                                  "frames_seen_by_poller": frames, "current_spp": d.current_spp()}
+    d.close()
+    return out
 
 
 def run_mesh():
