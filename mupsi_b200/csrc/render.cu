@@ -62,6 +62,19 @@ struct Paths {
   float* pred[2];
   uint32_t* rcounts;    // [it * rounds + r]: requests made in round r
   uint32_t* rcursors;   // [it * rounds + r]: work cursor of round r >= 1
+  // deferred shadow rays (sh_a null: transmittance is marched inline in the
+  // shading kernel): the NEE of a medium event at iteration it leaves a job at
+  // its path's slot, queued in sq[(it + 1) & 1]; the march launch of iteration
+  // it + 1 marches it and adds the term
+  float4* sh_a;         // origin xyz, far_t
+  float4* sh_b;         // direction xyz, medium (int bits)
+  float4* sh_x;         // X = thr * f * light weight (xyz), c = |cos| (w): the term is (tr * X) * c
+  float4* sh_ca;        // the conditioning at the event (C xyz, u)
+  float4* sh_cb;        //   (g xyz, active)
+  int4* sh_m;           // x: 1 = add to the final radiance (the path ended there), 0 = to its emission; y: seed
+  uint32_t* sq[2];
+  uint32_t* scounts;    // [it]: jobs for the march launch of iteration it
+  uint32_t* scursors;
 };
 
 MD uint64_t ld_rng(const uint2 v) { return ((uint64_t)v.y << 32) | v.x; }
@@ -157,6 +170,11 @@ __global__ void k_wave_begin(Paths P, int iters, int* wave_idx) {
       P.rcounts[i] = 0;
       P.rcursors[i] = 0;
     }
+  if (P.scounts)
+    for (int i = threadIdx.x; i < iters + 1; i += blockDim.x) {
+      P.scounts[i] = 0;
+      P.scursors[i] = 0;
+    }
   if (wave_idx && threadIdx.x == 0) *wave_idx += 1;
 }
 
@@ -201,6 +219,8 @@ __global__ void k_raygen(const DScene* const* __restrict__ scenes, Paths P, Wave
 
 // Launch-wide settings of the march and shade kernels.
 struct WaveCfg {
+  int defer;                     // shading leaves GP-medium shadow rays as jobs for the next march launch
+  int shadow_pass;               // this march launch marches the shadow jobs of iteration `it`
   int min_group;                 // smallest lane group per march
   int block_rays;                // block-per-ray marches while n <= block_rays * blocks (sphere means)
   int* err;                      // device error word (ERR_* bits)
@@ -403,14 +423,17 @@ __global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? 6 : 3) k_march(c
   // round 0 marches the iteration's medium queue; round r >= 1 resumes the
   // marches suspended in round r - 1 with their surrogate predictions
   // (a scene with sphere means only has no surrogate: one round, no resumes)
-  const bool resume = MK != MEAN_SPHERE_ONLY && round > 0;
+  // a shadow pass marches the shadow jobs the shading of iteration it - 1 left
+  // (GPMedium::transmittance, gpmedium.cpp:105-129) instead of the medium queue
+  const bool shadow = cfg.shadow_pass != 0;
+  const bool resume = MK != MEAN_SPHERE_ONLY && round > 0 && !shadow;
   const int R = P.rounds;
-  const uint32_t n = resume ? P.rcounts[it * R + round - 1] : P.counts[2 * it];
-  const uint32_t* q = P.q[it & 1];
-  uint32_t* cursor = resume ? P.rcursors + it * R + round : P.cursors + it;
-  const bool can_suspend = round + 1 < R;
+  const uint32_t n = shadow ? P.scounts[it] : resume ? P.rcounts[it * R + round - 1] : P.counts[2 * it];
+  const uint32_t* q = shadow ? P.sq[it & 1] : P.q[it & 1];
+  uint32_t* cursor = shadow ? P.scursors + it : resume ? P.rcursors + it * R + round : P.cursors + it;
+  const bool can_suspend = round + 1 < R && !shadow;
   if constexpr (MK == MEAN_SPHERE_ONLY) {
-    if ((uint64_t)n <= (uint64_t)gridDim.x * (uint64_t)cfg.block_rays) {
+    if (!shadow && (uint64_t)n <= (uint64_t)gridDim.x * (uint64_t)cfg.block_rays) {
       march_block_rays(scenes, P, n, q, cursor, cfg);
       return;
     }
@@ -447,8 +470,21 @@ __global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? 6 : 3) k_march(c
           int4 meta = P.meta[idx];
           int med = __float_as_int(d.w);
           S = scenes[meta_inst(meta.w)];
-          skipped = !resume && S->media[med].kind != MUPSI_MEDIUM_GP;  // k_march_field marches it
-          if (!skipped) {
+          if (shadow) {  // the shadow ray of the job (its own medium, seed and conditioning)
+            const float4 a = P.sh_a[idx], b = P.sh_b[idx], ca = P.sh_ca[idx], cb = P.sh_cb[idx];
+            med = __float_as_int(b.w);
+            Cond c;
+            c.C = mk3(ca.x, ca.y, ca.z);
+            c.u = ca.w;
+            c.g = mk3(cb.x, cb.y, cb.z);
+            c.active = __float_as_uint(cb.w);
+            march_begin(S, m, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), 0.0f, a.w, med, (uint32_t)P.sh_m[idx].y, c);
+            m.may_request = false;
+            if (grp.sub == 0) marches++;
+            active = true;
+          }
+          skipped = !shadow && !resume && S->media[med].kind != MUPSI_MEDIUM_GP;  // k_march_field marches it
+          if (!skipped && !shadow) {
             march_begin(S, m, mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), o.w, 3.402823466e+38f, med,
                         medium_seed(S, meta.x, meta.y, meta.z, meta_bounce(meta.w)), load_cond(P, idx));
             m.may_request = MK != MEAN_SPHERE_ONLY && can_suspend && m.lazy && S->media[med].surr;
@@ -487,6 +523,27 @@ __global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? 6 : 3) k_march(c
           const uint32_t slot = atomicAdd(&P.rcounts[it * R + round], 1u);
           P.req[round & 1][slot] = make_float4(p.x, p.y, p.z, __uint_as_float(idx));
           reqs++;
+          steps += m.n_steps;
+          psis += m.n_psi;
+          imps += (unsigned long long)m.n_psi * 27ull * (unsigned long long)S->media[m.medium].k.ppc;
+          mus += m.n_mu;
+          pars += m.n_par;
+        }
+        active = false;
+      } else if (m.status != 0 && shadow) {
+        if (grp.sub == 0) {  // transmittance 0 at a sign change: the NEE term (tr * X) * c
+          const float tr = m.status == 1 ? 0.0f : 1.0f;
+          const float4 x = P.sh_x[idx];
+          const float tx = (tr * x.x) * x.w, ty = (tr * x.y) * x.w, tz = (tr * x.z) * x.w;
+          if (P.sh_m[idx].x) {  // the path ended at that event: its radiance is written
+            float* r = P.rad + 3 * (int64_t)idx;
+            r[0] = r[0] + tx;
+            r[1] = r[1] + ty;
+            r[2] = r[2] + tz;
+          } else {
+            const float4 e = P.em[idx];
+            P.em[idx] = make_float4(e.x + tx, e.y + ty, e.z + tz, e.w);
+          }
           steps += m.n_steps;
           psis += m.n_psi;
           imps += (unsigned long long)m.n_psi * 27ull * (unsigned long long)S->media[m.medium].k.ppc;
@@ -591,6 +648,8 @@ __global__ void __launch_bounds__(128) k_shade(const DScene* const* __restrict__
   bool ovf = false;
   for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
     const uint32_t i = q[j];
+    bool job = false;  // this path's medium NEE left a shadow job
+    uint32_t jseed = 0;
     float4 o4 = P.o[i], d4 = P.d[i], t4 = P.thr[i], e4 = P.em[i];
     int4 meta = P.meta[i];
     const int inst = meta_inst(meta.w);
@@ -618,9 +677,24 @@ __global__ void __launch_bounds__(128) k_shade(const DScene* const* __restrict__
           Ray sr = make_ray(Pt + N * S->eps, ls.d);
           float bias = ls.dist - S->eps * fabsf(dot(ls.d, N));
           sr.ft = bias * 0.99f;
-          float tr = transmittance(S, medium, sr, medium_seed(S, meta.x, meta.y, meta.z, bounce), cond, ovf);
-          v3 f = bsdf_weight(MUPSI_BSDF_LAMBERTIAN, med_albedo, ls.d, wo, N);
-          em = em + (tr * cmul(thr, cmul(f, ls.weight))) * fabsf(dot(ls.d, N));
+          const uint32_t sseed = medium_seed(S, meta.x, meta.y, meta.z, bounce);
+          const v3 f = bsdf_weight(MUPSI_BSDF_LAMBERTIAN, med_albedo, ls.d, wo, N);
+          const v3 X = cmul(thr, cmul(f, ls.weight));
+          const float c = fabsf(dot(ls.d, N));
+          if (cfg.defer && S->media[medium].kind == MUPSI_MEDIUM_GP) {
+            // the next march launch marches the shadow ray (lane groups, the same
+            // values) and adds (tr * X) * c before anything else reaches this path
+            P.sh_a[i] = make_float4(sr.o.x, sr.o.y, sr.o.z, sr.ft);
+            P.sh_b[i] = make_float4(sr.d.x, sr.d.y, sr.d.z, __int_as_float(medium));
+            P.sh_x[i] = make_float4(X.x, X.y, X.z, c);
+            P.sh_ca[i] = make_float4(cond.C.x, cond.C.y, cond.C.z, cond.u);
+            P.sh_cb[i] = make_float4(cond.g.x, cond.g.y, cond.g.z, __uint_as_float(cond.active));
+            job = true;
+            jseed = sseed;
+          } else {
+            const float tr = transmittance(S, medium, sr, sseed, cond, ovf);
+            em = em + (tr * X) * c;
+          }
         }
         v3 w;
         v3 wi = bsdf_sample(MUPSI_BSDF_LAMBERTIAN, med_albedo, wo, N, rng, w);
@@ -691,11 +765,14 @@ __global__ void __launch_bounds__(128) k_shade(const DScene* const* __restrict__
       P.meta[i] = make_int4(meta.x, meta.y, meta.z, pack_meta(bounce, inst));
       push(qa_next, ca_next, i);
       if (medium >= 0 && !S->skip_medium) push(qm_next, cm_next, i);
+      if (job) P.sh_m[i] = make_int4(0, (int)jseed, 0, 0);
     } else {
       P.rad[3 * (int64_t)i] = em.x;
       P.rad[3 * (int64_t)i + 1] = em.y;
       P.rad[3 * (int64_t)i + 2] = em.z;
+      if (job) P.sh_m[i] = make_int4(1, (int)jseed, 0, 0);
     }
+    if (job) push(P.sq[(it + 1) & 1], P.scounts + it + 1, i);
   }
   if (ovf) atomicOr(cfg.err, ERR_BVH_STACK);
 }
@@ -879,6 +956,7 @@ struct PathBuf {
   int64_t cap = 0;
   int iters = 0;
   int rounds = 1;  // surrogate rounds the round buffers were sized for
+  bool shadow = false;  // shadow-job buffers present
 };
 
 struct mupsi_scene {
@@ -1137,8 +1215,8 @@ int build_scene(const mupsi_scene_desc* desc, mupsi_scene* s) {
 // PathTracer::trace's do-while runs at least one bounce iteration
 int wave_iters(const mupsi_scene* s) { return std::max(1, s->max_bounce); }
 
-int ensure_paths(PathBuf& b, int64_t cap, int iters, int rounds) {
-  if (cap <= b.cap && iters <= b.iters && rounds <= b.rounds && b.mem) return MUPSI_OK;
+int ensure_paths(PathBuf& b, int64_t cap, int iters, int rounds, bool shadow) {
+  if (cap <= b.cap && iters <= b.iters && rounds <= b.rounds && (b.shadow || !shadow) && b.mem) return MUPSI_OK;
   if (b.mem) {
     pool_give(b.mem, b.bytes);
     b.mem = nullptr;
@@ -1146,6 +1224,7 @@ int ensure_paths(PathBuf& b, int64_t cap, int iters, int rounds) {
   cap = std::max(cap, b.cap);
   iters = std::max(iters, b.iters);
   rounds = std::max(rounds, b.rounds);
+  shadow = shadow || b.shadow;
   size_t bytes = 0;
   auto take = [&](size_t sz) {
     size_t off = bytes;
@@ -1161,6 +1240,10 @@ int ensure_paths(PathBuf& b, int64_t cap, int iters, int rounds) {
   size_t o_s0 = sr ? take(cap * 16) : 0, o_s1 = sr ? take(cap * 16) : 0, o_rq0 = sr ? take(cap * 16) : 0,
          o_rq1 = sr ? take(cap * 16) : 0, o_pr0 = sr ? take(cap * 4) : 0, o_pr1 = sr ? take(cap * 4) : 0,
          o_rc = sr ? take((size_t)iters * rounds * 4) : 0, o_rr = sr ? take((size_t)iters * rounds * 4) : 0;
+  size_t o_sa = shadow ? take(cap * 16) : 0, o_sb = shadow ? take(cap * 16) : 0, o_sx = shadow ? take(cap * 16) : 0,
+         o_sca = shadow ? take(cap * 16) : 0, o_scb = shadow ? take(cap * 16) : 0, o_sm = shadow ? take(cap * 16) : 0,
+         o_sq0 = shadow ? take(cap * 4) : 0, o_sq1 = shadow ? take(cap * 4) : 0,
+         o_sc = shadow ? take((size_t)(iters + 1) * 4) : 0, o_scu = shadow ? take((size_t)(iters + 1) * 4) : 0;
   size_t got = 0;
   char* base = static_cast<char*>(pool_take(bytes, &got));
   if (!base) {
@@ -1197,13 +1280,25 @@ int ensure_paths(PathBuf& b, int64_t cap, int iters, int rounds) {
   P.pred[1] = sr ? (float*)(base + o_pr1) : nullptr;
   P.rcounts = sr ? (uint32_t*)(base + o_rc) : nullptr;
   P.rcursors = sr ? (uint32_t*)(base + o_rr) : nullptr;
+  P.sh_a = shadow ? (float4*)(base + o_sa) : nullptr;
+  P.sh_b = shadow ? (float4*)(base + o_sb) : nullptr;
+  P.sh_x = shadow ? (float4*)(base + o_sx) : nullptr;
+  P.sh_ca = shadow ? (float4*)(base + o_sca) : nullptr;
+  P.sh_cb = shadow ? (float4*)(base + o_scb) : nullptr;
+  P.sh_m = shadow ? (int4*)(base + o_sm) : nullptr;
+  P.sq[0] = shadow ? (uint32_t*)(base + o_sq0) : nullptr;
+  P.sq[1] = shadow ? (uint32_t*)(base + o_sq1) : nullptr;
+  P.scounts = shadow ? (uint32_t*)(base + o_sc) : nullptr;
+  P.scursors = shadow ? (uint32_t*)(base + o_scu) : nullptr;
+  b.shadow = shadow;
   b.cap = cap;
   b.iters = iters;
   b.rounds = rounds;
   return MUPSI_OK;
 }
+bool needs_shadow_jobs(const DScene& h);
 int ensure_paths(mupsi_scene* s, int64_t cap) {
-  return ensure_paths(s->pb, cap, wave_iters(s) + 1, s->surr_mlp ? s->surr_rounds : 1);
+  return ensure_paths(s->pb, cap, wave_iters(s) + 1, s->surr_mlp ? s->surr_rounds : 1, needs_shadow_jobs(s->h));
 }
 
 // Launch shapes of the wave kernels (mupsi_gpu_set_tuning; chosen by the
@@ -1246,6 +1341,14 @@ struct WaveExec {
 
 // The march of bounce iteration `it`: round 0, then, with a surrogate, the
 // inference of the round's requests and the round that resumes them.
+// The shadow jobs the shading of iteration it - 1 left (marched before the
+// shading of iteration it reads the emission they add to).
+void launch_shadow_pass(const WaveExec& w, const MarchLaunch& ml, int it, cudaStream_t st) {
+  WaveCfg c = w.cfg;
+  c.shadow_pass = 1;
+  ml.fn<<<ml.blocks, ml.block, 0, st>>>(w.scenes, w.P, it, 0, c);
+}
+
 void launch_march_rounds(const WaveExec& w, const MarchLaunch& ml, int it, cudaStream_t st) {
   if (w.field) k_march_field<<<num_sms() * 16, 128, 0, st>>>(w.scenes, w.P, it, w.cfg);
   const int R = w.P.rounds;
@@ -1255,6 +1358,7 @@ void launch_march_rounds(const WaveExec& w, const MarchLaunch& ml, int it, cudaS
       mlp_infer_device(w.mlp, w.P.cap, reinterpret_cast<const float*>(w.P.req[r & 1]), 4, w.P.rcounts + it * R + r,
                        w.P.pred[r & 1], st);
   }
+  if (w.cfg.defer && it > 0) launch_shadow_pass(w, ml, it, st);
 }
 
 // Launch one wave: clear the queue counters, generate the paths, then `iters`
@@ -1285,8 +1389,30 @@ void launch_wave(const WaveExec& w, const WaveSrc& src, cudaStream_t st, mupsi_s
       k_shade<<<sb, sblock, 0, st>>>(w.scenes, w.P, it, w.cfg);
     }
   }
+  if (w.cfg.defer) {  // the last shading's shadow jobs
+    if (prof && prof->profile) {
+      cudaEvent_t a = prof->next_event(), b = prof->next_event();
+      cudaEventRecord(a, st);
+      launch_shadow_pass(w, ml, w.iters, st);
+      cudaEventRecord(b, st);
+      prof->ev_march.push_back({a, b});
+    } else {
+      launch_shadow_pass(w, ml, w.iters, st);
+    }
+  }
 }
-int wave_launches(int iters, int rounds = 1, bool field = false) { return 2 + (2 * rounds + (field ? 1 : 0)) * iters; }
+int wave_launches(int iters, int rounds = 1, bool field = false, bool defer = false) {
+  return 2 + (2 * rounds + (field ? 1 : 0) + (defer ? 1 : 0)) * iters;
+}
+
+// Scenes whose medium events sample lights through a GP medium: their shadow
+// rays are marched by the march kernel (Paths::sh_*).
+bool needs_shadow_jobs(const DScene& h) {
+  if (h.nlights == 0) return false;
+  for (int i = 0; i < h.nmed; ++i)
+    if (h.media[i].kind == MUPSI_MEDIUM_GP) return true;
+  return false;
+}
 
 WaveExec scene_exec(mupsi_scene* s) {
   WaveExec w;
@@ -1295,6 +1421,8 @@ WaveExec scene_exec(mupsi_scene* s) {
   w.iters = wave_iters(s);
   w.sphere_only = s->h.sphere_only != 0;
   w.field = s->h.field != 0;
+  w.cfg.defer = w.P.sh_a != nullptr && needs_shadow_jobs(s->h);
+  w.cfg.shadow_pass = 0;
   w.cfg.min_group = g_tuning.min_group;
   w.cfg.block_rays = g_tuning.block_rays;
   w.cfg.err = s->err;
@@ -1322,7 +1450,7 @@ int run_wave(mupsi_scene* s, int64_t n, int pass0, const int32_t* xs, const int3
     src.nchunks = 1;
   }
   launch_wave(w, src, st, s);
-  count_launch(wave_launches(w.iters, w.P.rounds, w.field));
+  count_launch(wave_launches(w.iters, w.P.rounds, w.field, w.cfg.defer != 0));
   MUPSI_CUDA(cudaGetLastError());
   return MUPSI_OK;
 }
@@ -1441,6 +1569,10 @@ Paths noalloc_paths(void* base_ptr) {
   P.req[0] = P.req[1] = nullptr;
   P.pred[0] = P.pred[1] = nullptr;
   P.rcounts = P.rcursors = nullptr;
+  P.sh_a = P.sh_b = P.sh_x = P.sh_ca = P.sh_cb = nullptr;  // shadow rays marched inline
+  P.sh_m = nullptr;
+  P.sq[0] = P.sq[1] = nullptr;
+  P.scounts = P.scursors = nullptr;
   return P;
 }
 
@@ -1474,6 +1606,7 @@ struct mupsi_batch {
   PathBuf pb;
   bool sphere_only = true;     // k_march variant for every instance
   bool field = false;          // some instance has a field medium
+  bool shadow = false;         // some instance leaves shadow jobs
   cudaStream_t bs = nullptr;  // graphs are captured and replayed on this stream
   std::vector<BatchGraph> graphs;
   mupsi_tuning graph_tuning{};  // launch shapes the graphs were captured with
@@ -1518,6 +1651,8 @@ void batch_wave_launches(mupsi_batch* b, int iters) {
   w.iters = iters;
   w.sphere_only = b->sphere_only;
   w.field = b->field;
+  w.cfg.defer = b->shadow && w.P.sh_a != nullptr;
+  w.cfg.shadow_pass = 0;
   w.cfg.min_group = g_tuning.min_group;
   w.cfg.block_rays = g_tuning.block_rays;
   w.cfg.err = b->err;
@@ -1538,14 +1673,16 @@ bool same_tuning(const mupsi_tuning& a, const mupsi_tuning& c) {
 // The graph of a wave with `iters` bounce iterations, captured on first use.
 // The instances' medium flags as they are now; graphs captured under others go.
 void batch_flags(mupsi_batch* b) {
-  bool so = true, fd = false;
+  bool so = true, fd = false, sh = false;
   for (mupsi_scene* s : b->inst) {
     so = so && s->h.sphere_only != 0;
     fd = fd || s->h.field != 0;
+    sh = sh || needs_shadow_jobs(s->h);
   }
-  if (so != b->sphere_only || fd != b->field) b->drop_graphs();
+  if (so != b->sphere_only || fd != b->field || sh != b->shadow) b->drop_graphs();
   b->sphere_only = so;
   b->field = fd;
+  b->shadow = sh;
 }
 
 int batch_graph(mupsi_batch* b, int iters, cudaGraphExec_t* out) {
@@ -1825,6 +1962,7 @@ int mupsi_gpu_trace_samples_noalloc(mupsi_scene* scene, int64_t n, const int32_t
   cudaStream_t st = (cudaStream_t)stream;  // NULL: the default stream (no stream is created here)
   WaveExec w = scene_exec(scene);
   w.P = noalloc_paths(scratch);  // launch_wave clears its queue counters and cursors
+  w.cfg.defer = 0;               // no shadow-job buffers here: shadow rays are marched inline
   WaveSrc src;
   src.n = n;
   src.xs = x;
@@ -2014,7 +2152,7 @@ int mupsi_gpu_batch_render(mupsi_batch* b, const mupsi_batch_args* a) {
   bool moved = false;
   if (!waves.empty()) {
     if (max_n > b->pb.cap || max_it + 1 > b->pb.iters) moved = true;
-    if (int e = ensure_paths(b->pb, max_n, max_it + 1, 1)) return e;
+    if (int e = ensure_paths(b->pb, max_n, max_it + 1, 1, b->shadow)) return e;
     if (int e = grow_device(b->d_chunks, b->chunk_cap, chunks.size(), moved)) return e;
     if (int e = grow_device(b->d_waves, b->wave_cap, waves.size(), moved)) return e;
   }
@@ -2061,7 +2199,7 @@ int mupsi_gpu_batch_render(mupsi_batch* b, const mupsi_batch_args* a) {
     } else {
       batch_wave_launches(b, iters);
     }
-    count_launch(wave_launches(iters, 1, b->field) + 1);
+    count_launch(wave_launches(iters, 1, b->field, b->shadow) + 1);
     b->info.waves++;
     b->info.max_iters = std::max(b->info.max_iters, iters);
     b->info.paths += waves[w].n;
