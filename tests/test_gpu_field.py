@@ -49,17 +49,20 @@ def test_field_trace(gpu, golden, kind):
 
 
 def test_field_batch_and_noalloc(gpu):
-    """A batch mixing field and GP scenes renders each as alone; the
-    allocation-free trace runs the field march too."""
+    """A batch mixing field and GP scenes (one with a light, whose shadow rays
+    through the GP medium are marched by the shadow passes) renders each as
+    alone; the allocation-free trace runs the field march too."""
     import torch
-    scenes = [S.field_scene("sdf_mesh", 32, 32, 3), S.config0_scene(32, 32, 3), S.field_scene("external_gp", 32, 32, 3)]
+    tex = np.random.default_rng(2).uniform(0.1, 0.9, (8, 8, 3)).astype(np.float32)
+    scenes = [S.field_scene("sdf_mesh", 32, 32, 3), S.config0_scene(32, 32, 3), S.field_scene("external_gp", 32, 32, 3),
+              S.textured_floor_scene(tex, True, 32, 32, 3)]
     alone = []
     for sc in scenes:
         r = GpuRenderer()
         r.prepare_render(GpuScene(sc))
         alone.append(r.start_render_progressive(3))
     for graphs in (True, False):
-        imgs, _ = GpuBatch(scenes).render([3, 3, 3], use_graphs=graphs)
+        imgs, _ = GpuBatch(scenes).render([3, 3, 3, 3], use_graphs=graphs)
         for a, b in zip(imgs, alone):
             assert np.array_equal(bits(a), bits(b))
     gs = GpuScene(S.field_scene("external_gp", 32, 32, 2))
