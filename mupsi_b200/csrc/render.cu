@@ -94,6 +94,23 @@ MD void store_cond(const Paths& P, uint32_t i, const Cond& c) {
   P.cb[i] = make_float4(c.g.x, c.g.y, c.g.z, __uint_as_float(c.active));
 }
 
+// The NEE term of shadow job `idx` with transmittance tr, added where the path
+// stands: its final radiance if it ended at the event, else its emission.
+MD void add_shadow_term(const Paths& P, uint32_t idx, float tr) {
+  const float4 x = P.sh_x[idx];
+  const float tx = (tr * x.x) * x.w, ty = (tr * x.y) * x.w, tz = (tr * x.z) * x.w;
+  if (P.sh_m[idx].x) {
+    float* r = P.rad + 3 * (int64_t)idx;
+    r[0] = r[0] + tx;
+    r[1] = r[1] + ty;
+    r[2] = r[2] + tz;
+  } else {
+    const float4 e = P.em[idx];
+    P.em[idx] = make_float4(e.x + tx, e.y + ty, e.z + tz, e.w);
+  }
+}
+
+
 // ConstantSampler seed of bounce b's medium sampler (trace.cpp:146-147)
 MD uint32_t medium_seed(const DScene* S, int x, int y, int k, int b) {
   uint32_t s = S->gp_mode == MUPSI_GP_SINGLE_REALIZATION
@@ -470,7 +487,9 @@ __global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? 6 : 3) k_march(c
           int4 meta = P.meta[idx];
           int med = __float_as_int(d.w);
           S = scenes[meta_inst(meta.w)];
-          if (shadow) {  // the shadow ray of the job (its own medium, seed and conditioning)
+          if (shadow && S->media[__float_as_int(P.sh_b[idx].w)].kind != MUPSI_MEDIUM_GP) {
+            skipped = true;  // a field medium's job: k_march_field's shadow pass
+          } else if (shadow) {  // the shadow ray of the job (its own medium, seed and conditioning)
             const float4 a = P.sh_a[idx], b = P.sh_b[idx], ca = P.sh_ca[idx], cb = P.sh_cb[idx];
             med = __float_as_int(b.w);
             Cond c;
@@ -483,7 +502,7 @@ __global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? 6 : 3) k_march(c
             if (grp.sub == 0) marches++;
             active = true;
           }
-          skipped = !shadow && !resume && S->media[med].kind != MUPSI_MEDIUM_GP;  // k_march_field marches it
+          if (!shadow) skipped = !resume && S->media[med].kind != MUPSI_MEDIUM_GP;  // k_march_field marches it
           if (!skipped && !shadow) {
             march_begin(S, m, mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), o.w, 3.402823466e+38f, med,
                         medium_seed(S, meta.x, meta.y, meta.z, meta_bounce(meta.w)), load_cond(P, idx));
@@ -532,18 +551,7 @@ __global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? 6 : 3) k_march(c
         active = false;
       } else if (m.status != 0 && shadow) {
         if (grp.sub == 0) {  // transmittance 0 at a sign change: the NEE term (tr * X) * c
-          const float tr = m.status == 1 ? 0.0f : 1.0f;
-          const float4 x = P.sh_x[idx];
-          const float tx = (tr * x.x) * x.w, ty = (tr * x.y) * x.w, tz = (tr * x.z) * x.w;
-          if (P.sh_m[idx].x) {  // the path ended at that event: its radiance is written
-            float* r = P.rad + 3 * (int64_t)idx;
-            r[0] = r[0] + tx;
-            r[1] = r[1] + ty;
-            r[2] = r[2] + tz;
-          } else {
-            const float4 e = P.em[idx];
-            P.em[idx] = make_float4(e.x + tx, e.y + ty, e.z + tz, e.w);
-          }
+          add_shadow_term(P, idx, m.status == 1 ? 0.0f : 1.0f);
           steps += m.n_steps;
           psis += m.n_psi;
           imps += (unsigned long long)m.n_psi * 27ull * (unsigned long long)S->media[m.medium].k.ppc;
@@ -597,9 +605,25 @@ __global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? 6 : 3) k_march(c
 // sphere tracing bounded by the reference's iteration limits (512 / 1024).
 __global__ void __launch_bounds__(128) k_march_field(const DScene* const* __restrict__ scenes, Paths P, int it,
                                                      WaveCfg cfg) {
+  bool ovf = false;
+  if (cfg.shadow_pass) {  // the shadow jobs of field media (SDFMedium / ExternalGPMedium::transmittance)
+    const uint32_t n = P.scounts[it];
+    const uint32_t* q = P.sq[it & 1];
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+      const uint32_t idx = q[j];
+      const float4 a = P.sh_a[idx], b = P.sh_b[idx];
+      const DScene* S = scenes[meta_inst(P.meta[idx].w)];
+      const DMedium& md = S->media[__float_as_int(b.w)];
+      if (md.kind == MUPSI_MEDIUM_GP) continue;  // the march kernel's shadow pass
+      const float tr = field_transmittance(S, md, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), 0.0f, a.w,
+                                           (uint32_t)P.sh_m[idx].y, ovf);
+      add_shadow_term(P, idx, tr);
+    }
+    if (ovf) atomicOr(cfg.err, ERR_BVH_STACK);
+    return;
+  }
   const uint32_t n = P.counts[2 * it];
   const uint32_t* q = P.q[it & 1];
-  bool ovf = false;
   for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
     const uint32_t idx = q[j];
     const float4 d = P.d[idx];
@@ -681,7 +705,7 @@ __global__ void __launch_bounds__(128) k_shade(const DScene* const* __restrict__
           const v3 f = bsdf_weight(MUPSI_BSDF_LAMBERTIAN, med_albedo, ls.d, wo, N);
           const v3 X = cmul(thr, cmul(f, ls.weight));
           const float c = fabsf(dot(ls.d, N));
-          if (cfg.defer && S->media[medium].kind == MUPSI_MEDIUM_GP) {
+          if (cfg.defer) {
             // the next march launch marches the shadow ray (lane groups, the same
             // values) and adds (tr * X) * c before anything else reaches this path
             P.sh_a[i] = make_float4(sr.o.x, sr.o.y, sr.o.z, sr.ft);
@@ -1346,6 +1370,7 @@ struct WaveExec {
 void launch_shadow_pass(const WaveExec& w, const MarchLaunch& ml, int it, cudaStream_t st) {
   WaveCfg c = w.cfg;
   c.shadow_pass = 1;
+  if (w.field) k_march_field<<<num_sms() * 16, 128, 0, st>>>(w.scenes, w.P, it, c);
   ml.fn<<<ml.blocks, ml.block, 0, st>>>(w.scenes, w.P, it, 0, c);
 }
 
@@ -1402,17 +1427,12 @@ void launch_wave(const WaveExec& w, const WaveSrc& src, cudaStream_t st, mupsi_s
   }
 }
 int wave_launches(int iters, int rounds = 1, bool field = false, bool defer = false) {
-  return 2 + (2 * rounds + (field ? 1 : 0) + (defer ? 1 : 0)) * iters;
+  return 2 + (2 * rounds + (field ? 1 : 0) + (defer ? (field ? 2 : 1) : 0)) * iters;
 }
 
-// Scenes whose medium events sample lights through a GP medium: their shadow
-// rays are marched by the march kernel (Paths::sh_*).
-bool needs_shadow_jobs(const DScene& h) {
-  if (h.nlights == 0) return false;
-  for (int i = 0; i < h.nmed; ++i)
-    if (h.media[i].kind == MUPSI_MEDIUM_GP) return true;
-  return false;
-}
+// Scenes whose medium events sample lights: their shadow rays are marched by
+// the shadow passes (Paths::sh_*).
+bool needs_shadow_jobs(const DScene& h) { return h.nlights > 0 && h.nmed > 0; }
 
 WaveExec scene_exec(mupsi_scene* s) {
   WaveExec w;

@@ -117,15 +117,20 @@ def test_scene_occlusion_from_root(gpu):
     assert (root_mode.sum(axis=1) < ref_mode.sum(axis=1) - 1e-3).sum() > 10
 
 
-def test_deferred_shadow_rays_match_inline(gpu):
-    """A medium event's shadow ray (GPMedium::transmittance) is marched by the
-    march kernel's shadow pass of the next bounce iteration, which adds the
-    NEE term before the path's next shading; the allocation-free trace has no
-    room for those jobs and marches the ray inline in the shading kernel. Both
-    must give the same bits, with the NEE terms present."""
+@pytest.mark.parametrize("kind", ["gp", "sdf_sphere", "external_gp"])
+def test_deferred_shadow_rays_match_inline(gpu, kind):
+    """A medium event's shadow ray (Medium::transmittance) is marched by a
+    shadow pass of the next bounce iteration (the march kernel's for a GP
+    medium, the field march kernel's for an SDF or external GP medium), which
+    adds the NEE term before the path's next shading; the allocation-free
+    trace has no room for those jobs and marches the ray inline in the shading
+    kernel. Both must give the same bits, with the NEE terms present."""
     import torch
-    sc = S.config0_scene(64, 64, 4)
-    sc.add_sphere((40.0, 160.0, -380.0), 45.0, emission=(6.0, 5.0, 4.0))
+    if kind == "gp":
+        sc = S.config0_scene(64, 64, 4)
+        sc.add_sphere((40.0, 160.0, -380.0), 45.0, emission=(6.0, 5.0, 4.0))
+    else:
+        sc = S.field_scene(kind, 64, 64, 4)  # with its emissive sphere
     gs = GpuScene(sc)
     xs, ys, ks = (a.ravel().astype(np.int32) for a in np.meshgrid(np.arange(64), np.arange(64), np.arange(4),
                                                                  indexing="ij"))
@@ -135,5 +140,6 @@ def test_deferred_shadow_rays_match_inline(gpu):
     torch.cuda.synchronize()
     inline = out.cpu().numpy()
     assert np.array_equal(deferred.view(np.uint32), inline.view(np.uint32))
-    dark = GpuScene(S.config0_scene(64, 64, 4)).trace(xs, ys, ks)
-    assert (np.any(deferred != dark, axis=1)).mean() > 0.05  # the light reaches the medium's surface
+    if kind == "gp":
+        dark = GpuScene(S.config0_scene(64, 64, 4)).trace(xs, ys, ks)
+        assert (np.any(deferred != dark, axis=1)).mean() > 0.05  # the light reaches the medium's surface
