@@ -434,15 +434,19 @@ __device__ void march_block_rays(const DScene* const* __restrict__ scenes, Paths
 // marched by a group of G lanes that share its psi sums: G = 4 while the queue
 // fills the resident threads, larger (up to 32) as the queue shrinks, so the
 // late bounces' few long marches finish up to 8x sooner than on one lane.
-template <int MK>
-__global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? 6 : 3) k_march(const DScene* const* __restrict__ scenes, Paths P, int it, int round,
+// SH: the shadow-pass instantiation (the medium march carries none of its code).
+// The general (mesh-mean) march is bound by the latency of its BVH traversals
+// and runs best with every thread resident (16 blocks per SM, 32 registers,
+// the rest spilled to L1): 483 -> 331 ms for a level-6 mesh render at 512^2 x 4.
+template <int MK, bool SH>
+__global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? 6 : 16) k_march(const DScene* const* __restrict__ scenes, Paths P, int it, int round,
                                                WaveCfg cfg) {
   // round 0 marches the iteration's medium queue; round r >= 1 resumes the
   // marches suspended in round r - 1 with their surrogate predictions
   // (a scene with sphere means only has no surrogate: one round, no resumes)
   // a shadow pass marches the shadow jobs the shading of iteration it - 1 left
   // (GPMedium::transmittance, gpmedium.cpp:105-129) instead of the medium queue
-  const bool shadow = cfg.shadow_pass != 0;
+  constexpr bool shadow = SH;
   const bool resume = MK != MEAN_SPHERE_ONLY && round > 0 && !shadow;
   const int R = P.rounds;
   const uint32_t n = shadow ? P.scounts[it] : resume ? P.rcounts[it * R + round - 1] : P.counts[2 * it];
@@ -1332,7 +1336,9 @@ mupsi_tuning g_tuning = {128, 4, 128, 0, 8};
 // Persistent march grid: resident blocks per SM x SMs.
 struct MarchLaunch {
   void (*fn)(const DScene* const*, Paths, int, int, WaveCfg);
+  void (*fn_shadow)(const DScene* const*, Paths, int, int, WaveCfg);
   int blocks, block;
+  int blocks_shadow;
 };
 MarchLaunch march_launch(bool sphere_only) {
   static std::mutex mu;
@@ -1343,11 +1349,15 @@ MarchLaunch march_launch(bool sphere_only) {
   for (auto& e : memo)
     if (e.first == key) return e.second;
   MarchLaunch m;
-  m.fn = sphere_only ? k_march<MEAN_SPHERE_ONLY> : k_march<MEAN_ANY>;
+  m.fn = sphere_only ? k_march<MEAN_SPHERE_ONLY, false> : k_march<MEAN_ANY, false>;
+  m.fn_shadow = sphere_only ? k_march<MEAN_SPHERE_ONLY, true> : k_march<MEAN_ANY, true>;
   m.block = block;
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, m.fn, block, 0);
   m.blocks = std::max(1, per_sm) * num_sms();
+  per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, m.fn_shadow, block, 0);
+  m.blocks_shadow = std::max(1, per_sm) * num_sms();
   memo.push_back({key, m});
   return m;
 }
@@ -1371,7 +1381,7 @@ void launch_shadow_pass(const WaveExec& w, const MarchLaunch& ml, int it, cudaSt
   WaveCfg c = w.cfg;
   c.shadow_pass = 1;
   if (w.field) k_march_field<<<num_sms() * 16, 128, 0, st>>>(w.scenes, w.P, it, c);
-  ml.fn<<<ml.blocks, ml.block, 0, st>>>(w.scenes, w.P, it, 0, c);
+  ml.fn_shadow<<<ml.blocks_shadow, ml.block, 0, st>>>(w.scenes, w.P, it, 0, c);
 }
 
 void launch_march_rounds(const WaveExec& w, const MarchLaunch& ml, int it, cudaStream_t st) {
