@@ -31,7 +31,8 @@
 extern "C" {
 #endif
 
-#define MUPSI_GPU_ABI_VERSION 1
+/* 2: mupsi_tuning gained block_rays */
+#define MUPSI_GPU_ABI_VERSION 2
 
 typedef enum { MUPSI_MEM_HOST = 0, MUPSI_MEM_DEVICE = 1 } mupsi_mem;
 
@@ -161,6 +162,13 @@ typedef struct mupsi_mesh mupsi_mesh;
 const char* mupsi_gpu_last_error(void);
 /* ABI version compiled into the library (MUPSI_GPU_ABI_VERSION). */
 int32_t mupsi_gpu_abi_version(void);
+
+/* Released scenes leave their device buffers to the library for reuse (the
+ * path state of up to 4 scenes per device, and per-scene buffers up to 256 MB
+ * per device), so a host that creates a scene per frame pays no cudaMalloc /
+ * cudaFree. This hands all of them back to the driver; call it when no scene
+ * is rendering. */
+int mupsi_gpu_release_pools(void);
 /* Number of kernel launches this library has issued on this process. */
 int64_t mupsi_gpu_launch_count(void);
 

@@ -240,6 +240,12 @@ _TUNING_KEYS = ("march_block", "min_group", "shade_block", "wave_paths", "block_
 _tuning_applied = False
 
 
+def release_pools():
+    """Give the device memory kept from released scenes back to the driver
+    (mupsi_gpu_release_pools); call it when no scene is rendering."""
+    check(load().mupsi_gpu_release_pools())
+
+
 def get_tuning():
     """The launch shapes in use (mupsi_gpu_get_tuning) as a dict."""
     t = _abi.Tuning()

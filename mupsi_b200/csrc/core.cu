@@ -259,6 +259,22 @@ void dev_give(void* p) {
   cudaFree(p);
 }
 
+void dev_cache_release() {
+  std::vector<CachedBuf> all;
+  {
+    std::lock_guard<std::mutex> lock(g_buf_mu);
+    all.swap(g_buf_free);
+    g_buf_cached = 0;
+  }
+  int cur = 0;
+  cudaGetDevice(&cur);
+  for (const CachedBuf& b : all) {
+    cudaSetDevice(b.dev);
+    cudaFree(b.p);
+  }
+  cudaSetDevice(cur);
+}
+
 // ------------------------------------------------------------ meshes / BVH
 struct MeshStore {
   DMesh d;

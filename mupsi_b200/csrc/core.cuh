@@ -26,6 +26,7 @@ int make_device_mesh(const mupsi_mesh_desc& md, DMesh& d, std::vector<void*>& al
 // synchronised: no work in flight uses the buffer.
 cudaError_t dev_take(void** out, size_t bytes);
 void dev_give(void* p);
+void dev_cache_release();  // cudaFree every cached buffer
 
 // A buffer of one batch call: aliases the caller's pointer for device memory,
 // otherwise a stream-ordered device allocation with the copy in (in()) or the

@@ -1073,6 +1073,21 @@ void pool_give(void* p, size_t bytes) {
   }
 }
 
+void pool_release() {
+  std::vector<PoolEntry> all;
+  {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    all.swap(g_pool);
+  }
+  int cur = 0;
+  cudaGetDevice(&cur);
+  for (const PoolEntry& e : all) {
+    cudaSetDevice(e.dev);
+    cudaFree(e.ptr);
+  }
+  cudaSetDevice(cur);
+}
+
 }  // namespace
 
 mupsi_scene::~mupsi_scene() {
@@ -2349,6 +2364,14 @@ int mupsi_gpu_scene_set_sky_texture(mupsi_scene* scene, int32_t width, int32_t h
     scene->h.sky_h = height;
   }
   MUPSI_CUDA(cudaMemcpy(scene->d, &scene->h, sizeof(DScene), cudaMemcpyHostToDevice));
+  return MUPSI_OK;
+}
+
+int mupsi_gpu_release_pools(void) {
+  clear_error();
+  MUPSI_CUDA(cudaDeviceSynchronize());
+  pool_release();
+  dev_cache_release();
   return MUPSI_OK;
 }
 

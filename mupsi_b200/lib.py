@@ -68,6 +68,7 @@ def _setup(L):
     L.mupsi_gpu_scene_set_external_gp_medium.argtypes = [vp, i32, i32, vp, vp, vp, vp, C.c_float]
     L.mupsi_gpu_transmittance.argtypes = [vp, i32, i64, vp, vp, vp, vp, C.c_int, vp]
     L.mupsi_gpu_scene_get_size.argtypes = [vp, C.POINTER(i32), C.POINTER(i32)]
+    L.mupsi_gpu_release_pools.argtypes = []
     L.mupsi_obj_load.argtypes = [C.c_char_p, C.POINTER(_abi.Obj)]
     L.mupsi_obj_free.argtypes = [C.POINTER(_abi.Obj)]
     L.mupsi_obj_free.restype = None
@@ -99,7 +100,7 @@ def load():
         if not os.path.exists(LIB_PATH):
             raise FileNotFoundError(f"{LIB_PATH} is missing: build it with `python -m mupsi_b200.build`")
         _lib = _setup(C.CDLL(LIB_PATH))
-        if _lib.mupsi_gpu_abi_version() != 1:
+        if _lib.mupsi_gpu_abi_version() != 2:
             raise RuntimeError("libmupsi_gpu.so ABI version mismatch")
     return _lib
 

@@ -144,3 +144,19 @@ def test_render_cancel_and_callback(gpu):
     assert seen and seen[-1] == 8
     r.cancel()
     assert r.start_render_progressive(8) is None
+
+
+def test_release_pools_between_renders(gpu):
+    """Scenes released and their cached buffers handed back to the driver: a
+    scene created afterwards renders the same image."""
+    from mupsi_b200.api import release_pools
+    sc = S.config0_scene(32, 32, 2)
+    imgs = []
+    for _ in range(2):
+        gs = GpuScene(sc)
+        r = GpuRenderer()
+        r.prepare_render(gs)
+        imgs.append(r.start_render_progressive(2))
+        gs.close()
+        release_pools()
+    assert np.array_equal(bits(imgs[0]), bits(imgs[1]))
