@@ -272,6 +272,9 @@ __device__ __forceinline__ int nth_need(const unsigned* need, int nw, int stop, 
   return 0;  // not reached: r < the count of such steps
 }
 
+// SH: the rays are shadow jobs (GPMedium::transmittance: the result is the
+// NEE term added where the path stands).
+template <bool SH>
 __device__ void march_block_rays(const DScene* const* __restrict__ scenes, Paths& P, uint32_t n,
                                  const uint32_t* __restrict__ q, uint32_t* cursor, const WaveCfg& cfg) {
   constexpr int kMaxWarps = 4, kWindow = 32 * kMaxWarps;
@@ -302,15 +305,27 @@ __device__ void march_block_rays(const DScene* const* __restrict__ scenes, Paths
     const uint32_t j = s_j;
     if (j >= n) break;
     const uint32_t idx = q[j];
-    const float4 o = P.o[idx], d = P.d[idx];
     const int4 meta = P.meta[idx];
-    const int med = __float_as_int(d.w);
     const DScene* S = scenes[meta_inst(meta.w)];
-    const DMedium& md = S->media[med];
-    if (md.kind != MUPSI_MEDIUM_GP) continue;  // k_march_field marches it
     March m;
-    march_begin(S, m, mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), o.w, 3.402823466e+38f, med,
-                medium_seed(S, meta.x, meta.y, meta.z, meta_bounce(meta.w)), load_cond(P, idx));
+    if constexpr (SH) {  // the job's shadow ray, medium, seed and conditioning
+      const float4 a = P.sh_a[idx], b = P.sh_b[idx], ca = P.sh_ca[idx], cb = P.sh_cb[idx];
+      const int med = __float_as_int(b.w);
+      if (S->media[med].kind != MUPSI_MEDIUM_GP) continue;  // k_march_field's shadow pass
+      Cond c;
+      c.C = mk3(ca.x, ca.y, ca.z);
+      c.u = ca.w;
+      c.g = mk3(cb.x, cb.y, cb.z);
+      c.active = __float_as_uint(cb.w);
+      march_begin(S, m, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), 0.0f, a.w, med, (uint32_t)P.sh_m[idx].y, c);
+    } else {
+      const float4 o = P.o[idx], d = P.d[idx];
+      const int med = __float_as_int(d.w);
+      if (S->media[med].kind != MUPSI_MEDIUM_GP) continue;  // k_march_field marches it
+      march_begin(S, m, mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), o.w, 3.402823466e+38f, med,
+                  medium_seed(S, meta.x, meta.y, meta.z, meta_bounce(meta.w)), load_cond(P, idx));
+    }
+    const DMedium& md = S->media[m.medium];
     m.may_request = false;
     marches++;
     {  // the origin (every warp alike)
@@ -329,11 +344,29 @@ __device__ void march_block_rays(const DScene* const* __restrict__ scenes, Paths
       // the next W steps (table marches), one per thread: 0 sign settled and
       // kept, 1 needs psi, 2 sign settled and changed (hit), 3 past the end
       int stop = W, total = 0, take = 0;
-      if (m.use_tab) {
+      {
         const int i = (int)threadIdx.x, kk = k0 + 1 + i;
         int cls = 3;
-        if (i < W && kk < S->tab_steps) {
-          const float tw = __ldg(S->tab + kk);
+        // step k0 + 1 + i: from the table, or by the i + 1 sequential adds the
+        // one-group march performs (a step that does not advance t ends the
+        // march with ERR_MARCH_GUARD, as march_advance does)
+        float tw = 0.0f;
+        bool valid = false;
+        if (m.use_tab) {
+          valid = i < W && kk < S->tab_steps;
+          if (valid) tw = __ldg(S->tab + kk);
+        } else if (i < W) {
+          tw = m.t;
+          bool stuck = false;
+          for (int s = 0; s <= i; ++s) {
+            const float tn = tw + m.dt;
+            stuck = stuck || tn == tw;
+            tw = tn;
+          }
+          valid = !stuck && tw < m.ft;
+          if (stuck) cls = 4;
+        }
+        if (valid) {
           const v3 pw = m.o + m.d * tw;
           const float mw = mean_value<MEAN_SPHERE_ONLY>(S, md, pw, ovf);
           const float lb = fabsf(mw);
@@ -341,11 +374,11 @@ __device__ void march_block_rays(const DScene* const* __restrict__ scenes, Paths
             cls = ((mw > 0.0f) != m.fprev_pos) ? 2 : 0;
           else
             cls = 1;
-          s_tw[i] = tw;
           s_mw[i] = mw;
         }
+        if (i < W) s_tw[i] = tw;
         const unsigned need = __ballot_sync(0xffffffffu, cls == 1), end = __ballot_sync(0xffffffffu, cls >= 2);
-        if (i < W && cls >= 2) s_cls[i] = cls;
+        if (i < W && cls >= 2) s_cls[i] = cls;  // 2 hit, 3 past the end, 4 t stopped advancing
         if (lane == 0 && warp < kMaxWarps) {
           s_need[warp] = need;
           s_end[warp] = end;
@@ -388,30 +421,41 @@ __device__ void march_block_rays(const DScene* const* __restrict__ scenes, Paths
         m.k = k0 + 1 + pos;
         m.t = s_tw[pos];
         m.status = 1;
-      } else if (!m.use_tab) {
-        march_advance(S, m, -INFINITY);  // one step on, as after a psi step without a hit
       } else if (take < total) {  // more psi steps in the window than candidates: resume after the last one
-        m.k = k0 + 2 + nth_need(s_need, nw, stop, take - 1);
-        m.t = __ldg(S->tab + m.k);
+        const int pos = nth_need(s_need, nw, stop, take - 1) + 1;  // < stop <= W
+        m.k = k0 + 1 + pos;
+        m.t = m.use_tab ? __ldg(S->tab + m.k) : s_tw[pos];
       } else if (stop < W) {  // the window's first settled change of sign, or the end
         m.k = k0 + 1 + stop;
         if (s_cls[stop] == 2) {
           m.t = s_tw[stop];
           m.status = 1;
         } else {
-          m.t = __ldg(S->tab + m.k);
+          m.t = m.use_tab ? __ldg(S->tab + m.k) : s_tw[stop];
+          if (s_cls[stop] == 4 && threadIdx.x == 0) atomicOr(S->err, ERR_MARCH_GUARD);
           m.status = 2;
         }
-      } else {
+      } else {  // every window step keeps its sign: on after the window
         m.k = k0 + 1 + W;
-        m.t = __ldg(S->tab + m.k);
+        if (m.use_tab) {
+          m.t = __ldg(S->tab + m.k);
+        } else {
+          const float tn = s_tw[W - 1] + m.dt;
+          if (tn == s_tw[W - 1]) {
+            if (threadIdx.x == 0) atomicOr(S->err, ERR_MARCH_GUARD);
+            m.status = 2;
+          }
+          m.t = tn;
+        }
       }
       m.n_steps += (uint32_t)min(stop, W);
       psis += (unsigned long long)nc;
       imps += (unsigned long long)nc * 27ull * (unsigned long long)md.k.ppc;
       __syncthreads();  // the shared candidate state is written again next round
     }
-    if (warp == 0) {
+    if constexpr (SH) {
+      if (threadIdx.x == 0) add_shadow_term(P, idx, m.status == 1 ? 0.0f : 1.0f);
+    } else if (warp == 0) {
       mupsi_medium_sample r;
       march_result<MEAN_SPHERE_ONLY, true>(S, m, r, ovf, full);
       if (lane == 0) {
@@ -454,8 +498,8 @@ __global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? 6 : 16) k_march(
   uint32_t* cursor = shadow ? P.scursors + it : resume ? P.rcursors + it * R + round : P.cursors + it;
   const bool can_suspend = round + 1 < R && !shadow;
   if constexpr (MK == MEAN_SPHERE_ONLY) {
-    if (!shadow && (uint64_t)n <= (uint64_t)gridDim.x * (uint64_t)cfg.block_rays) {
-      march_block_rays(scenes, P, n, q, cursor, cfg);
+    if ((uint64_t)n <= (uint64_t)gridDim.x * (uint64_t)cfg.block_rays) {
+      march_block_rays<SH>(scenes, P, n, q, cursor, cfg);
       return;
     }
   }
