@@ -97,7 +97,7 @@ MHD uint32_t pcg_next(uint64_t& state) {
 // (i >> 9) | 0x3F800000 as a float, minus 1: uniform in [0, 1)
 MHD float u01(uint32_t i) {
 #ifdef __CUDA_ARCH__
-  return __uint_as_float((i >> 9u) | 0x3F800000u) - 1.0f;
+  return __uint_as_float((i >> 9u) + 0x3F800000u) - 1.0f;
 #else
   union {
     uint32_t u;

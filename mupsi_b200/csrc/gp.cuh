@@ -7,8 +7,8 @@
 // the PCG stream started at cell_seed + 1 (32-bit wrap), the impulse positions
 // s = cell*kr + U^3*kr and the +-1 weights, and the accumulation order
 // (dx, dy, dz, i). The Gaussian h uses the SFU exp2 (ex2.approx) on the
-// argument |p-s|^2 * (-log2(e)/L2); the reference calls glibc expf on
-// -|p-s|^2 / L2. The resulting psi differs from the reference by ~1e-7 of the
+// argument |p-s|^2 * (-log2(e)/L2), |p-s|^2 formed with fused multiply-adds;
+// the reference calls glibc expf on -|p-s|^2 / L2. The resulting psi differs from the reference by ~1e-7 of the
 // sum of |terms| (tested at 1e-5).
 #pragma once
 #include <climits>
@@ -50,23 +50,36 @@ MD void cell_of(const KParams& k, v3 p, int& cx, int& cy, int& cz) {
   }
 }
 
-// Impulses of one cell, visited in the reference's order. F(s, w) is called per
-// impulse with its position and sign (+1 / -1).
+// Impulses of one cell, visited in the reference's order. F(s, wsign) is called
+// per impulse with its position and the sign bit of its weight (0 for +1,
+// 0x80000000 for -1).
+template <typename F>
+MD void cell_impulse(const KParams& k, uint64_t& st, float bx, float by, float bz, F&& f) {
+  // Vector3f(next1D(), next1D(), next1D()) as the reference's build evaluates it:
+  // constructor arguments right to left, so the first draw is z.
+  float a = pcg_next1d(st);
+  float b = pcg_next1d(st);
+  float c = pcg_next1d(st);
+  v3 s = v3{bx + c * k.kr, by + b * k.kr, bz + a * k.kr};
+  // weight next1D() < 0.5 ? -1 : +1; next1D() = float((i >> 9) | 0x3F800000) - 1
+  // is below 0.5 exactly when bit 31 of i is clear
+  const uint32_t wsign = ~pcg_next(st) & 0x80000000u;
+  f(s, wsign);
+}
 template <typename F>
 MD void for_each_impulse(const KParams& k, int nx, int ny, int nz, uint32_t seed, F&& f) {
   uint32_t cs = make_seed4((uint32_t)nx, (uint32_t)ny, (uint32_t)nz, seed);
   uint64_t st = (uint64_t)(uint32_t)(cs + 1u);
   const float bx = (float)nx * k.kr, by = (float)ny * k.kr, bz = (float)nz * k.kr;
-  for (int i = 0; i < k.ppc; ++i) {
-    // Vector3f(next1D(), next1D(), next1D()) as the reference's build evaluates it:
-    // constructor arguments right to left, so the first draw is z.
-    float a = pcg_next1d(st);
-    float b = pcg_next1d(st);
-    float c = pcg_next1d(st);
-    v3 s = v3{bx + c * k.kr, by + b * k.kr, bz + a * k.kr};
-    float w = pcg_next1d(st) < 0.5f ? -1.0f : 1.0f;
-    f(s, w);
+  // the common count, unrolled (configuration-0 render 6.92 -> 6.71 ms); unrolling
+  // the 1- and 8-impulse cells as well made that render slower (7.05 and
+  // 7.74 ms), and unrolling the general loop by 2 or 4 gained nothing
+  if (k.ppc == 3) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) cell_impulse(k, st, bx, by, bz, f);
+    return;
   }
+  for (int i = 0; i < k.ppc; ++i) cell_impulse(k, st, bx, by, bz, f);
 }
 
 // Unnormalised InternalNoise sums over neighbour cells [c0, c1) of the 27, in
@@ -79,16 +92,19 @@ MD void psi_sums_cells(const KParams& k, v3 p, int cx, int cy, int cz, uint32_t 
 #pragma unroll 1
   for (int c = c0; c < c1; ++c) {
     const int dx = c / 9 - 1, dy = (c / 3) % 3 - 1, dz = c % 3 - 1;
-    for_each_impulse(k, cx + dx, cy + dy, cz + dz, seed, [&](v3 s, float w) {
+    for_each_impulse(k, cx + dx, cy + dy, cz + dz, seed, [&](v3 s, uint32_t wsign) {
       v3 d = p - s;
-      float r2 = d.x * d.x + (d.y * d.y + d.z * d.z);
-      float h = ex2_approx(r2 * k.k2);
-      v = fmaf(w, h, v);  // w = +-1: w*h is exact, so this equals v + w*h
-      if (GRAD) {
-        float gs = h * k.c2;
-        gx = fmaf(w, gs * d.x, gx);
-        gy = fmaf(w, gs * d.y, gy);
-        gz = fmaf(w, gs * d.z, gz);
+      // |p - s|^2 with two fused multiply-adds (psi carries the exp2
+      // approximation's error already; the impulse positions stay exact)
+      float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
+      // w*h with w = +-1 and h >= 0: h with the weight's sign bit (exact)
+      const float hs = __uint_as_float(__float_as_uint(ex2_approx(r2 * k.k2)) | wsign);
+      v = v + hs;
+      if (GRAD) {  // (w*h)*c2*d = w*((h*c2)*d) bit for bit: rounding is sign-symmetric
+        float gs = hs * k.c2;
+        gx = gx + gs * d.x;
+        gy = gy + gs * d.y;
+        gz = gz + gs * d.z;
       }
     });
   }
