@@ -197,12 +197,13 @@ def _profiled_traffic():
 
 # Source-level operations per impulse evaluation of the march's psi sum (the
 # roofline unit): 4 PCG32 steps at 10 integer ops each (64-bit multiply-add as
-# three 32-bit multiply-adds plus carry, xorshift, rotate), 4 mantissa-trick
-# uniforms (shift/or + subtract), the impulse position (3 multiply + 3 add), the
-# weight compare/select, |p - s|^2 (3 sub, 3 mul, 2 add), the exponent scale
-# (1 mul), exp2 on the SFU (1), the signed accumulate (1): 40 integer + 25 float
-# = 65 issue slots, 1 of them on the SFU.
-OPS_PER_IMPULSE = 65
+# three 32-bit multiply-adds plus carry, xorshift, rotate), 3 mantissa-trick
+# uniforms for the position (shift/or, subtract: 1 integer + 1 float each), the
+# weight's sign bit put onto the Gaussian (1 three-input logic op), the impulse
+# position (3 multiply + 3 add), |p - s|^2 (3 sub, 1 mul, 2 fused multiply-add),
+# the exponent scale (1 mul), exp2 on the SFU (1), the signed accumulate (1 add):
+# 44 integer + 18 float = 62 issue slots, 1 of them on the SFU.
+OPS_PER_IMPULSE = 62
 
 
 def run_gpu(args):
