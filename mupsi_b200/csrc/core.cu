@@ -147,7 +147,8 @@ int num_sms() {
 }
 
 // ------------------------------------------------------------ GP noise batch
-template <bool GRAD>
+// PPC: the kernel's points per cell at compile time (0: read at run time)
+template <bool GRAD, int PPC>
 __global__ void __launch_bounds__(256) k_psi(KParams k, int64_t n, const float* __restrict__ p,
                                              const uint32_t* __restrict__ seed, const Cond* __restrict__ cond,
                                              float* __restrict__ out) {
@@ -155,14 +156,14 @@ __global__ void __launch_bounds__(256) k_psi(KParams k, int64_t n, const float* 
     v3 P = v3{p[3 * i], p[3 * i + 1], p[3 * i + 2]};
     uint32_t s = seed[i];
     if (GRAD) {
-      float4 f = raw_noise(k, P, s);
+      float4 f = raw_noise<PPC>(k, P, s);
       if (cond) f = add_cond(k, cond[i], P, f);
       out[4 * i] = f.x;
       out[4 * i + 1] = f.y;
       out[4 * i + 2] = f.z;
       out[4 * i + 3] = f.w;
     } else {
-      float v = raw_noise_value(k, P, s);
+      float v = raw_noise_value<PPC>(k, P, s);
       if (cond && cond[i].active) v += cond_value(k, cond[i], P);
       out[i] = v;
     }
@@ -188,10 +189,10 @@ static int psi_common(bool grad, const mupsi_kernel* kernel, int64_t n, const fl
   MUPSI_CUDA(dout.out(out, ocomp * n, mem));
   int64_t blocks = std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 64);
   const Cond* cptr = cond ? reinterpret_cast<const Cond*>(dc.ptr) : nullptr;
-  if (grad)
-    k_psi<true><<<(unsigned)blocks, 256, 0, st>>>(k, n, dp.ptr, ds.ptr, cptr, dout.ptr);
-  else
-    k_psi<false><<<(unsigned)blocks, 256, 0, st>>>(k, n, dp.ptr, ds.ptr, cptr, dout.ptr);
+  auto fn = grad ? (k.ppc == 1 ? k_psi<true, 1> : k.ppc == 3 ? k_psi<true, 3> : k.ppc == 8 ? k_psi<true, 8> : k_psi<true, 0>)
+                 : (k.ppc == 1 ? k_psi<false, 1> : k.ppc == 3 ? k_psi<false, 3> : k.ppc == 8 ? k_psi<false, 8>
+                                                                                    : k_psi<false, 0>);
+  fn<<<(unsigned)blocks, 256, 0, st>>>(k, n, dp.ptr, ds.ptr, cptr, dout.ptr);
   count_launch();
   MUPSI_CUDA(cudaGetLastError());
   MUPSI_CUDA(dout.finish());

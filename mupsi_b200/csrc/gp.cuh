@@ -66,63 +66,102 @@ MD void cell_impulse(const KParams& k, uint64_t& st, float bx, float by, float b
   const uint32_t wsign = ~pcg_next(st) & 0x80000000u;
   f(s, wsign);
 }
-template <typename F>
+// PPC > 0: k.ppc is known to be PPC at compile time (the batch entry's
+// instantiations for the common counts); 0: a loop over k.ppc; -1: the same
+// with the 3-impulse cell unrolled (the sphere-mean march kernels).
+template <int PPC = 0, typename F>
 MD void for_each_impulse(const KParams& k, int nx, int ny, int nz, uint32_t seed, F&& f) {
   uint32_t cs = make_seed4((uint32_t)nx, (uint32_t)ny, (uint32_t)nz, seed);
   uint64_t st = (uint64_t)(uint32_t)(cs + 1u);
   const float bx = (float)nx * k.kr, by = (float)ny * k.kr, bz = (float)nz * k.kr;
-  // the common count, unrolled (configuration-0 render 6.92 -> 6.71 ms); unrolling
-  // the 1- and 8-impulse cells as well made that render slower (7.05 and
-  // 7.74 ms), and unrolling the general loop by 2 or 4 gained nothing
-  if (k.ppc == 3) {
+  if constexpr (PPC > 0) {
 #pragma unroll
-    for (int i = 0; i < 3; ++i) cell_impulse(k, st, bx, by, bz, f);
-    return;
+    for (int i = 0; i < PPC; ++i) cell_impulse(k, st, bx, by, bz, f);
+  } else {
+    // the common count, unrolled: configuration-0 render 6.92 -> 6.71 ms.
+    // Unrolling the 1- and 8-impulse cells as well made that render slower
+    // (7.05 and 7.74 ms), unrolling the general loop by 2 or 4 gained nothing,
+    // and in the mesh-mean march (32 registers) the unrolled cell cost 5%
+    // (level-6 mesh render 704 -> 740 ms), so only PPC = -1 takes it.
+    if constexpr (PPC < 0) {
+      if (k.ppc == 3) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) cell_impulse(k, st, bx, by, bz, f);
+        return;
+      }
+    }
+    for (int i = 0; i < k.ppc; ++i) cell_impulse(k, st, bx, by, bz, f);
   }
-  for (int i = 0; i < k.ppc; ++i) cell_impulse(k, st, bx, by, bz, f);
 }
+
+// One impulse's term w h (and w grad h when GRAD) added to the running sums.
+template <bool GRAD>
+struct PsiAcc {
+  const KParams& k;
+  v3 p;
+  float v = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f;
+  MD void operator()(v3 s, uint32_t wsign) {
+    v3 d = p - s;
+    // |p - s|^2 with two fused multiply-adds (psi carries the exp2
+    // approximation's error already; the impulse positions stay exact)
+    float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
+    // w*h with w = +-1 and h >= 0: h with the weight's sign bit (exact)
+    const float hs = __uint_as_float(__float_as_uint(ex2_approx(r2 * k.k2)) | wsign);
+    v = v + hs;
+    if (GRAD) {  // (w*h)*c2*d = w*((h*c2)*d) bit for bit: rounding is sign-symmetric
+      float gs = hs * k.c2;
+      gx = gx + gs * d.x;
+      gy = gy + gs * d.y;
+      gz = gz + gs * d.z;
+    }
+  }
+};
 
 // Unnormalised InternalNoise sums over neighbour cells [c0, c1) of the 27, in
 // the reference's (dx, dy, dz) order (cell c = 9(dx+1) + 3(dy+1) + (dz+1)).
 // GRAD = false computes the value only.
-template <bool GRAD>
+template <bool GRAD, int PPC = 0>
 MD void psi_sums_cells(const KParams& k, v3 p, int cx, int cy, int cz, uint32_t seed, int c0, int c1, float& sv,
                        float& sx, float& sy, float& sz) {
-  float v = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f;
+  PsiAcc<GRAD> acc{k, p};
 #pragma unroll 1
   for (int c = c0; c < c1; ++c) {
     const int dx = c / 9 - 1, dy = (c / 3) % 3 - 1, dz = c % 3 - 1;
-    for_each_impulse(k, cx + dx, cy + dy, cz + dz, seed, [&](v3 s, uint32_t wsign) {
-      v3 d = p - s;
-      // |p - s|^2 with two fused multiply-adds (psi carries the exp2
-      // approximation's error already; the impulse positions stay exact)
-      float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
-      // w*h with w = +-1 and h >= 0: h with the weight's sign bit (exact)
-      const float hs = __uint_as_float(__float_as_uint(ex2_approx(r2 * k.k2)) | wsign);
-      v = v + hs;
-      if (GRAD) {  // (w*h)*c2*d = w*((h*c2)*d) bit for bit: rounding is sign-symmetric
-        float gs = hs * k.c2;
-        gx = gx + gs * d.x;
-        gy = gy + gs * d.y;
-        gz = gz + gs * d.z;
-      }
-    });
+    for_each_impulse<PPC>(k, cx + dx, cy + dy, cz + dz, seed, acc);
   }
-  sv = v;
-  sx = gx;
-  sy = gy;
-  sz = gz;
+  sv = acc.v;
+  sx = acc.gx;
+  sy = acc.gy;
+  sz = acc.gz;
 }
-template <bool GRAD>
+template <bool GRAD, int PPC = 0>
 MD void psi_sums_range(const KParams& k, v3 p, uint32_t seed, int c0, int c1, float& sv, float& sx, float& sy,
                        float& sz) {
   int cx, cy, cz;
   cell_of(k, p, cx, cy, cz);
-  psi_sums_cells<GRAD>(k, p, cx, cy, cz, seed, c0, c1, sv, sx, sy, sz);
+  psi_sums_cells<GRAD, PPC>(k, p, cx, cy, cz, seed, c0, c1, sv, sx, sy, sz);
 }
-template <bool GRAD>
+template <bool GRAD, int PPC = 0>
 MD void psi_sums(const KParams& k, v3 p, uint32_t seed, float& sv, float& sx, float& sy, float& sz) {
-  psi_sums_range<GRAD>(k, p, seed, 0, 27, sv, sx, sy, sz);
+  if constexpr (PPC > 0) {  // the same order with the dz cells unrolled (psi sweep 100 -> 81 ms)
+    int cx, cy, cz;
+    cell_of(k, p, cx, cy, cz);
+    PsiAcc<GRAD> acc{k, p};
+#pragma unroll 1
+    for (int dx = -1; dx <= 1; ++dx) {
+#pragma unroll 1
+      for (int dy = -1; dy <= 1; ++dy) {
+#pragma unroll
+        for (int dz = -1; dz <= 1; ++dz) for_each_impulse<PPC>(k, cx + dx, cy + dy, cz + dz, seed, acc);
+      }
+    }
+    sv = acc.v;
+    sx = acc.gx;
+    sy = acc.gy;
+    sz = acc.gz;
+  } else {
+    psi_sums_range<GRAD, PPC>(k, p, seed, 0, 27, sv, sx, sy, sz);
+  }
 }
 
 // A group of G lanes (G a power of two, lanes gbase..gbase+G-1 of the warp)
@@ -147,12 +186,12 @@ MD void slot_cells(int q, int& c0, int& c1) {
   c0 = 7 * (q >> 2) + 2 * r - (q == 15 ? 1 : 0);
   c1 = c0 + ((r == 3 || q == 14) ? 1 : 2);
 }
-template <bool GRAD>
+template <bool GRAD, int PPC = 0>
 MD float4 slot_sums(const KParams& k, v3 p, int cx, int cy, int cz, uint32_t seed, int q) {
   int c0, c1;
   slot_cells(q, c0, c1);
   float4 x;
-  psi_sums_cells<GRAD>(k, p, cx, cy, cz, seed, c0, c1, x.x, x.y, x.z, x.w);
+  psi_sums_cells<GRAD, PPC>(k, p, cx, cy, cz, seed, c0, c1, x.x, x.y, x.z, x.w);
   return x;
 }
 template <bool GRAD>
@@ -162,7 +201,7 @@ MD float4 add_s(float4 a, float4 b) {
 }
 // WIDE: the caller guarantees G >= 4 (V <= 4: the subtree is written out);
 // otherwise a stack of partial sums walks the lane's V <= 16 slots.
-template <bool GRAD, bool WIDE>
+template <bool GRAD, bool WIDE, int PPC = 0>
 MD float4 psi_sums_group(const KParams& k, v3 p, uint32_t seed, const Group& g) {
   int cx, cy, cz;
   cell_of(k, p, cx, cy, cz);
@@ -170,17 +209,17 @@ MD float4 psi_sums_group(const KParams& k, v3 p, uint32_t seed, const Group& g) 
   const int q0 = g.G >= 16 ? (g.sub & 15) : g.sub * V;
   float4 r;
   if (WIDE) {
-    r = slot_sums<GRAD>(k, p, cx, cy, cz, seed, q0);
-    if (V >= 2) r = add_s<GRAD>(r, slot_sums<GRAD>(k, p, cx, cy, cz, seed, q0 + 1));
+    r = slot_sums<GRAD, PPC>(k, p, cx, cy, cz, seed, q0);
+    if (V >= 2) r = add_s<GRAD>(r, slot_sums<GRAD, PPC>(k, p, cx, cy, cz, seed, q0 + 1));
     if (V >= 4) {
-      const float4 a = slot_sums<GRAD>(k, p, cx, cy, cz, seed, q0 + 2);
-      r = add_s<GRAD>(r, add_s<GRAD>(a, slot_sums<GRAD>(k, p, cx, cy, cz, seed, q0 + 3)));
+      const float4 a = slot_sums<GRAD, PPC>(k, p, cx, cy, cz, seed, q0 + 2);
+      r = add_s<GRAD>(r, add_s<GRAD>(a, slot_sums<GRAD, PPC>(k, p, cx, cy, cz, seed, q0 + 3)));
     }
   } else {
     float4 st[5];
 #pragma unroll 1
     for (int j = 0; j < V; ++j) {
-      float4 x = slot_sums<GRAD>(k, p, cx, cy, cz, seed, q0 + j);
+      float4 x = slot_sums<GRAD, PPC>(k, p, cx, cy, cz, seed, q0 + j);
       bool carry = true;
 #pragma unroll
       for (int l = 0; l < 5; ++l) {
@@ -207,27 +246,29 @@ MD float4 psi_sums_group(const KParams& k, v3 p, uint32_t seed, const Group& g) 
   }
   return r;
 }
-template <bool WIDE = false>
+template <bool WIDE = false, int PPC = 0>
 MD float raw_noise_value_group(const KParams& k, v3 p, uint32_t seed, const Group& g) {
-  return (k.sigma * psi_sums_group<false, WIDE>(k, p, seed, g).x) / k.sqrt_var;
+  return (k.sigma * psi_sums_group<false, WIDE, PPC>(k, p, seed, g).x) / k.sqrt_var;
 }
-template <bool WIDE = false>
+template <bool WIDE = false, int PPC = 0>
 MD float4 raw_noise_group(const KParams& k, v3 p, uint32_t seed, const Group& g) {
-  const float4 s = psi_sums_group<true, WIDE>(k, p, seed, g);
+  const float4 s = psi_sums_group<true, WIDE, PPC>(k, p, seed, g);
   return make_float4((k.sigma * s.x) / k.sqrt_var, (k.sigma * s.y) / k.sqrt_var, (k.sigma * s.z) / k.sqrt_var,
                      (k.sigma * s.w) / k.sqrt_var);
 }
 
 // RawNoise(p, seed) = sigma * InternalNoise / sqrt(Var) (gpnoise.h:44)
+template <int PPC = 0>
 MD float4 raw_noise(const KParams& k, v3 p, uint32_t seed) {
   float v, x, y, z;
-  psi_sums<true>(k, p, seed, v, x, y, z);
+  psi_sums<true, PPC>(k, p, seed, v, x, y, z);
   return make_float4((k.sigma * v) / k.sqrt_var, (k.sigma * x) / k.sqrt_var, (k.sigma * y) / k.sqrt_var,
                      (k.sigma * z) / k.sqrt_var);
 }
+template <int PPC = 0>
 MD float raw_noise_value(const KParams& k, v3 p, uint32_t seed) {
   float v, x, y, z;
-  psi_sums<false>(k, p, seed, v, x, y, z);
+  psi_sums<false, PPC>(k, p, seed, v, x, y, z);
   return (k.sigma * v) / k.sqrt_var;
 }
 

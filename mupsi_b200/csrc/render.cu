@@ -401,7 +401,7 @@ __device__ void march_block_rays(const DScene* const* __restrict__ scenes, Paths
           myp = m.o + m.d * s_tw[pos];
           mymu = s_mw[pos];
         }
-        const float qv = (md.k.sigma * psi_sums_group<false, true>(md.k, myp, m.seed, half).x) / md.k.sqrt_var;
+        const float qv = (md.k.sigma * psi_sums_group<false, true, -1>(md.k, myp, m.seed, half).x) / md.k.sqrt_var;
         float f = mymu + qv;
         if (m.c.active) f += cond_value(md.k, m.c, myp);
         const bool hit = (f > 0.0f) != m.fprev_pos && (m.fprev_big || (double)fabsf(m.fprev - f) > 1e-6);

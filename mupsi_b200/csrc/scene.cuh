@@ -756,14 +756,14 @@ MD void march_psi(const DScene* S, March& m, v3 p, const Group& g, bool& ovf) {
     h.sub = g.sub & 15;
     h.mask = upper ? 0xffff0000u : 0x0000ffffu;
     const v3 pe = upper && ok ? m.o + m.d * tn : p;
-    const float v = (md.k.sigma * psi_sums_group<false, true>(md.k, pe, m.seed, h).x) / md.k.sqrt_var;
+    const float v = (md.k.sigma * psi_sums_group<false, true, -1>(md.k, pe, m.seed, h).x) / md.k.sqrt_var;
     const float vo = __shfl_xor_sync(0xffffffffu, v, 16);
     q = upper ? vo : v;
     m.spec_q = upper ? v : vo;
     m.spec_t = tn;
     m.spec_valid = ok;
   } else {
-    q = raw_noise_value_group<WIDE>(md.k, p, m.seed, g);
+    q = raw_noise_value_group<WIDE, MK == MEAN_SPHERE_ONLY ? -1 : 0>(md.k, p, m.seed, g);
   }
   float c = m.c.active ? cond_value(md.k, m.c, p) : 0.0f;
   float f;
@@ -822,7 +822,7 @@ template <int MK = MEAN_ANY, bool WIDE = false>
 MD float4 medium_eval_group(const DScene* S, const DMedium& md, v3 p, uint32_t seed, const Cond& c, bool& ovf,
                             const Group& g) {
   float4 mu = mean_value_grad<MK>(S, md, p, ovf);
-  float4 nz = raw_noise_group<WIDE>(md.k, p, seed, g);
+  float4 nz = raw_noise_group<WIDE, MK == MEAN_SPHERE_ONLY ? -1 : 0>(md.k, p, seed, g);
   float4 f = make_float4(mu.x + nz.x, mu.y + nz.y, mu.z + nz.z, mu.w + nz.w);
   return add_cond(md.k, c, p, f);
 }
