@@ -93,19 +93,20 @@ struct DScene {
 // carries no BVH code and keeps its registers).
 #define MEAN_ANY (-1)
 #define MEAN_SPHERE_ONLY 0
-template <int MK = MEAN_ANY>
+// INL: the BVH traversals inline (the field march's sphere tracer)
+template <int MK = MEAN_ANY, bool INL = false>
 MD float mean_value(const DScene* S, const DMedium& md, v3 p, bool& ovf) {
   if constexpr (MK == MEAN_SPHERE_ONLY) return norm3(p - md.center) - md.radius;
   if (md.mean_type == MUPSI_MEAN_SPHERE) return norm3(p - md.center) - md.radius;
   const DMesh& m = S->meshes[md.mesh];
-  float inside = mesh_inside(m, p, ovf) ? -1.0f : 1.0f;
+  float inside = mesh_inside<INL>(m, p, ovf) ? -1.0f : 1.0f;
   uint32_t tri;
   v3 q;
-  return inside * mesh_dist(m, p, tri, q, ovf);
+  return inside * mesh_dist<INL>(m, p, tri, q, ovf);
 }
 // eval + gradient (meanfunction.cpp:13-39); the mesh gradient reuses the single
 // inside/closest query of the value (the reference repeats both queries).
-template <int MK = MEAN_ANY>
+template <int MK = MEAN_ANY, bool INL = false>
 MD float4 mean_value_grad(const DScene* S, const DMedium& md, v3 p, bool& ovf) {
   if (MK == MEAN_SPHERE_ONLY || md.mean_type == MUPSI_MEAN_SPHERE) {
     v3 g = normalized(p - md.center);
@@ -113,10 +114,10 @@ MD float4 mean_value_grad(const DScene* S, const DMedium& md, v3 p, bool& ovf) {
   }
   if constexpr (MK == MEAN_SPHERE_ONLY) return make_float4(0, 0, 0, 0);
   const DMesh& m = S->meshes[md.mesh];
-  float inside = mesh_inside(m, p, ovf) ? -1.0f : 1.0f;
+  float inside = mesh_inside<INL>(m, p, ovf) ? -1.0f : 1.0f;
   uint32_t tri = 0;
   v3 q;
-  float d = mesh_dist(m, p, tri, q, ovf);
+  float d = mesh_dist<INL>(m, p, tri, q, ovf);
   v3 g;
   if (d < 1e-6f) {
     g = ld3(m.face_n + 3 * (int64_t)tri);
@@ -218,10 +219,10 @@ MD float4 ext_value_grad(const DMedium& md, v3 p, uint32_t seed) {
 }
 // value of a field medium: SDFMedium::eval is the mean function itself
 MD float field_value(const DScene* S, const DMedium& md, v3 p, uint32_t seed, bool& ovf) {
-  return md.kind == MUPSI_MEDIUM_SDF ? mean_value(S, md, p, ovf) : ext_value(md, p, seed);
+  return md.kind == MUPSI_MEDIUM_SDF ? mean_value<MEAN_ANY, true>(S, md, p, ovf) : ext_value(md, p, seed);
 }
 MD float4 field_value_grad(const DScene* S, const DMedium& md, v3 p, uint32_t seed, bool& ovf) {
-  return md.kind == MUPSI_MEDIUM_SDF ? mean_value_grad(S, md, p, ovf) : ext_value_grad(md, p, seed);
+  return md.kind == MUPSI_MEDIUM_SDF ? mean_value_grad<MEAN_ANY, true>(S, md, p, ovf) : ext_value_grad(md, p, seed);
 }
 
 // SDFMedium::sampleDistance (sdfmedium.cpp:16-63) / ExternalGPMedium::
@@ -433,8 +434,9 @@ MD float mu_lower(const March& m, float t) { return fabsf(m.mu_j) - fabsf(t - m.
 // best, and among triangles at the best distance the lowest index wins, so the
 // returned triangle and closest point do not depend on G or on which lane
 // visited what. `found`: a triangle beat best_init.
-MD float bvh_closest_group(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overflow, float best_init, bool& found,
-                           const Group& g) {
+// (Out of line, as the single-lane traversals are: level-6 mesh render 358 -> 263 ms alone.)
+static __device__ __noinline__ float bvh_closest_group(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overflow,
+                                                        float best_init, bool& found, const Group& g) {
   const int lane = (int)(threadIdx.x & 31);
   const unsigned gm = g.mask;
   uint32_t st[BVH_STACK];
