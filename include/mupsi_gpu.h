@@ -184,6 +184,30 @@ int mupsi_gpu_psi(const mupsi_kernel* kernel, int64_t n, const float* p, const u
 int mupsi_gpu_psi_value(const mupsi_kernel* kernel, int64_t n, const float* p, const uint32_t* seed,
                         const mupsi_cond* cond, float* out, mupsi_mem mem, void* stream);
 
+/* ------------------------------------------- integer known-answer probes -- */
+
+/* The device's own hash, PCG32 and grid-cell routines, one query per thread,
+ * so the integer parts of the path can be compared bit for bit with the
+ * reference on the GPU.
+ * make_seed (math/random.h:13-25): out[i] = make_seed(args[i*nargs .. +nargs)),
+ * nargs 4 (per cell / per pixel) or 5 (per bounce). */
+int mupsi_gpu_probe_make_seed(int64_t n, int32_t nargs, const uint32_t* args, uint32_t* out, mupsi_mem mem,
+                              void* stream);
+/* Random(seed) (math/random.h:73-119; zero seed -> 1, two warm-up draws), then
+ * `draws` outputs per seed: out_u32[n*draws] = nextUInt(), out_f32[n*draws] =
+ * next1D() of a second generator with the same seed; out_cs_i[n] =
+ * ConstantSampler(seed).nextI() (math/sampler.h:47-54, seed taken as u32). */
+int mupsi_gpu_probe_random(int64_t n, const uint64_t* seeds, int32_t draws, uint32_t* out_u32, float* out_f32,
+                           uint32_t* out_cs_i, mupsi_mem mem, void* stream);
+/* The impulses SparseGPNoiseGenerator::InternalNoise visits at p
+ * (gp/gpnoise.cpp:51-87): out_cells[n*27*3] the neighbour cells (truncated
+ * p / kernel_radius + (dx, dy, dz), dx slowest), out_cell_seeds[n*27]
+ * make_seed(cell, seed), out_s[n*27*ppc*3] the impulse positions and
+ * out_w[n*27*ppc] their weights (+-1), in the order of the sum. */
+int mupsi_gpu_probe_impulses(const mupsi_kernel* kernel, int64_t n, const float* p, const uint32_t* seed,
+                             int32_t* out_cells, uint32_t* out_cell_seeds, float* out_s, float* out_w, mupsi_mem mem,
+                             void* stream);
+
 /* ----------------------------------------------------- meshes and BVHs -- */
 
 /* Host BVH build (bvh/bvh.cpp:115-193): same split rule, leaf size, partition
@@ -292,12 +316,20 @@ int mupsi_gpu_render(mupsi_scene* scene, const mupsi_render_args* args);
  * the reference. The path state lives in one static device array of the library
  * (about 3 MB, held by every GPU that loads the library until exit), so:
  *   - n is at most 16384 samples per call (larger n returns MUPSI_ERR_INVALID);
- *   - x, y, k and out_rgb must be device memory; nothing is staged or allocated;
+ *   - x, y, k and out_rgb must be device memory of the current device
+ *     (MUPSI_ERR_INVALID otherwise); nothing is staged or allocated;
  *   - the first call on a device looks up the array's device address; make that
  *     first call before any stream capture on that device;
  *   - all calls share the array: calls that overlap on the GPU (other streams or
  *     host threads) race on it and must be serialised by the caller;
- *   - stream NULL means the default stream (no internal stream is created).
+ *   - stream NULL means the default stream (no internal stream is created); the
+ *     call returns once the trace on that stream has finished;
+ *   - a surrogate attached with mupsi_gpu_scene_set_surrogate is not used: the
+ *     mesh mean is always evaluated exactly, so for a scene with a surrogate the
+ *     radiance can differ from mupsi_gpu_trace_samples' (equal for every other
+ *     scene);
+ *   - shadow rays through a medium are marched inline rather than deferred to
+ *     shadow passes (same results).
  * The scene itself is created with mupsi_gpu_scene_create beforehand. */
 int mupsi_gpu_trace_samples_noalloc(mupsi_scene* scene, int64_t n, const int32_t* x, const int32_t* y,
                                     const int32_t* k, float* out_rgb, void* stream);

@@ -200,6 +200,56 @@ static int psi_common(bool grad, const mupsi_kernel* kernel, int64_t n, const fl
   return MUPSI_OK;
 }
 
+// ----------------------------------------------- integer known-answer probes
+// The hash, PCG32 and grid-cell routines the kernels use, exposed one query per
+// thread so their outputs can be compared bit for bit with the reference
+// (math/random.h:13-25,73-119, math/sampler.h:47-54, gp/gpnoise.cpp:54-62).
+__global__ void k_probe_seed(int64_t n, int nargs, const uint32_t* __restrict__ a, uint32_t* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t* v = a + i * nargs;
+    out[i] = nargs == 4 ? make_seed4(v[0], v[1], v[2], v[3]) : make_seed5(v[0], v[1], v[2], v[3], v[4]);
+  }
+}
+// Random(seed) then `draws` outputs: nextUInt as u32 and, from a second
+// generator with the same seed, next1D as float; cs_i: ConstantSampler(seed).nextI()
+__global__ void k_probe_random(int64_t n, const uint64_t* __restrict__ seeds, int draws, uint32_t* __restrict__ u,
+                               float* __restrict__ f, uint32_t* __restrict__ cs_i) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t a = pcg_seeded(seeds[i]), b = a;
+    for (int j = 0; j < draws; ++j) {
+      u[i * draws + j] = pcg_next(a);
+      f[i * draws + j] = pcg_next1d(b);
+    }
+    cs_i[i] = constant_sampler_i((uint32_t)seeds[i]);
+  }
+}
+// Per point: the 27 neighbour cells (cell_of + (dx, dy, dz) in the psi order),
+// their seeds, and every impulse's position and weight as the psi loop draws them.
+__global__ void k_probe_impulses(KParams k, int64_t n, const float* __restrict__ p, const uint32_t* __restrict__ seed,
+                                 int32_t* __restrict__ cells, uint32_t* __restrict__ cseed, float* __restrict__ s_out,
+                                 float* __restrict__ w_out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const v3 P = v3{p[3 * i], p[3 * i + 1], p[3 * i + 2]};
+    int cx, cy, cz;
+    cell_of(k, P, cx, cy, cz);
+    int64_t m = i * 27 * (int64_t)k.ppc;
+    for (int c = 0; c < 27; ++c) {
+      const int nx = cx + c / 9 - 1, ny = cy + (c / 3) % 3 - 1, nz = cz + c % 3 - 1;
+      cells[(i * 27 + c) * 3] = nx;
+      cells[(i * 27 + c) * 3 + 1] = ny;
+      cells[(i * 27 + c) * 3 + 2] = nz;
+      cseed[i * 27 + c] = make_seed4((uint32_t)nx, (uint32_t)ny, (uint32_t)nz, seed[i]);
+      for_each_impulse(k, nx, ny, nz, seed[i], [&](v3 s, uint32_t wsign) {
+        s_out[3 * m] = s.x;
+        s_out[3 * m + 1] = s.y;
+        s_out[3 * m + 2] = s.z;
+        w_out[m] = wsign ? -1.0f : 1.0f;
+        ++m;
+      });
+    }
+  }
+}
+
 // ------------------------------------------------------- buffer cache
 namespace {
 struct CachedBuf {
@@ -460,6 +510,81 @@ int mupsi_gpu_psi(const mupsi_kernel* kernel, int64_t n, const float* p, const u
 int mupsi_gpu_psi_value(const mupsi_kernel* kernel, int64_t n, const float* p, const uint32_t* seed,
                         const mupsi_cond* cond, float* out, mupsi_mem mem, void* stream) {
   return psi_common(false, kernel, n, p, seed, cond, out, mem, stream);
+}
+
+int mupsi_gpu_probe_make_seed(int64_t n, int32_t nargs, const uint32_t* args, uint32_t* out, mupsi_mem mem,
+                              void* stream) {
+  clear_error();
+  if (n < 0 || (nargs != 4 && nargs != 5)) return fail(MUPSI_ERR_INVALID, "n >= 0 and nargs 4 or 5");
+  if (n == 0) return MUPSI_OK;
+  if (!args || !out) return fail(MUPSI_ERR_INVALID, "null buffer");
+  cudaStream_t st = resolve_stream(stream);
+  Staged<uint32_t> da(st), dout(st);
+  MUPSI_CUDA(da.in(args, (size_t)n * nargs, mem));
+  MUPSI_CUDA(dout.out(out, n, mem));
+  k_probe_seed<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, st>>>(n, nargs, da.ptr, dout.ptr);
+  count_launch();
+  MUPSI_CUDA(cudaGetLastError());
+  MUPSI_CUDA(dout.finish());
+  MUPSI_CUDA(cudaStreamSynchronize(st));
+  return MUPSI_OK;
+}
+
+int mupsi_gpu_probe_random(int64_t n, const uint64_t* seeds, int32_t draws, uint32_t* out_u32, float* out_f32,
+                           uint32_t* out_cs_i, mupsi_mem mem, void* stream) {
+  clear_error();
+  if (n < 0 || draws < 0 || draws > 4096) return fail(MUPSI_ERR_INVALID, "n >= 0 and 0 <= draws <= 4096");
+  if (n == 0) return MUPSI_OK;
+  if (!seeds || !out_cs_i || (draws && (!out_u32 || !out_f32))) return fail(MUPSI_ERR_INVALID, "null buffer");
+  cudaStream_t st = resolve_stream(stream);
+  Staged<uint64_t> ds(st);
+  Staged<uint32_t> du(st), dc(st);
+  Staged<float> df(st);
+  MUPSI_CUDA(ds.in(seeds, n, mem));
+  MUPSI_CUDA(du.out(out_u32, (size_t)n * draws, mem));
+  MUPSI_CUDA(df.out(out_f32, (size_t)n * draws, mem));
+  MUPSI_CUDA(dc.out(out_cs_i, n, mem));
+  k_probe_random<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, st>>>(n, ds.ptr, draws, du.ptr,
+                                                                                     df.ptr, dc.ptr);
+  count_launch();
+  MUPSI_CUDA(cudaGetLastError());
+  MUPSI_CUDA(du.finish());
+  MUPSI_CUDA(df.finish());
+  MUPSI_CUDA(dc.finish());
+  MUPSI_CUDA(cudaStreamSynchronize(st));
+  return MUPSI_OK;
+}
+
+int mupsi_gpu_probe_impulses(const mupsi_kernel* kernel, int64_t n, const float* p, const uint32_t* seed,
+                             int32_t* out_cells, uint32_t* out_cell_seeds, float* out_s, float* out_w, mupsi_mem mem,
+                             void* stream) {
+  clear_error();
+  if (int e = check_kernel(kernel)) return e;
+  if (n < 0) return fail(MUPSI_ERR_INVALID, "n must be >= 0");
+  if (n == 0) return MUPSI_OK;
+  if (!p || !seed || !out_cells || !out_cell_seeds || !out_s || !out_w) return fail(MUPSI_ERR_INVALID, "null buffer");
+  cudaStream_t st = resolve_stream(stream);
+  KParams k = make_kparams(*kernel);
+  const size_t m = (size_t)n * 27 * k.ppc;
+  Staged<float> dp(st), ds_(st), dw(st);
+  Staged<uint32_t> dseed(st), dcs(st);
+  Staged<int32_t> dcell(st);
+  MUPSI_CUDA(dp.in(p, 3 * (size_t)n, mem));
+  MUPSI_CUDA(dseed.in(seed, n, mem));
+  MUPSI_CUDA(dcell.out(out_cells, (size_t)n * 81, mem));
+  MUPSI_CUDA(dcs.out(out_cell_seeds, (size_t)n * 27, mem));
+  MUPSI_CUDA(ds_.out(out_s, 3 * m, mem));
+  MUPSI_CUDA(dw.out(out_w, m, mem));
+  k_probe_impulses<<<(unsigned)std::min<int64_t>((n + 127) / 128, 4096), 128, 0, st>>>(
+      k, n, dp.ptr, dseed.ptr, dcell.ptr, dcs.ptr, ds_.ptr, dw.ptr);
+  count_launch();
+  MUPSI_CUDA(cudaGetLastError());
+  MUPSI_CUDA(dcell.finish());
+  MUPSI_CUDA(dcs.finish());
+  MUPSI_CUDA(ds_.finish());
+  MUPSI_CUDA(dw.finish());
+  MUPSI_CUDA(cudaStreamSynchronize(st));
+  return MUPSI_OK;
 }
 
 int mupsi_bvh_build_host(int64_t num_vertices, const float* vertices, int64_t num_faces, const int32_t* faces,

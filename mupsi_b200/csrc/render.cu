@@ -2028,8 +2028,10 @@ int mupsi_gpu_render(mupsi_scene* scene, const mupsi_render_args* a) {
 }
 
 // Allocation-free variant of mupsi_gpu_trace_samples (no counterpart in the
-// reference): same kernels and results, path state in the library's static
-// scratch array, device buffers only, at most kNoAllocMaxSamples samples.
+// reference): same kernels, path state in the library's static scratch array,
+// device buffers of the current device only, at most kNoAllocMaxSamples
+// samples. Without surrogate rounds (P.rounds = 1) a scene's surrogate is not
+// consulted, so results equal mupsi_gpu_trace_samples' for scenes without one.
 int mupsi_gpu_trace_samples_noalloc(mupsi_scene* scene, int64_t n, const int32_t* x, const int32_t* y,
                                     const int32_t* k, float* out_rgb, void* stream) {
   clear_error();
@@ -2039,12 +2041,19 @@ int mupsi_gpu_trace_samples_noalloc(mupsi_scene* scene, int64_t n, const int32_t
                                        std::to_string(kNoAllocMaxSamples) + " samples per call");
   if (n == 0) return MUPSI_OK;
   if (!x || !y || !k || !out_rgb) return fail(MUPSI_ERR_INVALID, "null buffer");
+  int cur_dev = 0;
+  MUPSI_CUDA(cudaGetDevice(&cur_dev));
   for (const void* ptr : {(const void*)x, (const void*)y, (const void*)k, (const void*)out_rgb}) {
     cudaPointerAttributes at;
     if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess || at.type != cudaMemoryTypeDevice) {
       cudaGetLastError();
       return fail(MUPSI_ERR_INVALID, "trace_samples_noalloc takes device buffers only");
     }
+    // the kernels run on the current device; another GPU's buffer would be
+    // reached without peer access
+    if (at.device != cur_dev)
+      return fail(MUPSI_ERR_INVALID, "trace_samples_noalloc: buffer on device " + std::to_string(at.device) +
+                                         ", current device " + std::to_string(cur_dev));
   }
   void* scratch = nullptr;
   if (int e = noalloc_scratch(&scratch)) return e;

@@ -26,6 +26,9 @@ def _setup(L):
     L.mupsi_gpu_launch_count.restype = i64
     L.mupsi_gpu_psi.argtypes = [C.POINTER(_abi.Kernel), i64, vp, vp, vp, vp, C.c_int, vp]
     L.mupsi_gpu_psi_value.argtypes = [C.POINTER(_abi.Kernel), i64, vp, vp, vp, vp, C.c_int, vp]
+    L.mupsi_gpu_probe_make_seed.argtypes = [i64, i32, vp, vp, C.c_int, vp]
+    L.mupsi_gpu_probe_random.argtypes = [i64, vp, i32, vp, vp, vp, C.c_int, vp]
+    L.mupsi_gpu_probe_impulses.argtypes = [C.POINTER(_abi.Kernel), i64, vp, vp, vp, vp, vp, vp, C.c_int, vp]
     L.mupsi_bvh_build_host.argtypes = [i64, vp, i64, vp, vp, vp, C.POINTER(i64), C.POINTER(u32)]
     L.mupsi_gpu_mesh_create.argtypes = [C.POINTER(_abi.MeshDesc), C.POINTER(vp)]
     L.mupsi_gpu_mesh_destroy.argtypes = [vp]

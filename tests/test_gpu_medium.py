@@ -2,8 +2,11 @@
 on the GPU against the CPU oracle and the reference's fixtures.
 
 Bit-exact: mean values/gradients (sphere and mesh), march step t and hit
-point p, conditioning point C. Within tolerance (1e-5 relative to the term
-scale, as tests/test_gpu_psi.py states): f and grad f, u_tilde, g_tilde.
+point p, conditioning point C. Within tolerance: f and grad f of
+evalWithGradient to 1e-5 of the scale of their noise terms (the sum of the
+absolute values of the psi impulse terms and of the Renewal+ conditioning
+terms; the mean part is bit-exact and adds nothing) plus one rounding of the
+final sum, 2^-22 |f|; u_tilde, g_tilde to 1e-4.
 The march outcome depends on signs of f, which the GPU's exp can flip only
 when f is within ~1e-6 of zero, so march agreement is asserted per ray at
 >= 99.5% with every disagreement reported."""
@@ -31,8 +34,24 @@ def _cond(rng, p, spread=2.0, active_every=2):
     return c
 
 
-def _scale(c):
-    return 1e-5 * (30.0 + np.abs(c[:, 3:4]) + 3 * np.linalg.norm(c[:, 4:7], axis=1, keepdims=True))
+def _noise_tol(port, med, p, seed, cond, f):
+    """1e-5 of the per-output scale of the noise terms at p, plus one rounding
+    of f = mu + psi + conditioning (2^-22 |f| covers two roundings' spread)."""
+    from oracle import bind
+    k = bind.kernel_struct(med["sigma"], med["length"], med["aniso"], med["ppc"])
+    _, s_psi = port.psi_f64(k, p, seed)
+    L2 = float(np.float32(med["aniso"][0]) ** 2 + (np.float32(med["aniso"][1]) ** 2 + np.float32(med["aniso"][2]) ** 2))
+    c2, c4 = -2.0 / L2, 4.0 / (L2 * L2)
+    r = p.astype(np.float64) - cond[:, :3]
+    h = np.exp(-np.sum(r * r, axis=1) / L2)
+    u, g = cond[:, 3].astype(np.float64), cond[:, 4:7].astype(np.float64)
+    hg = (h * c2)[:, None] * r
+    rg = np.sum(r * g, axis=1)
+    s_c = np.zeros((len(p), 4))
+    s_c[:, 0] = np.abs(u * h) + np.sum(np.abs(g * hg), axis=1)
+    s_c[:, 1:] = np.abs(u[:, None] * hg) + np.abs(h[:, None] * c2 * g) + np.abs((h * c4 * rg)[:, None] * r)
+    s_c[cond[:, 7] == 0] = 0.0
+    return 1e-5 * (s_psi + s_c) + 2.0 ** -22 * np.abs(f)
 
 
 @pytest.fixture(scope="module")
@@ -68,16 +87,20 @@ def test_medium_eval(gpu, port, sphere_scene, mesh_scene):
             cond = _cond(rng, q)
             got = g.eval_with_gradient(0, q, s, cond)
             ref = port.medium_eval(h, 0, q, s, cond)
-            assert np.all(np.abs(got - ref) <= _scale(cond) * (1 + np.abs(ref)))
+            tol = _noise_tol(port, sc.media[0], q, s, cond, ref)
+            err = np.abs(got.astype(np.float64) - ref)
+            assert np.all(err <= tol), f"max err/tol {np.max(err / tol):.3g}"
         finally:
             port.scene_free(h)
 
 
-def test_medium_fixtures(gpu, golden):
+def test_medium_fixtures(gpu, port, golden):
     g = golden("medium_sphere.npz")
-    gs = GpuScene(S.config0_scene(8, 8, 1))
+    sc0 = S.config0_scene(8, 8, 1)
+    gs = GpuScene(sc0)
     got = gs.eval_with_gradient(0, g["points"], g["seeds"], g["cond"])
-    assert np.all(np.abs(got - g["medium_eval"]) <= _scale(g["cond"]) * (1 + np.abs(g["medium_eval"])))
+    ref = g["medium_eval"].astype(np.float64)
+    assert np.all(np.abs(got - ref) <= _noise_tol(port, sc0.media[0], g["points"], g["seeds"], g["cond"], ref))
     sd = gs.sample_distance(0, g["rays"], g["seeds"], g["cond"])
     ref = g["sample_distance"]
     same = (sd[:, 0] == ref[:, 0]) & (bits(sd[:, 1]) == bits(ref[:, 1]))
@@ -92,7 +115,8 @@ def test_medium_fixtures(gpu, golden):
     gm = GpuScene(sc)
     assert np.array_equal(bits(gm.mean(0, mb["points"])), bits(mb["mean"]))
     got = gm.eval_with_gradient(0, mb["points"], mb["seeds"], mb["cond"])
-    assert np.all(np.abs(got - mb["medium_eval"]) <= _scale(mb["cond"]) * (1 + np.abs(mb["medium_eval"])))
+    ref = mb["medium_eval"].astype(np.float64)
+    assert np.all(np.abs(got - ref) <= _noise_tol(port, sc.media[0], mb["points"], mb["seeds"], mb["cond"], ref))
 
 
 def _march_rays(rng, n, center, rin, rout, nt=1.5e-3):
