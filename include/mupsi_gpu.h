@@ -31,8 +31,8 @@
 extern "C" {
 #endif
 
-/* 2: mupsi_tuning gained block_rays */
-#define MUPSI_GPU_ABI_VERSION 2
+/* 2: mupsi_tuning gained block_rays; 3: mupsi_render_stats gained bvh_nodes/bvh_tris */
+#define MUPSI_GPU_ABI_VERSION 3
 
 typedef enum { MUPSI_MEM_HOST = 0, MUPSI_MEM_DEVICE = 1 } mupsi_mem;
 
@@ -357,8 +357,15 @@ typedef struct {
   uint64_t parity_casts;  /* of which needed the Mesh::inside parity cast */
   uint64_t surr_requests; /* surrogate predictions the marches asked for */
   uint64_t surr_accepted; /* of which outside the band (used as the lazy mean's bound) */
+  /* BVH work of the marches' mesh-mean queries and the shading's mesh
+   * intersections, counted only with profiling mode 2: nodes loaded (32 bytes
+   * each) and triangles tested (52 bytes: index, face, three vertices) */
+  uint64_t bvh_nodes;
+  uint64_t bvh_tris;
 } mupsi_render_stats;
-/* enable != 0 starts counting work and timing kernels on later renders. */
+/* enable != 0 starts counting work and timing kernels on later renders;
+ * enable == 2 also counts BVH work (the traversals then run counted copies,
+ * slower: time kernels with enable == 1). */
 int mupsi_gpu_scene_profile(mupsi_scene* scene, int32_t enable);
 /* Copy the accumulated statistics; reset != 0 clears them afterwards. */
 int mupsi_gpu_scene_stats(mupsi_scene* scene, mupsi_render_stats* out, int32_t reset);

@@ -148,6 +148,8 @@ class RenderStats(C.Structure):
         ("parity_casts", C.c_uint64),
         ("surr_requests", C.c_uint64),
         ("surr_accepted", C.c_uint64),
+        ("bvh_nodes", C.c_uint64),
+        ("bvh_tris", C.c_uint64),
     ]
 
 

@@ -473,9 +473,11 @@ class GpuScene:
         """Mesh mean at every visited step (the plain exact form) or lazily (default)."""
         check(load().mupsi_gpu_scene_set_mean_eval(self.h, medium, 1 if every_step else 0))
 
-    def profile(self, enable=True):
-        """Count march work and time the wavefront kernels with CUDA events."""
-        check(load().mupsi_gpu_scene_profile(self.h, 1 if enable else 0))
+    def profile(self, enable=True, bvh=False):
+        """Count march work and time the wavefront kernels with CUDA events;
+        bvh=True also counts BVH nodes and triangles (counted traversals: slower,
+        so take times from a render without it)."""
+        check(load().mupsi_gpu_scene_profile(self.h, (2 if bvh else 1) if enable else 0))
 
     def stats(self, reset=False):
         st = _abi.RenderStats()

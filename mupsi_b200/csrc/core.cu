@@ -358,6 +358,7 @@ int make_device_mesh(const mupsi_mesh_desc& md, DMesh& d, std::vector<void*>& al
   if (md.num_faces > 0x3FFFFFFF) return fail(MUPSI_ERR_INVALID, "too many faces");
   for (int64_t i = 0; i < 3 * md.num_faces; ++i)
     if (md.faces[i] < 0 || md.faces[i] >= md.num_vertices) return fail(MUPSI_ERR_INVALID, "face index out of range");
+  d.count = nullptr;
   std::vector<HostNode> nodes;
   std::vector<uint32_t> idx;
   uint32_t root = build_bvh(md.vertices, md.faces, md.num_faces, nodes, idx);

@@ -45,6 +45,35 @@ struct DMesh {
   m4 T, Tinv;
   int identity;           // Tinv.isIdentity()
   int normal_identity;    // normal transform (Tinv^T 3x3) is identity
+  // nullable: BVH work counters (instrumentation), kBvhCountSlots pairs of
+  // (nodes loaded, triangles tested); set only while a scene counts its work
+  unsigned long long* count;
+};
+
+// BVH work tallies of one traversal: every node load (32 bytes) and every
+// triangle tested (index 4 + face 12 + vertices 36 = 52 bytes). CNT = false
+// compiles to nothing; the counted copies of the traversals run only while a
+// scene's profiling asks for BVH counts (the uncounted code is unchanged).
+constexpr int kBvhCountSlots = 64;
+template <bool CNT>
+struct BvhTally {
+  MD void node(uint32_t = 1) {}
+  MD void tri() {}
+  MD void flush(const DMesh&) {}
+};
+template <>
+struct BvhTally<true> {
+  uint32_t n = 0, t = 0;
+  MD void node(uint32_t k = 1) { n += k; }
+  MD void tri() { ++t; }
+  MD void flush(const DMesh& m) {
+    if (m.count && (n | t)) {  // spread over slots: fewer same-address atomics
+      unsigned long long* c = m.count + 2 * (blockIdx.x % kBvhCountSlots);
+      atomicAdd(c, (unsigned long long)n);
+      atomicAdd(c + 1, (unsigned long long)t);
+    }
+    n = t = 0;
+  }
 };
 
 MD v3 vert(const DMesh& m, int32_t i) { return ld3(m.verts + 3 * (int64_t)i); }
@@ -107,18 +136,22 @@ MD float node_centroid(const BNode& b, int a) { return (b.mn[a] + b.mx[a]) * 0.5
 // BVH::intersect (bvh.cpp:197-250): closest hit, front-to-back by child centroid
 // along the parent's longest axis; narrows r.ft. `overflow` is set if the
 // traversal would exceed the reference's 64-entry stack.
+template <bool CNT = false>
 MD bool bvh_intersect_inl(const DMesh& m, Ray& r, uint32_t& tri, float& uu, float& vv, bool& overflow) {
   if (m.num_nodes == 0) return false;
+  BvhTally<CNT> tl;
   bool hit = false;
   uint32_t st[BVH_STACK];
   int sp = 0;
   st[sp++] = m.root;
   while (sp > 0) {
     BNode nd = load_node(m.nodes, st[--sp]);
+    tl.node();
     if (!aabb_hit(nd, r)) continue;
     if (nd.right & LEAF_FLAG) {
       uint32_t start = nd.left, cnt = nd.right & ~LEAF_FLAG;
       for (uint32_t i = start; i < start + cnt; ++i) {
+        tl.tri();
         uint32_t ti = __ldg(m.tri_idx + i);
         const int32_t* f = m.faces + 3 * (int64_t)ti;
         float t, u, v;
@@ -132,17 +165,20 @@ MD bool bvh_intersect_inl(const DMesh& m, Ray& r, uint32_t& tri, float& uu, floa
       }
     } else {
       BNode ln = load_node(m.nodes, nd.left), rn = load_node(m.nodes, nd.right);
+      tl.node(2);
       int axis = node_axis(nd);
       float lc = node_centroid(ln, axis), rc = node_centroid(rn, axis);
       bool near_first = (get(r.d, axis) > 0) ? (lc < rc) : (lc > rc);
       if (sp + 2 > BVH_STACK) {
         overflow = true;
+        tl.flush(m);
         return hit;
       }
       st[sp++] = near_first ? nd.right : nd.left;
       st[sp++] = near_first ? nd.left : nd.right;
     }
   }
+  tl.flush(m);
   return hit;
 }
 
@@ -246,9 +282,11 @@ MD float dist2_tri(v3 p, v3 a, v3 b, v3 c, v3& out) {
 // best_init (FLT_MAX in the reference) may be any value above the true squared
 // distance: boxes farther than it are pruned from the start and the same
 // minimum is found (`found` reports whether a triangle beat best_init).
+template <bool CNT = false>
 MD float bvh_closest_inl(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overflow,
                          float best_init = 3.402823466e+38f, bool* found = nullptr) {
   if (m.num_nodes == 0) return 0.0f;
+  BvhTally<CNT> tl;
   uint32_t st[BVH_STACK];
   int sp = 0;
   st[sp++] = m.root;
@@ -256,10 +294,12 @@ MD float bvh_closest_inl(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overf
   if (found) *found = false;
   while (sp > 0) {
     BNode nd = load_node(m.nodes, st[--sp]);
+    tl.node();
     if (dist2_aabb(p, nd) >= best) continue;
     if (nd.right & LEAF_FLAG) {
       uint32_t start = nd.left, cnt = nd.right & ~LEAF_FLAG;
       for (uint32_t i = start; i < start + cnt; ++i) {
+        tl.tri();
         uint32_t ti = __ldg(m.tri_idx + i);
         const int32_t* f = m.faces + 3 * (int64_t)ti;
         v3 tmp;
@@ -273,6 +313,7 @@ MD float bvh_closest_inl(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overf
       }
     } else {
       BNode ln = load_node(m.nodes, nd.left), rn = load_node(m.nodes, nd.right);
+      tl.node(2);
       float dl = dist2_aabb(p, ln), dr = dist2_aabb(p, rn);
       if (sp + 2 > BVH_STACK) {
         overflow = true;
@@ -287,6 +328,7 @@ MD float bvh_closest_inl(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overf
       }
     }
   }
+  tl.flush(m);
   return sqrtf(best);
 }
 
@@ -295,12 +337,23 @@ MD float bvh_closest_inl(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overf
 // instruction fetch, renders a level-6 mesh at 512x512x4 in 227 ms instead of
 // 358; the field march's sphere tracer keeps them inline (_inl: 224 ms
 // against 304 ms out of line for its mesh SDF).
+// The counted copies (bvh_*_counted) run instead while m.count is set.
+static __device__ __noinline__ bool bvh_intersect_counted(const DMesh& m, Ray& r, uint32_t& tri, float& uu,
+                                                          float& vv, bool& overflow) {
+  return bvh_intersect_inl<true>(m, r, tri, uu, vv, overflow);
+}
+static __device__ __noinline__ float bvh_closest_counted(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overflow,
+                                                         float best_init, bool* found) {
+  return bvh_closest_inl<true>(m, p, tri, q, overflow, best_init, found);
+}
 static __device__ __noinline__ bool bvh_intersect(const DMesh& m, Ray& r, uint32_t& tri, float& uu, float& vv,
                                                   bool& overflow) {
+  if (m.count) return bvh_intersect_counted(m, r, tri, uu, vv, overflow);
   return bvh_intersect_inl(m, r, tri, uu, vv, overflow);
 }
 static __device__ __noinline__ float bvh_closest(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overflow,
                                                  float best_init = 3.402823466e+38f, bool* found = nullptr) {
+  if (m.count) return bvh_closest_counted(m, p, tri, q, overflow, best_init, found);
   return bvh_closest_inl(m, p, tri, q, overflow, best_init, found);
 }
 

@@ -1155,6 +1155,10 @@ mupsi_scene::~mupsi_scene() {
 
 namespace {
 
+// work counters of a scene: 8 march counters, then the BVH tallies
+// (kBvhCountSlots pairs of nodes loaded, triangles tested)
+constexpr int kSceneCounters = 8 + 2 * kBvhCountSlots;
+
 int build_scene(const mupsi_scene_desc* desc, mupsi_scene* s) {
   DScene& S = s->h;
   std::memset(&S, 0, sizeof S);
@@ -1283,8 +1287,8 @@ int build_scene(const mupsi_scene_desc* desc, mupsi_scene* s) {
   MUPSI_CUDA(dev_take((void**)&s->err, sizeof(int)));
   MUPSI_CUDA(cudaMemset(s->err, 0, sizeof(int)));
   S.err = s->err;
-  MUPSI_CUDA(dev_take((void**)&s->counters, 8 * sizeof(unsigned long long)));
-  MUPSI_CUDA(cudaMemset(s->counters, 0, 8 * sizeof(unsigned long long)));
+  MUPSI_CUDA(dev_take((void**)&s->counters, kSceneCounters * sizeof(unsigned long long)));
+  MUPSI_CUDA(cudaMemset(s->counters, 0, kSceneCounters * sizeof(unsigned long long)));
   S.counters = nullptr;
   MUPSI_CUDA(dev_take((void**)&s->d, sizeof(DScene)));
   MUPSI_CUDA(cudaMemcpy(s->d, &S, sizeof(DScene), cudaMemcpyHostToDevice));
@@ -2085,6 +2089,8 @@ int mupsi_gpu_scene_profile(mupsi_scene* scene, int32_t enable) {
   scene->iter_counts.clear();
   scene->iter_march_ms.clear();
   scene->h.counters = enable ? scene->counters : nullptr;
+  // enable == 2 also tallies BVH work (counted copies of the traversals)
+  for (int i = 0; i < scene->h.nmesh; ++i) scene->h.meshes[i].count = enable == 2 ? scene->counters + 8 : nullptr;
   MUPSI_CUDA(cudaMemcpy(scene->d, &scene->h, sizeof(DScene), cudaMemcpyHostToDevice));
   return MUPSI_OK;
 }
@@ -2094,8 +2100,13 @@ int mupsi_gpu_scene_stats(mupsi_scene* scene, mupsi_render_stats* out, int32_t r
   if (!scene || !out) return fail(MUPSI_ERR_INVALID, "null argument");
   MUPSI_CUDA(cudaDeviceSynchronize());
   collect_events(scene);
-  unsigned long long c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  unsigned long long c[kSceneCounters] = {};
   MUPSI_CUDA(cudaMemcpy(c, scene->counters, sizeof c, cudaMemcpyDeviceToHost));
+  out->bvh_nodes = out->bvh_tris = 0;
+  for (int i = 0; i < kBvhCountSlots; ++i) {
+    out->bvh_nodes += c[8 + 2 * i];
+    out->bvh_tris += c[9 + 2 * i];
+  }
   out->march_steps = c[0];
   out->psi_evals = c[1];
   out->marches = c[2];

@@ -436,8 +436,10 @@ MD float mu_lower(const March& m, float t) { return fabsf(m.mu_j) - fabsf(t - m.
 // visited what. `found`: a triangle beat best_init.
 // Out of line, as the single-lane traversals are (on its own this took a level-6
 // mesh render at 512x512x4 from 358 to 263 ms).
-static __device__ __noinline__ float bvh_closest_group(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overflow,
-                                                        float best_init, bool& found, const Group& g) {
+template <bool CNT>
+MD float bvh_closest_group_impl(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overflow, float best_init,
+                                bool& found, const Group& g) {
+  BvhTally<CNT> tl;
   const int lane = (int)(threadIdx.x & 31);
   const unsigned gm = g.mask;
   uint32_t st[BVH_STACK];
@@ -472,10 +474,12 @@ static __device__ __noinline__ float bvh_closest_group(const DMesh& m, v3 p, uin
     if (sp == 0 && src != lane) st[sp++] = got;
     if (sp > 0) {
       const BNode nd = load_node(m.nodes, st[--sp]);
+      tl.node();
       if (!(dist2_aabb(p, nd) > bound)) {
         if (nd.right & LEAF_FLAG) {
           const uint32_t start = nd.left, cnt = nd.right & ~LEAF_FLAG;
           for (uint32_t i = start; i < start + cnt; ++i) {
+            tl.tri();
             const uint32_t ti = __ldg(m.tri_idx + i);
             const int32_t* f = m.faces + 3 * (int64_t)ti;
             v3 tmp;
@@ -491,6 +495,7 @@ static __device__ __noinline__ float bvh_closest_group(const DMesh& m, v3 p, uin
           ovf = true;
         } else {
           const BNode ln = load_node(m.nodes, nd.left), rn = load_node(m.nodes, nd.right);
+          tl.node(2);
           const float dl = dist2_aabb(p, ln), dr = dist2_aabb(p, rn);
           if (dl < dr) {
             if (!(dr > bound)) st[sp++] = nd.right;
@@ -518,7 +523,24 @@ static __device__ __noinline__ float bvh_closest_group(const DMesh& m, v3 p, uin
     q = wq;
     tri = t;
   }
+  if constexpr (CNT) {  // the group's tallies, added once by its first lane
+    for (int off = 1; off < g.G; off <<= 1) {
+      tl.n += __shfl_xor_sync(gm, tl.n, off, g.G);
+      tl.t += __shfl_xor_sync(gm, tl.t, off, g.G);
+    }
+    if (g.sub == 0) tl.flush(m);
+  }
   return gbest;
+}
+static __device__ __noinline__ float bvh_closest_group_counted(const DMesh& m, v3 p, uint32_t& tri, v3& q,
+                                                                bool& overflow, float best_init, bool& found,
+                                                                const Group& g) {
+  return bvh_closest_group_impl<true>(m, p, tri, q, overflow, best_init, found, g);
+}
+static __device__ __noinline__ float bvh_closest_group(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overflow,
+                                                        float best_init, bool& found, const Group& g) {
+  if (m.count) return bvh_closest_group_counted(m, p, tri, q, overflow, best_init, found, g);
+  return bvh_closest_group_impl<false>(m, p, tri, q, overflow, best_init, found, g);
 }
 
 // g (nullable): the lane group marching this ray; with G > 1 the closest-point

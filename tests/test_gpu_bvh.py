@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 from mupsi_b200 import scene as S
-from mupsi_b200.api import DeviceMesh
+from mupsi_b200.api import DeviceMesh, GpuScene
 
 pytestmark = pytest.mark.gpu
 FMAX = np.finfo(np.float32).max
@@ -106,3 +106,29 @@ def test_occlusion_from_root_matches_intersect(gpu):
     assert (reference != root).sum() > 100
     m.set_occlusion(False)
     assert np.array_equal(m.occluded(rays).astype(bool), reference)
+
+
+def test_bvh_work_counting_changes_nothing(gpu):
+    """Profiling mode 2 runs counted copies of the BVH traversals (nodes loaded,
+    triangles tested, for the bench's algorithmic BVH bytes): the image is the
+    same bit for bit and the counts are those of real traversals."""
+    from mupsi_b200.api import GpuRenderer
+    sc = S.config_mesh_scene(level=4, width=32, height=32, spp=2, seed=3)
+    g = GpuScene(sc)
+    r = GpuRenderer()
+    r.prepare_render(g)
+    plain = r.start_render_progressive(2)
+    g.profile(True, bvh=True)
+    g.stats(reset=True)
+    counted = r.start_render_progressive(2)
+    st = g.stats(reset=True)
+    g.profile(True)
+    again = r.start_render_progressive(2)
+    st1 = g.stats(reset=True)
+    g.profile(False)
+    assert np.array_equal(plain.view(np.uint32), counted.view(np.uint32))
+    assert np.array_equal(plain.view(np.uint32), again.view(np.uint32))
+    assert st["bvh_nodes"] > 0 and st["bvh_tris"] > 0 and st["mean_evals"] > 0
+    assert st1["bvh_nodes"] == 0 and st1["bvh_tris"] == 0  # mode 1 does not count BVH work
+    # every query loads at least its root node
+    assert st["bvh_nodes"] >= st["mean_evals"]

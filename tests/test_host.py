@@ -34,7 +34,7 @@ def test_exports_every_declared_symbol(lib):
     assert len(names) >= 20
     for n in names:
         assert hasattr(lib, n), n
-    assert lib.mupsi_gpu_abi_version() == 2
+    assert lib.mupsi_gpu_abi_version() == 3
 
 
 def test_host_bvh_build_matches_reference_fixture(lib, golden):
