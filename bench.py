@@ -129,10 +129,18 @@ def cpu_render_rate(eng, h, w, hh, passes, seconds, subsets, k0=0, seed=0, keep=
     image, every pixel at passes [k0, k0 + passes), sized together to about
     `seconds`. Returns the rate over all timed subsets, the per-subset rates and
     (keep) the traced pixels and radiance."""
-    probe = _pixel_subsets(w, hh, 16, 1, seed + 1000)[0]
-    t = time.perf_counter()
-    eng.trace(h, *_samples(probe, w, 1, k0))
-    rate0 = len(probe) / max(1e-6, time.perf_counter() - t)
+    # the rate from a probe of random pixels (one pass each), grown until it
+    # takes a measurable time
+    rate0, m = 0.0, 16
+    for _ in range(8):
+        probe = _pixel_subsets(w, hh, m, 1, seed + 1000)[0]
+        t = time.perf_counter()
+        eng.trace(h, *_samples(probe, w, 1, k0))
+        dt = time.perf_counter() - t
+        rate0 = len(probe) / max(1e-6, dt)
+        if dt > 0.05 * seconds or len(probe) >= w * hh:
+            break
+        m *= 4
     npix = int(max(4, rate0 * seconds / max(1, subsets + warmup) / passes))
     subs = _pixel_subsets(w, hh, npix, subsets + warmup, seed)
     rates, n_all, t_all, kept = [], 0, 0.0, []

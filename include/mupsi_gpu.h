@@ -31,7 +31,8 @@
 extern "C" {
 #endif
 
-/* 2: mupsi_tuning gained block_rays; 3: mupsi_render_stats gained bvh_nodes/bvh_tris */
+/* 2: mupsi_tuning gained block_rays; 3: mupsi_render_stats gained bvh_nodes/bvh_tris,
+ * mupsi_tuning gained lane_rays */
 #define MUPSI_GPU_ABI_VERSION 3
 
 typedef enum { MUPSI_MEM_HOST = 0, MUPSI_MEM_DEVICE = 1 } mupsi_mem;
@@ -507,6 +508,12 @@ typedef struct mupsi_tuning {
   int32_t block_rays;  /* sphere-mean marches: one ray per block, its next 2 x warps psi steps at
                           once, while the queue holds at most block_rays rays per persistent
                           block (late bounces); 0 = never. 0..256 */
+  int32_t lane_rays;   /* marches of longer queues: > 0 = one ray per lane, each ray visiting at
+                          most this many steps between the warp's psi rounds (psi sums pooled
+                          two points at a time); 0 = lane groups of min_group. 0..64 */
+  int32_t lane_max_tris; /* mesh means: one ray per lane only while every mesh mean of the scene
+                            has at most this many triangles (larger meshes keep lane groups,
+                            which share each closest-point query); >= 0 */
 } mupsi_tuning;
 int mupsi_gpu_set_tuning(const mupsi_tuning* t);
 int mupsi_gpu_get_tuning(mupsi_tuning* out);

@@ -168,6 +168,8 @@ class Tuning(C.Structure):
         ("shade_block", C.c_int32),
         ("wave_paths", C.c_int32),
         ("block_rays", C.c_int32),
+        ("lane_rays", C.c_int32),
+        ("lane_max_tris", C.c_int32),
     ]
 
 

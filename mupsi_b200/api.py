@@ -236,7 +236,7 @@ class DeviceMesh:
 
 
 TUNING_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning.json")
-_TUNING_KEYS = ("march_block", "min_group", "shade_block", "wave_paths", "block_rays")
+_TUNING_KEYS = ("march_block", "min_group", "shade_block", "wave_paths", "block_rays", "lane_rays", "lane_max_tris")
 _tuning_applied = False
 
 
@@ -254,7 +254,11 @@ def get_tuning():
 
 
 def set_tuning(**kw):
-    """Change some launch shapes (march_block, min_group, shade_block, wave_paths, block_rays)."""
+    """Change some launch shapes (march_block, min_group, shade_block, wave_paths, block_rays, lane_rays,
+    lane_max_tris). The committed tuning file is applied first, so a value set
+    here is not replaced when the first scene is created."""
+    if kw:
+        _ensure_tuning()
     cur = get_tuning()
     for k, v in kw.items():
         if k not in _TUNING_KEYS:

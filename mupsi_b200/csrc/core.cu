@@ -225,6 +225,7 @@ __global__ void k_probe_random(int64_t n, const uint64_t* __restrict__ seeds, in
 }
 // Per point: the 27 neighbour cells (cell_of + (dx, dy, dz) in the psi order),
 // their seeds, and every impulse's position and weight as the psi loop draws them.
+template <int PPC>
 __global__ void k_probe_impulses(KParams k, int64_t n, const float* __restrict__ p, const uint32_t* __restrict__ seed,
                                  int32_t* __restrict__ cells, uint32_t* __restrict__ cseed, float* __restrict__ s_out,
                                  float* __restrict__ w_out) {
@@ -239,7 +240,7 @@ __global__ void k_probe_impulses(KParams k, int64_t n, const float* __restrict__
       cells[(i * 27 + c) * 3 + 1] = ny;
       cells[(i * 27 + c) * 3 + 2] = nz;
       cseed[i * 27 + c] = make_seed4((uint32_t)nx, (uint32_t)ny, (uint32_t)nz, seed[i]);
-      for_each_impulse(k, nx, ny, nz, seed[i], [&](v3 s, uint32_t wsign) {
+      for_each_impulse<PPC>(k, nx, ny, nz, seed[i], [&](v3 s, uint32_t wsign) {
         s_out[3 * m] = s.x;
         s_out[3 * m + 1] = s.y;
         s_out[3 * m + 2] = s.z;
@@ -576,8 +577,12 @@ int mupsi_gpu_probe_impulses(const mupsi_kernel* kernel, int64_t n, const float*
   MUPSI_CUDA(dcs.out(out_cell_seeds, (size_t)n * 27, mem));
   MUPSI_CUDA(ds_.out(out_s, 3 * m, mem));
   MUPSI_CUDA(dw.out(out_w, m, mem));
-  k_probe_impulses<<<(unsigned)std::min<int64_t>((n + 127) / 128, 4096), 128, 0, st>>>(
-      k, n, dp.ptr, dseed.ptr, dcell.ptr, dcs.ptr, ds_.ptr, dw.ptr);
+  // the psi kernels' cell variants: unrolled for 1, 3 and 8 impulses (states
+  // jumped ahead), a stepped loop for other counts
+  auto fn = k.ppc == 1 ? k_probe_impulses<1> : k.ppc == 3 ? k_probe_impulses<3> : k.ppc == 8 ? k_probe_impulses<8>
+                                                                                              : k_probe_impulses<0>;
+  fn<<<(unsigned)std::min<int64_t>((n + 127) / 128, 4096), 128, 0, st>>>(k, n, dp.ptr, dseed.ptr, dcell.ptr, dcs.ptr,
+                                                                          ds_.ptr, dw.ptr);
   count_launch();
   MUPSI_CUDA(cudaGetLastError());
   MUPSI_CUDA(dcell.finish());

@@ -282,7 +282,11 @@ MD float dist2_tri(v3 p, v3 a, v3 b, v3 c, v3& out) {
 // best_init (FLT_MAX in the reference) may be any value above the true squared
 // distance: boxes farther than it are pruned from the start and the same
 // minimum is found (`found` reports whether a triangle beat best_init).
-template <bool CNT = false>
+// LOWTIE: prune only boxes strictly farther than the best and take the lowest
+// triangle index among equal distances, the rule of the lane-group query
+// (bvh_closest_group): the same triangle and closest point as that query for
+// any group size. Without it the reference's rule (first found wins).
+template <bool CNT = false, bool LOWTIE = false>
 MD float bvh_closest_inl(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overflow,
                          float best_init = 3.402823466e+38f, bool* found = nullptr) {
   if (m.num_nodes == 0) return 0.0f;
@@ -292,10 +296,13 @@ MD float bvh_closest_inl(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overf
   st[sp++] = m.root;
   float best = best_init;
   if (found) *found = false;
+  uint32_t btri = 0xffffffffu;
+  // a box is kept while its distance is below the best (at or below it: LOWTIE)
+  auto keep = [&](float db) { return LOWTIE ? !(db > best) : db < best; };
   while (sp > 0) {
     BNode nd = load_node(m.nodes, st[--sp]);
     tl.node();
-    if (dist2_aabb(p, nd) >= best) continue;
+    if (!keep(dist2_aabb(p, nd))) continue;
     if (nd.right & LEAF_FLAG) {
       uint32_t start = nd.left, cnt = nd.right & ~LEAF_FLAG;
       for (uint32_t i = start; i < start + cnt; ++i) {
@@ -304,9 +311,10 @@ MD float bvh_closest_inl(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overf
         const int32_t* f = m.faces + 3 * (int64_t)ti;
         v3 tmp;
         float d = dist2_tri(p, vert(m, __ldg(f)), vert(m, __ldg(f + 1)), vert(m, __ldg(f + 2)), tmp);
-        if (d < best) {
+        if (d < best || (LOWTIE && d == best && d < best_init && ti < btri)) {
           best = d;
           tri = ti;
+          btri = ti;
           q = tmp;
           if (found) *found = true;
         }
@@ -320,11 +328,11 @@ MD float bvh_closest_inl(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overf
         break;
       }
       if (dl < dr) {
-        if (dr < best) st[sp++] = nd.right;
-        if (dl < best) st[sp++] = nd.left;
+        if (keep(dr)) st[sp++] = nd.right;
+        if (keep(dl)) st[sp++] = nd.left;
       } else {
-        if (dl < best) st[sp++] = nd.left;
-        if (dr < best) st[sp++] = nd.right;
+        if (keep(dl)) st[sp++] = nd.left;
+        if (keep(dr)) st[sp++] = nd.right;
       }
     }
   }
@@ -355,6 +363,12 @@ static __device__ __noinline__ float bvh_closest(const DMesh& m, v3 p, uint32_t&
                                                  float best_init = 3.402823466e+38f, bool* found = nullptr) {
   if (m.count) return bvh_closest_counted(m, p, tri, q, overflow, best_init, found);
   return bvh_closest_inl(m, p, tri, q, overflow, best_init, found);
+}
+// One lane's closest-point query with the lane-group rule (LOWTIE).
+static __device__ __noinline__ float bvh_closest_lowtie(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overflow,
+                                                        float best_init, bool* found) {
+  if (m.count) return bvh_closest_inl<true, true>(m, p, tri, q, overflow, best_init, found);
+  return bvh_closest_inl<false, true>(m, p, tri, q, overflow, best_init, found);
 }
 
 // Mesh::inside (mesh.cpp:341-362): parity of crossings of a +x ray from p,

@@ -66,17 +66,59 @@ MD void cell_impulse(const KParams& k, uint64_t& st, float bx, float by, float b
   const uint32_t wsign = ~pcg_next(st) & 0x80000000u;
   f(s, wsign);
 }
+// The PCG32 state n steps after s0: s_n = A_n s0 + C_n (mod 2^64), A_n = M^n,
+// C_n = M^(n-1) + ... + M + 1 for the LCG multiplier M and increment 1. Exact
+// integer arithmetic: the same states as n sequential steps.
+template <int N>
+struct PcgAhead {
+  static constexpr uint64_t A = PcgAhead<N - 1>::A * 6364136223846793005ULL;
+  static constexpr uint64_t C = PcgAhead<N - 1>::C * 6364136223846793005ULL + 1ULL;
+};
+template <>
+struct PcgAhead<0> {
+  static constexpr uint64_t A = 1ULL, C = 0ULL;
+};
+// XSH-RR output of a state (the value pcg_next returns before stepping from it)
+MD uint32_t pcg_output(uint64_t old) {
+  const uint32_t xs = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+  const uint32_t rot = (uint32_t)(old >> 59u);
+#ifdef __CUDA_ARCH__
+  return __funnelshift_r(xs, xs, rot);
+#else
+  return (xs >> rot) | (xs << ((uint32_t)(-(int32_t)rot) & 31u));
+#endif
+}
+// Impulse I of a cell whose stream starts at s0 (< 2^32: the cell seed + 1):
+// draws 4I..4I+3, each from its own state computed from s0 (no chain of
+// dependent LCG steps), the same values cell_impulse draws in sequence.
+template <int I, typename F>
+MD void cell_impulse_at(const KParams& k, uint64_t s0, float bx, float by, float bz, F&& f) {
+  const float a = u01(pcg_output(PcgAhead<4 * I>::A * s0 + PcgAhead<4 * I>::C));
+  const float b = u01(pcg_output(PcgAhead<4 * I + 1>::A * s0 + PcgAhead<4 * I + 1>::C));
+  const float c = u01(pcg_output(PcgAhead<4 * I + 2>::A * s0 + PcgAhead<4 * I + 2>::C));
+  const v3 s = v3{bx + c * k.kr, by + b * k.kr, bz + a * k.kr};
+  const uint32_t wsign = ~pcg_output(PcgAhead<4 * I + 3>::A * s0 + PcgAhead<4 * I + 3>::C) & 0x80000000u;
+  f(s, wsign);
+}
+template <int N, int I = 0, typename F>
+MD void cell_impulses_ahead(const KParams& k, uint64_t s0, float bx, float by, float bz, F&& f) {
+  if constexpr (I < N) {
+    cell_impulse_at<I>(k, s0, bx, by, bz, f);
+    cell_impulses_ahead<N, I + 1>(k, s0, bx, by, bz, f);
+  }
+}
+
 // PPC > 0: k.ppc is known to be PPC at compile time (the batch entry's
 // instantiations for the common counts); 0: a loop over k.ppc; -1: the same
-// with the 3-impulse cell unrolled (the sphere-mean march kernels).
+// with the 3-impulse cell unrolled (the sphere-mean march kernels). Unrolled
+// cells draw from jumped-ahead states (cell_impulse_at), the loop steps.
 template <int PPC = 0, typename F>
 MD void for_each_impulse(const KParams& k, int nx, int ny, int nz, uint32_t seed, F&& f) {
   uint32_t cs = make_seed4((uint32_t)nx, (uint32_t)ny, (uint32_t)nz, seed);
   uint64_t st = (uint64_t)(uint32_t)(cs + 1u);
   const float bx = (float)nx * k.kr, by = (float)ny * k.kr, bz = (float)nz * k.kr;
   if constexpr (PPC > 0) {
-#pragma unroll
-    for (int i = 0; i < PPC; ++i) cell_impulse(k, st, bx, by, bz, f);
+    cell_impulses_ahead<PPC>(k, st, bx, by, bz, f);
   } else {
     // the common count, unrolled: configuration-0 render 6.92 -> 6.71 ms.
     // Unrolling the 1- and 8-impulse cells as well made that render slower
@@ -85,8 +127,7 @@ MD void for_each_impulse(const KParams& k, int nx, int ny, int nz, uint32_t seed
     // (level-6 mesh render 704 -> 740 ms), so only PPC = -1 takes it.
     if constexpr (PPC < 0) {
       if (k.ppc == 3) {
-#pragma unroll
-        for (int i = 0; i < 3; ++i) cell_impulse(k, st, bx, by, bz, f);
+        cell_impulses_ahead<3>(k, st, bx, by, bz, f);
         return;
       }
     }
@@ -180,6 +221,9 @@ MD void psi_sums(const KParams& k, v3 p, uint32_t seed, float& sv, float& sx, fl
 struct Group {
   int G, sub;
   unsigned mask;
+  // G = 1 only: a mesh mean's closest-point queries take the lane-group tie
+  // rule (bvh_closest_lowtie), so a lane alone finds what a group of any size finds
+  bool lowtie = false;
 };
 MD void slot_cells(int q, int& c0, int& c1) {
   const int r = q & 3;

@@ -240,6 +240,8 @@ struct WaveCfg {
   int shadow_pass;               // this march launch marches the shadow jobs of iteration `it`
   int min_group;                 // smallest lane group per march
   int block_rays;                // block-per-ray marches while n <= block_rays * blocks (sphere means)
+  int lane_rays;                 // > 0: one ray per lane for long sphere-mean queues (march_lanes), this
+                                 // many visited steps per ray between the warp's psi rounds
   int* err;                      // device error word (ERR_* bits)
   unsigned long long* counters;  // nullable work counters
 };
@@ -474,6 +476,201 @@ __device__ void march_block_rays(const DScene* const* __restrict__ scenes, Paths
   }
 }
 
+// Marches of a long queue: one ray per lane. Which steps need psi is settled
+// per ray without psi (the mean, the global and per-point noise bounds, the
+// Lipschitz jumps and, for mesh means, the lazy exact mean and its BVH
+// queries: march_cheap), each lane on its own ray with no copy of that work on
+// other lanes; the psi sums of every lane that reached a psi step are then
+// evaluated by the whole warp, two points at a time, each by a half-warp in the
+// 16-slot order (psi_sums_group with G = 16: the values the lane-group march
+// computes for any group size, so the march outcome and the hit normal are the
+// same bits). A hit's gradient sum goes the same way. A mesh mean's BVH queries
+// run on the querying lane alone (their results do not depend on the group).
+// `rays_per_warp` (a power of two <= 32) spreads a shorter queue over all warps:
+// only every (32 / rays_per_warp)-th lane takes a ray. Each round a ray visits at
+// most `budget` steps before the warp's psi round, so a ray far from the
+// surface (Lipschitz jumps, settled steps) does not hold the others' psi.
+// Round r >= 1 of a march with a surrogate resumes the marches suspended in
+// round r - 1 with their predictions (req/pred lists); a march that asks for a
+// prediction is saved and suspended as in the lane-group march.
+template <int MK>
+__device__ void march_lanes(const DScene* const* __restrict__ scenes, Paths& P, uint32_t n,
+                            const uint32_t* __restrict__ q, uint32_t* cursor, const WaveCfg& cfg, int rays_per_warp,
+                            int budget, int it, int round, bool resume, bool can_suspend) {
+  const unsigned full = 0xffffffffu;
+  const int lane = (int)(threadIdx.x & 31);
+  const int stride = 32 / rays_per_warp;
+  const bool owner = (lane & (stride - 1)) == 0;
+  const int R = P.rounds;
+  Group half;  // a half-warp evaluates one point's psi (16 slots, one per lane)
+  half.G = 16;
+  half.sub = lane & 15;
+  half.mask = full;
+  Group solo;  // this lane alone (mesh means: closest-point queries with the group tie rule)
+  solo.G = 1;
+  solo.sub = 0;
+  solo.mask = 1u << lane;
+  solo.lowtie = true;
+  March m;
+  const DScene* S = scenes[0];
+  uint32_t idx = 0;
+  bool active = false, ovf = false;
+  // this lane's rays (32 bits suffice per lane)
+  uint32_t steps = 0, psis = 0, marches = 0, imps = 0, mus = 0, pars = 0, reqs = 0, accs = 0;
+  while (true) {
+    // owners without a ray take the next ones from the queue (one atomic per warp)
+    bool drew = false;
+    const unsigned need = __ballot_sync(full, owner && !active);
+    if (need) {
+      uint32_t base = 0;
+      const int leader = __ffs(need) - 1;
+      if (lane == leader) base = atomicAdd(cursor, (uint32_t)__popc(need));
+      base = __shfl_sync(full, base, leader);
+      if (owner && !active) {
+        const uint32_t j = base + __popc(need & ((1u << lane) - 1u));
+        if (j < n) {
+          drew = true;
+          idx = resume ? __float_as_uint(P.req[(round - 1) & 1][j].w) : q[j];
+          const float4 o = P.o[idx], d = P.d[idx];
+          const int4 meta = P.meta[idx];
+          const int med = __float_as_int(d.w);
+          S = scenes[meta_inst(meta.w)];
+          if (resume || S->media[med].kind == MUPSI_MEDIUM_GP) {  // else k_march_field marches it
+            march_begin(S, m, mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), o.w, 3.402823466e+38f, med,
+                        medium_seed(S, meta.x, meta.y, meta.z, meta_bounce(meta.w)), load_cond(P, idx));
+            m.may_request = MK != MEAN_SPHERE_ONLY && can_suspend && m.lazy && S->media[med].surr;
+            if (MK != MEAN_SPHERE_ONLY && resume) {
+              const float4 a = P.ms0[idx], b = P.ms1[idx];
+              const int fl = __float_as_int(a.w);
+              m.t = a.x;
+              m.k = __float_as_int(a.y);
+              m.fprev = a.z;
+              m.fprev_pos = (fl & 1) != 0;
+              m.fprev_big = (fl & 2) != 0;
+              m.n_req = fl >> 8;
+              m.init = false;
+              m.mu_j = b.x;
+              m.mu_hi = b.y;
+              m.t_j = b.z;
+              if (march_apply_prediction(S->media[med], m, P.pred[(round - 1) & 1][j])) accs++;
+            } else {
+              marches++;
+            }
+            active = true;
+          }
+        }
+      }
+    }
+    if (!__any_sync(full, active || drew)) break;
+    // this lane's ray up to its next psi step (at most `budget` visited steps)
+    v3 p = mk3(0.0f, 0.0f, 0.0f);
+    const bool want = active && march_cheap<MK>(S, m, p, ovf, &solo, budget);
+    if (MK != MEAN_SPHERE_ONLY && active && m.status == 3) {  // suspended: save the march, request a prediction at p
+      const int fl = (m.fprev_pos ? 1 : 0) | (m.fprev_big ? 2 : 0) | (m.n_req << 8);
+      P.ms0[idx] = make_float4(m.t, __int_as_float(m.k), m.fprev, __int_as_float(fl));
+      P.ms1[idx] = make_float4(m.mu_j, m.mu_hi, m.t_j, 0.0f);
+      const uint32_t slot = atomicAdd(&P.rcounts[it * R + round], 1u);
+      P.req[round & 1][slot] = make_float4(p.x, p.y, p.z, __uint_as_float(idx));
+      reqs++;
+      steps += m.n_steps;
+      psis += m.n_psi;
+      imps += m.n_psi * 27u * (uint32_t)S->media[m.medium].k.ppc;
+      mus += m.n_mu;
+      pars += m.n_par;
+      active = false;
+    }
+    // the warp's psi values, two points per round; the kernel parameters are
+    // read once when every ray of the warp has the same scene and medium
+    float qv = 0.0f;
+    const unsigned vmask = __ballot_sync(full, want);
+    const int ref = vmask ? __ffs(vmask) - 1 : 0;
+    const DScene* S0 = reinterpret_cast<const DScene*>(__shfl_sync(full, reinterpret_cast<unsigned long long>(S), ref));
+    const int m0 = __shfl_sync(full, m.medium, ref);
+    const bool uni = __all_sync(full, !want || (S == S0 && m.medium == m0));
+    for (unsigned vm = vmask; vm;) {
+      const int a = __ffs(vm) - 1;
+      vm &= vm - 1u;
+      int b = a;
+      if (vm) {
+        b = __ffs(vm) - 1;
+        vm &= vm - 1u;
+      }
+      const int src = lane < 16 ? a : b;
+      const v3 ps = mk3(__shfl_sync(full, p.x, src), __shfl_sync(full, p.y, src), __shfl_sync(full, p.z, src));
+      const uint32_t sd = __shfl_sync(full, m.seed, src);
+      const DScene* Ss = S0;
+      int ms = m0;
+      if (!uni) {
+        Ss = reinterpret_cast<const DScene*>(__shfl_sync(full, reinterpret_cast<unsigned long long>(S), src));
+        ms = __shfl_sync(full, m.medium, src);
+      }
+      const KParams& k = Ss->media[ms].k;
+      const float v = raw_noise_value_group<true, MK == MEAN_SPHERE_ONLY ? -1 : 0>(k, ps, sd, half);
+      const float va = __shfl_sync(full, v, 0), vb = __shfl_sync(full, v, 16);
+      if (lane == a) qv = va;
+      if (lane == b && b != a) qv = vb;
+    }
+    if (want) {
+      m.n_psi++;
+      march_decide<MK>(S, m, p, qv, &solo, ovf);
+    }
+    // hits: the gradient at the hit point (GPMedium::evalWithGradient), two per round
+    const bool hit = active && m.status == 1;
+    const v3 ph = hit ? m.o + m.d * m.t : mk3(0.0f, 0.0f, 0.0f);
+    float4 nz = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    for (unsigned hm = __ballot_sync(full, hit); hm;) {
+      const int a = __ffs(hm) - 1;
+      hm &= hm - 1u;
+      int b = a;
+      if (hm) {
+        b = __ffs(hm) - 1;
+        hm &= hm - 1u;
+      }
+      const int src = lane < 16 ? a : b;
+      const v3 ps = mk3(__shfl_sync(full, ph.x, src), __shfl_sync(full, ph.y, src), __shfl_sync(full, ph.z, src));
+      const uint32_t sd = __shfl_sync(full, m.seed, src);
+      const DScene* Ss = reinterpret_cast<const DScene*>(__shfl_sync(full, reinterpret_cast<unsigned long long>(S), src));
+      const int ms = __shfl_sync(full, m.medium, src);
+      const KParams& k = Ss->media[ms].k;
+      const float4 g = raw_noise_group<true, MK == MEAN_SPHERE_ONLY ? -1 : 0>(k, ps, sd, half);
+      const float4 ga = make_float4(__shfl_sync(full, g.x, 0), __shfl_sync(full, g.y, 0), __shfl_sync(full, g.z, 0),
+                                    __shfl_sync(full, g.w, 0));
+      const float4 gb = make_float4(__shfl_sync(full, g.x, 16), __shfl_sync(full, g.y, 16),
+                                    __shfl_sync(full, g.z, 16), __shfl_sync(full, g.w, 16));
+      if (lane == a) nz = ga;
+      if (lane == b && b != a) nz = gb;
+    }
+    if (active && m.status != 0) {
+      if (hit) {  // march_result: normalize(grad f) at the hit step
+        const DMedium& md = S->media[m.medium];
+        const float4 mu = mean_value_grad<MK>(S, md, ph, ovf);
+        float4 f = make_float4(mu.x + nz.x, mu.y + nz.y, mu.z + nz.z, mu.w + nz.w);
+        f = add_cond(md.k, m.c, ph, f);
+        const v3 nn = normalized(mk3(f.y, f.z, f.w));
+        P.ha[idx] = make_float4(m.t, ph.x, ph.y, ph.z);
+        P.hb[idx] = make_float4(nn.x, nn.y, nn.z, __uint_as_float(0u));
+      } else {  // exited: t, p and normal zero
+        P.ha[idx] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        P.hb[idx] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(1u));
+      }
+      steps += m.n_steps;
+      psis += m.n_psi;
+      imps += m.n_psi * 27u * (uint32_t)S->media[m.medium].k.ppc;
+      mus += m.n_mu;
+      pars += m.n_par;
+      active = false;
+    }
+  }
+  if (ovf) atomicOr(cfg.err, ERR_BVH_STACK);
+  if (cfg.counters) {
+    unsigned long long c[8] = {steps, psis, marches, imps, mus, pars, reqs, accs};
+    for (int i = 0; i < (MK == MEAN_SPHERE_ONLY ? 4 : 8); ++i) {
+      for (int o = 16; o > 0; o >>= 1) c[i] += __shfl_down_sync(full, c[i], o);
+      if (lane == 0) atomicAdd(&cfg.counters[i], c[i]);
+    }
+  }
+}
+
 // Persistent march over the medium queue of iteration `it`. Each ray is
 // marched by a group of G lanes that share its psi sums: G = 4 while the queue
 // fills the resident threads, larger (up to 32) as the queue shrinks, so the
@@ -482,8 +679,15 @@ __device__ void march_block_rays(const DScene* const* __restrict__ scenes, Paths
 // The general (mesh-mean) march is bound by the latency of its BVH traversals
 // and runs best with every thread resident (16 blocks per SM, 32 registers,
 // the rest spilled to L1): 483 -> 331 ms for a level-6 mesh render at 512^2 x 4.
+#ifndef MUPSI_SPHERE_MARCH_BLOCKS
+#define MUPSI_SPHERE_MARCH_BLOCKS 4  // resident 128-thread blocks per SM of the sphere-mean march
+#endif
+#ifndef MUPSI_MESH_MARCH_BLOCKS
+#define MUPSI_MESH_MARCH_BLOCKS 16  // ... and of the general (mesh-mean) march
+#endif
 template <int MK, bool SH>
-__global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? 6 : 16) k_march(const DScene* const* __restrict__ scenes, Paths P, int it, int round,
+__global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? MUPSI_SPHERE_MARCH_BLOCKS : MUPSI_MESH_MARCH_BLOCKS)
+    k_march(const DScene* const* __restrict__ scenes, Paths P, int it, int round,
                                                WaveCfg cfg) {
   // round 0 marches the iteration's medium queue; round r >= 1 resumes the
   // marches suspended in round r - 1 with their surrogate predictions
@@ -500,6 +704,16 @@ __global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? 6 : 16) k_march(
   if constexpr (MK == MEAN_SPHERE_ONLY) {
     if ((uint64_t)n <= (uint64_t)gridDim.x * (uint64_t)cfg.block_rays) {
       march_block_rays<SH>(scenes, P, n, q, cursor, cfg);
+      return;
+    }
+  }
+  if (!SH && cfg.lane_rays) {
+    // long queues: one ray per lane, at least 2 rays per warp on average
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    if ((uint64_t)n >= 2 * warps) {
+      int r = 2;
+      while (r < 32 && (uint64_t)n >= warps * (uint64_t)(2 * r)) r <<= 1;
+      march_lanes<MK>(scenes, P, n, q, cursor, cfg, r, cfg.lane_rays, it, round, resume, can_suspend);
       return;
     }
   }
@@ -1394,7 +1608,7 @@ int ensure_paths(mupsi_scene* s, int64_t cap) {
 
 // Launch shapes of the wave kernels (mupsi_gpu_set_tuning; chosen by the
 // project's autotuner, mupsi_b200/autotune.py).
-mupsi_tuning g_tuning = {128, 4, 128, 0, 8};
+mupsi_tuning g_tuning = {128, 4, 128, 0, 8, 1, 262144};
 
 // Persistent march grid: resident blocks per SM x SMs.
 struct MarchLaunch {
@@ -1518,6 +1732,12 @@ WaveExec scene_exec(mupsi_scene* s) {
   w.cfg.shadow_pass = 0;
   w.cfg.min_group = g_tuning.min_group;
   w.cfg.block_rays = g_tuning.block_rays;
+  w.cfg.lane_rays = g_tuning.lane_rays;
+  // a large mesh mean's closest-point queries are shared by lane groups
+  for (int i = 0; i < s->h.nmed; ++i)
+    if (s->h.media[i].mean_type == MUPSI_MEAN_MESH && s->h.media[i].kind == MUPSI_MEDIUM_GP &&
+        s->h.meshes[s->h.media[i].mesh].num_faces > g_tuning.lane_max_tris)
+      w.cfg.lane_rays = 0;
   w.cfg.err = s->err;
   w.cfg.counters = s->profile ? s->counters : nullptr;
   w.mlp = s->surr_mlp;
@@ -1748,6 +1968,7 @@ void batch_wave_launches(mupsi_batch* b, int iters) {
   w.cfg.shadow_pass = 0;
   w.cfg.min_group = g_tuning.min_group;
   w.cfg.block_rays = g_tuning.block_rays;
+  w.cfg.lane_rays = g_tuning.lane_rays;
   w.cfg.err = b->err;
   w.cfg.counters = nullptr;
   WaveSrc src;
@@ -1760,7 +1981,7 @@ void batch_wave_launches(mupsi_batch* b, int iters) {
 
 bool same_tuning(const mupsi_tuning& a, const mupsi_tuning& c) {
   return a.march_block == c.march_block && a.min_group == c.min_group && a.shade_block == c.shade_block &&
-         a.block_rays == c.block_rays;
+         a.block_rays == c.block_rays && a.lane_rays == c.lane_rays && a.lane_max_tris == c.lane_max_tris;
 }
 
 // The graph of a wave with `iters` bounce iterations, captured on first use.
@@ -2143,6 +2364,8 @@ int mupsi_gpu_set_tuning(const mupsi_tuning* t) {
     return fail(MUPSI_ERR_INVALID, "shade_block must be a multiple of 32 in [32, 128]");
   if (t->wave_paths < 0 || t->wave_paths > (1 << 28)) return fail(MUPSI_ERR_INVALID, "wave_paths out of range");
   if (t->block_rays < 0 || t->block_rays > 256) return fail(MUPSI_ERR_INVALID, "block_rays must be in [0, 256]");
+  if (t->lane_rays < 0 || t->lane_rays > 64) return fail(MUPSI_ERR_INVALID, "lane_rays must be in [0, 64]");
+  if (t->lane_max_tris < 0) return fail(MUPSI_ERR_INVALID, "lane_max_tris must be >= 0");
   g_tuning = *t;
   return MUPSI_OK;
 }

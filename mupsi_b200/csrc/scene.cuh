@@ -566,6 +566,9 @@ MD float mean_exact(const DScene* S, March& m, v3 p, float t, bool& ovf, const G
   if (g && g->G > 1) {
     bvh_closest_group(mesh, p, tri, q, ovf, ub * ub * 1.0001f + 1e-4f, found, *g);
     if (!found) bvh_closest_group(mesh, p, tri, q, ovf, 3.402823466e+38f, found, *g);  // bound too tight
+  } else if (g && g->lowtie) {
+    bvh_closest_lowtie(mesh, p, tri, q, ovf, ub * ub * 1.0001f + 1e-4f, &found);
+    if (!found) bvh_closest_lowtie(mesh, p, tri, q, ovf, 3.402823466e+38f, &found);
   } else {
     bvh_closest(mesh, p, tri, q, ovf, ub * ub * 1.0001f + 1e-4f, &found);
     if (!found) bvh_closest(mesh, p, tri, q, ovf);  // the bound was too tight: full query
@@ -618,8 +621,10 @@ MD float noise_bound_at(const KParams& k, const Cond& c, v3 p) {
 // settles this step's sign without psi. For a mesh mean lb comes from the last
 // exact mu (Lipschitz) or the mesh's bounding sphere, and mu is re-evaluated
 // (BVH) only when that is stale and cannot settle the step.
+// budget: visited steps this call may settle; when it runs out the march is
+// left running (status 0) at a step not yet visited, to continue in a later call.
 template <int MK = MEAN_ANY>
-MD bool march_cheap(const DScene* S, March& m, v3& p, bool& ovf, const Group* g = nullptr) {
+MD bool march_cheap(const DScene* S, March& m, v3& p, bool& ovf, const Group* g = nullptr, int budget = 1 << 16) {
   const DMedium& md = S->media[m.medium];
   if (m.init) {
     p = m.o;
@@ -658,6 +663,7 @@ MD bool march_cheap(const DScene* S, March& m, v3& p, bool& ovf, const Group* g 
     }
   }
   for (int guard = 0; guard < 1 << 16; ++guard) {
+    if (guard >= budget) return false;  // continue later at this step
     if (!(m.t < m.ft)) {
       m.status = 2;
       return false;
@@ -750,6 +756,9 @@ MD bool march_apply_prediction(const DMedium& md, March& m, float pred) {
   return false;
 }
 
+template <int MK>
+MD void march_decide(const DScene* S, March& m, v3 p, float q, const Group* g, bool& ovf);
+
 // Phase B: f at the pending point (value only); decides hit or next step. The
 // psi sum is shared by the lanes of group g (all of which hold the same march).
 // WIDE: the group has G >= 4 lanes.
@@ -790,6 +799,14 @@ MD void march_psi(const DScene* S, March& m, v3 p, const Group& g, bool& ovf) {
   } else {
     q = raw_noise_value_group<WIDE, MK == MEAN_SPHERE_ONLY ? -1 : 0>(md.k, p, m.seed, g);
   }
+  march_decide<MK>(S, m, p, q, &g, ovf);
+}
+
+// Phase B after psi: q = RawNoise(p) at the pending point; f decides a hit or
+// the next step.
+template <int MK>
+MD void march_decide(const DScene* S, March& m, v3 p, float q, const Group* g, bool& ovf) {
+  const DMedium& md = S->media[m.medium];
   float c = m.c.active ? cond_value(md.k, m.c, p) : 0.0f;
   float f;
   if (m.pend_exact) {
@@ -822,7 +839,7 @@ MD void march_psi(const DScene* S, March& m, v3 p, const Group& g, bool& ovf) {
         return;
       }
     }
-    float mu = mean_exact<MK>(S, m, p, m.t, ovf, &g);
+    float mu = mean_exact<MK>(S, m, p, m.t, ovf, g);
     m.mu_j = mu;
     m.mu_hi = fabsf(mu);
     m.t_j = m.t;

@@ -84,6 +84,47 @@ def test_results_do_not_depend_on_launch_shape(gpu, tuning_restored, scene):
         assert np.array_equal(bits(rad), bits(base)), (mb, mg, sb, br)
 
 
+def test_lane_rays_render_matches(gpu, tuning_restored):
+    """Long sphere-mean queues marched one ray per lane (psi pooled per warp)
+    or by lane groups, under several launch shapes: identical images."""
+    sc = S.config0_scene(160, 160, 6)
+    imgs = []
+    for lr, mb, mg, br in ((0, 128, 16, 8), (4, 128, 16, 8), (1, 64, 4, 0), (16, 96, 32, 16), (0, 32, 4, 0)):
+        set_tuning(lane_rays=lr, march_block=mb, min_group=mg, block_rays=br)
+        r = GpuRenderer()
+        g = GpuScene(sc)
+        r.prepare_render(g)
+        g.profile(True)
+        imgs.append(r.start_render_progressive(6))
+        st = g.stats(reset=True)
+        g.profile(False)
+        assert st["iter_medium"][1] > 2 * 148 * 8 * 4  # bounce 1's queue is long enough for one ray per lane
+    for im in imgs[1:]:
+        assert np.array_equal(bits(imgs[0]), bits(im))
+    assert (imgs[0][..., 0] < 1).sum() > 100
+
+
+def test_lane_rays_mesh_render_matches(gpu, tuning_restored):
+    """Mesh means marched one ray per lane (the lazy mean's closest-point
+    queries on one lane with the lane-group tie rule) or by lane groups, and a
+    mesh above lane_max_tris kept on lane groups: identical images."""
+    sc = S.config_mesh_scene(level=5, width=128, height=128, spp=4, seed=2)
+    imgs = []
+    for lr, lmt in ((0, 1 << 18), (1, 1 << 18), (4, 1 << 18), (1, 0)):
+        set_tuning(lane_rays=lr, lane_max_tris=lmt)
+        r = GpuRenderer()
+        g = GpuScene(sc)
+        r.prepare_render(g)
+        g.profile(True)
+        imgs.append(r.start_render_progressive(4))
+        st = g.stats(reset=True)
+        g.profile(False)
+        assert st["iter_medium"][1] > 2 * 148 * 16 * 4 and st["mean_evals"] > 0
+    for im in imgs[1:]:
+        assert np.array_equal(bits(imgs[0]), bits(im))
+    assert (imgs[0][..., 0] < 0.9).sum() > 500
+
+
 def test_block_rays_render_matches(gpu, tuning_restored):
     """A full 96x96x6 configuration-0 render with the block-per-ray march for
     every short queue (block_rays 16) and for none (0): identical images."""

@@ -99,7 +99,9 @@ def test_random_streams_golden_and_edges(gpu, port, golden):
 @pytest.mark.parametrize("kr,ppc", [(1.0, 3), (0.5, 1), (4.0, 8), (0.3, 3), (3.0, 2)])
 def test_grid_cells_and_impulses(gpu, port, kr, ppc):
     """Cells by truncation toward zero (not floor) at cell boundaries, at +-0 and
-    tiny values of both signs, for power-of-two and other cell sizes."""
+    tiny values of both signs, for power-of-two and other cell sizes; 1, 3 and 8
+    impulses per cell take the unrolled cells whose PCG states are jumped ahead
+    from the cell seed, 2 the stepped loop."""
     rng = np.random.default_rng(int(kr * 10) + ppc)
     n = 96
     p = rng.uniform(-150, 150, (n, 3)).astype(np.float32)
