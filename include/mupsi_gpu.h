@@ -545,7 +545,9 @@ typedef struct mupsi_batch_args {
 } mupsi_batch_args;
 enum {
   MUPSI_SCHEDULE_SHORTEST_FIRST = 0, /* instances by ascending paths (least mean completion time) */
-  MUPSI_SCHEDULE_IN_ORDER = 1        /* instances in the order given */
+  MUPSI_SCHEDULE_IN_ORDER = 1,       /* instances in the order given */
+  MUPSI_SCHEDULE_INTERLEAVED = 2     /* every wave takes a share of every instance's passes: all
+                                        instances progress together and complete in the last wave */
 };
 int mupsi_gpu_batch_render(mupsi_batch* batch, const mupsi_batch_args* args);
 

@@ -198,3 +198,4 @@ class BatchInfo(C.Structure):
 
 SCHEDULE_SHORTEST_FIRST = 0
 SCHEDULE_IN_ORDER = 1
+SCHEDULE_INTERLEAVED = 2

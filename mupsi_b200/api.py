@@ -617,7 +617,8 @@ class GpuBatch:
     whose paths carry their scene's index. No reference counterpart (the
     reference renders one scene per Renderer)."""
 
-    SCHEDULES = {"shortest_first": _abi.SCHEDULE_SHORTEST_FIRST, "in_order": _abi.SCHEDULE_IN_ORDER}
+    SCHEDULES = {"shortest_first": _abi.SCHEDULE_SHORTEST_FIRST, "in_order": _abi.SCHEDULE_IN_ORDER,
+                 "interleaved": _abi.SCHEDULE_INTERLEAVED}
 
     def __init__(self, scenes):
         _ensure_tuning()

@@ -683,10 +683,17 @@ __device__ void march_lanes(const DScene* const* __restrict__ scenes, Paths& P, 
 #define MUPSI_SPHERE_MARCH_BLOCKS 4  // resident 128-thread blocks per SM of the sphere-mean march
 #endif
 #ifndef MUPSI_MESH_MARCH_BLOCKS
-#define MUPSI_MESH_MARCH_BLOCKS 16  // ... and of the general (mesh-mean) march
+#define MUPSI_MESH_MARCH_BLOCKS 16  // ... of the general (mesh-mean) march with lane groups
 #endif
-template <int MK, bool SH>
-__global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? MUPSI_SPHERE_MARCH_BLOCKS : MUPSI_MESH_MARCH_BLOCKS)
+#ifndef MUPSI_MESH_LANE_MARCH_BLOCKS
+#define MUPSI_MESH_LANE_MARCH_BLOCKS 8  // ... and of the mesh-mean march with one ray per lane
+#endif
+// LANES: the instantiation carries march_lanes (one ray per lane); the mesh
+// kernel without it keeps its registers for the lane-group march alone
+template <int MK, bool SH, bool LANES = MK == MEAN_SPHERE_ONLY>
+__global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? MUPSI_SPHERE_MARCH_BLOCKS
+                                       : LANES               ? MUPSI_MESH_LANE_MARCH_BLOCKS
+                                                             : MUPSI_MESH_MARCH_BLOCKS)
     k_march(const DScene* const* __restrict__ scenes, Paths P, int it, int round,
                                                WaveCfg cfg) {
   // round 0 marches the iteration's medium queue; round r >= 1 resumes the
@@ -707,7 +714,7 @@ __global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? MUPSI_SPHERE_MAR
       return;
     }
   }
-  if (!SH && cfg.lane_rays) {
+  if (LANES && !SH && cfg.lane_rays) {
     // long queues: one ray per lane, at least 2 rays per warp on average
     const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
     if ((uint64_t)n >= 2 * warps) {
@@ -1617,16 +1624,20 @@ struct MarchLaunch {
   int blocks, block;
   int blocks_shadow;
 };
-MarchLaunch march_launch(bool sphere_only) {
+// lanes: a mesh-mean wave marched one ray per lane (the sphere-mean kernel
+// always carries that mode)
+MarchLaunch march_launch(bool sphere_only, bool lanes = false) {
   static std::mutex mu;
-  static std::vector<std::pair<int, MarchLaunch>> memo;  // key: variant | block << 1
+  static std::vector<std::pair<int, MarchLaunch>> memo;  // key: variant | lanes << 1 | block << 2
   const int block = g_tuning.march_block;
-  const int key = (sphere_only ? 1 : 0) | (block << 1);
+  lanes = lanes && !sphere_only;
+  const int key = (sphere_only ? 1 : 0) | (lanes ? 2 : 0) | (block << 2);
   std::lock_guard<std::mutex> lock(mu);
   for (auto& e : memo)
     if (e.first == key) return e.second;
   MarchLaunch m;
-  m.fn = sphere_only ? k_march<MEAN_SPHERE_ONLY, false> : k_march<MEAN_ANY, false>;
+  m.fn = sphere_only ? k_march<MEAN_SPHERE_ONLY, false>
+                     : (lanes ? k_march<MEAN_ANY, false, true> : k_march<MEAN_ANY, false, false>);
   m.fn_shadow = sphere_only ? k_march<MEAN_SPHERE_ONLY, true> : k_march<MEAN_ANY, true>;
   m.block = block;
   int per_sm = 0;
@@ -1683,7 +1694,7 @@ void launch_wave(const WaveExec& w, const WaveSrc& src, cudaStream_t st, mupsi_s
   int64_t gb = (int64_t)num_sms() * 16;
   if (!src.wave_idx) gb = std::max<int64_t>(1, std::min<int64_t>(gb, (src.n + 255) / 256));
   k_raygen<<<(int)gb, 256, 0, st>>>(w.scenes, w.P, src);
-  const MarchLaunch ml = march_launch(w.sphere_only);
+  const MarchLaunch ml = march_launch(w.sphere_only, w.cfg.lane_rays != 0);
   const int sblock = g_tuning.shade_block;
   const int sb = num_sms() * (2048 / sblock);
   for (int it = 0; it < w.iters; ++it) {
@@ -1721,6 +1732,16 @@ int wave_launches(int iters, int rounds = 1, bool field = false, bool defer = fa
 // the shadow passes (Paths::sh_*).
 bool needs_shadow_jobs(const DScene& h) { return h.nlights > 0 && h.nmed > 0; }
 
+// One ray per lane (lane_rays) unless a mesh mean of the scene is larger than
+// lane_max_tris: a large mesh's closest-point queries are shared by lane groups.
+int lane_rays_for(const DScene& S) {
+  for (int i = 0; i < S.nmed; ++i)
+    if (S.media[i].mean_type == MUPSI_MEAN_MESH && S.media[i].kind == MUPSI_MEDIUM_GP &&
+        S.meshes[S.media[i].mesh].num_faces > g_tuning.lane_max_tris)
+      return 0;
+  return g_tuning.lane_rays;
+}
+
 WaveExec scene_exec(mupsi_scene* s) {
   WaveExec w;
   w.scenes = s->d_list;
@@ -1732,12 +1753,7 @@ WaveExec scene_exec(mupsi_scene* s) {
   w.cfg.shadow_pass = 0;
   w.cfg.min_group = g_tuning.min_group;
   w.cfg.block_rays = g_tuning.block_rays;
-  w.cfg.lane_rays = g_tuning.lane_rays;
-  // a large mesh mean's closest-point queries are shared by lane groups
-  for (int i = 0; i < s->h.nmed; ++i)
-    if (s->h.media[i].mean_type == MUPSI_MEAN_MESH && s->h.media[i].kind == MUPSI_MEDIUM_GP &&
-        s->h.meshes[s->h.media[i].mesh].num_faces > g_tuning.lane_max_tris)
-      w.cfg.lane_rays = 0;
+  w.cfg.lane_rays = lane_rays_for(s->h);
   w.cfg.err = s->err;
   w.cfg.counters = s->profile ? s->counters : nullptr;
   w.mlp = s->surr_mlp;
@@ -1956,6 +1972,12 @@ int grow_device(T*& ptr, size_t& cap, size_t need, bool& moved) {
   return MUPSI_OK;
 }
 
+int batch_lane_rays(const mupsi_batch* b) {
+  int lr = g_tuning.lane_rays;
+  for (const mupsi_scene* s : b->inst) lr = std::min(lr, lane_rays_for(s->h));
+  return lr;
+}
+
 // One wave of the plan on stream bs: paths, bounces, accumulation.
 void batch_wave_launches(mupsi_batch* b, int iters) {
   WaveExec w;
@@ -1968,7 +1990,7 @@ void batch_wave_launches(mupsi_batch* b, int iters) {
   w.cfg.shadow_pass = 0;
   w.cfg.min_group = g_tuning.min_group;
   w.cfg.block_rays = g_tuning.block_rays;
-  w.cfg.lane_rays = g_tuning.lane_rays;
+  w.cfg.lane_rays = batch_lane_rays(b);
   w.cfg.err = b->err;
   w.cfg.counters = nullptr;
   WaveSrc src;
@@ -2009,7 +2031,7 @@ int batch_graph(mupsi_batch* b, int iters, cudaGraphExec_t* out) {
       *out = g.exec;
       return MUPSI_OK;
     }
-  march_launch(b->sphere_only);  // occupancy query outside the capture
+  march_launch(b->sphere_only, batch_lane_rays(b) != 0);  // occupancy query outside the capture
   cudaGraph_t graph = nullptr;
   MUPSI_CUDA(cudaStreamBeginCapture(b->bs, cudaStreamCaptureModeThreadLocal));
   batch_wave_launches(b, iters);
@@ -2425,7 +2447,8 @@ int mupsi_gpu_batch_render(mupsi_batch* b, const mupsi_batch_args* a) {
   const int n = (int)b->inst.size();
   for (int i = 0; i < n; ++i)
     if (a->spp[i] < 0) return fail(MUPSI_ERR_INVALID, "negative spp");
-  if (a->schedule != MUPSI_SCHEDULE_SHORTEST_FIRST && a->schedule != MUPSI_SCHEDULE_IN_ORDER)
+  if (a->schedule != MUPSI_SCHEDULE_SHORTEST_FIRST && a->schedule != MUPSI_SCHEDULE_IN_ORDER &&
+      a->schedule != MUPSI_SCHEDULE_INTERLEAVED)
     return fail(MUPSI_ERR_INVALID, "unknown schedule");
   b->info.waves = b->info.graph_launches = b->info.max_iters = 0;
   b->info.paths = 0;
@@ -2438,6 +2461,29 @@ int mupsi_gpu_batch_render(mupsi_batch* b, const mupsi_batch_args* a) {
   if (a->schedule == MUPSI_SCHEDULE_SHORTEST_FIRST)
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return work(x) < work(y); });
   const int64_t W = wave_paths();
+  // interleaved: every wave takes a share of every instance's passes, so all
+  // instances progress together and complete in the last wave; K waves of at
+  // most W paths each, instance i contributing about spp_i / K passes to each
+  int K = 1;
+  if (a->schedule == MUPSI_SCHEDULE_INTERLEAVED) {
+    int64_t total = 0;
+    for (int i = 0; i < n; ++i) total += work(i);
+    K = (int)std::max<int64_t>(1, (total + W - 1) / W);
+    for (;; ++K) {  // the smallest K whose largest wave fits W (one pass may exceed W alone)
+      int64_t worst = 0;
+      for (int k = 0; k < K; ++k) {
+        int64_t load = 0;
+        for (int i = 0; i < n; ++i) {
+          const int64_t p0 = (int64_t)a->spp[i] * k / K, p1 = (int64_t)a->spp[i] * (k + 1) / K;
+          load += (p1 - p0) * b->inst[i]->width * b->inst[i]->height;
+        }
+        worst = std::max(worst, load);
+      }
+      bool single = false;  // a wave holding one pass of one instance cannot shrink further
+      for (int i = 0; i < n; ++i) single |= work(i) / std::max(1, a->spp[i]) > W;
+      if (worst <= W || single || K >= (1 << 16)) break;
+    }
+  }
   std::vector<WaveChunk> chunks;
   std::vector<WaveDesc> waves;
   std::vector<int> wave_iters_v, last_wave(n, -1);
@@ -2450,6 +2496,24 @@ int mupsi_gpu_batch_render(mupsi_batch* b, const mupsi_batch_args* a) {
     cur = WaveDesc{0, 0, (int)chunks.size(), 0};
     cur_iters = 0;
   };
+  if (a->schedule == MUPSI_SCHEDULE_INTERLEAVED) {
+    for (int k = 0; k < K; ++k) {
+      for (int i = 0; i < n; ++i) {
+        mupsi_scene* s = b->inst[i];
+        const int64_t wh = (int64_t)s->width * s->height;
+        const int p0 = (int)((int64_t)a->spp[i] * k / K), p1 = (int)((int64_t)a->spp[i] * (k + 1) / K);
+        if (p1 <= p0) continue;
+        chunks.push_back(WaveChunk{i, p0, p1 - p0, s->width, cur.n, wh, cur.npix});
+        cur.n += (int64_t)(p1 - p0) * wh;
+        cur.npix += wh;
+        cur.nchunks++;
+        cur_iters = std::max(cur_iters, wave_iters(s));
+        last_wave[i] = (int)waves.size();
+      }
+      close_wave();
+    }
+    order.clear();  // planned
+  }
   for (int i : order) {
     mupsi_scene* s = b->inst[i];
     const int64_t wh = (int64_t)s->width * s->height;

@@ -43,7 +43,7 @@ def single_renders(scenes):
 
 
 @pytest.mark.parametrize("graphs", [True, False])
-@pytest.mark.parametrize("schedule", ["shortest_first", "in_order"])
+@pytest.mark.parametrize("schedule", ["shortest_first", "in_order", "interleaved"])
 def test_batch_equals_single_renders(gpu, tuning_restored, graphs, schedule):
     scenes = small_instances()
     ref = single_renders(scenes)
@@ -57,6 +57,8 @@ def test_batch_equals_single_renders(gpu, tuning_restored, graphs, schedule):
     assert info["paths"] == sum(s.width * s.height * s.spp for s in scenes)
     assert info["graph_launches"] == (info["waves"] if graphs else 0)
     assert np.all(done > 0)
+    if schedule == "interleaved":  # every instance has passes in the last wave
+        assert np.all(done == done.max())
     # a second render replays the captured graphs without new captures
     before = info["graphs_captured"]
     imgs2, _ = b.render([s.spp for s in scenes], use_graphs=graphs, schedule=schedule)
