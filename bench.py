@@ -248,7 +248,7 @@ def _peaks():
 OPS_PER_IMPULSE = 62
 # the gradient adds (w h) c2 (1 multiply) and three multiply + add pairs
 OPS_PER_IMPULSE_GRAD = 69
-BVH_NODE_BYTES, BVH_TRI_BYTES = 32, 52  # node; triangle index 4 + face 12 + vertices 36
+BVH_NODE_BYTES, BVH_TRI_BYTES = 32, 48  # node; leaf-ordered triangle record (3 vertices + id, padded)
 
 
 def issue_bound(ops, local=0):
@@ -305,7 +305,7 @@ def march_roofline(st, samples, ops=OPS_PER_IMPULSE, bvh=None, l2_gbs=None, hbm_
         gbs = bvh * samples / (ms / 1e3) / 1e9 if ms > 0 else 0.0
         out["bvh"] = {"bytes_per_sample": bvh, "achieved_gbs": gbs, "l2_gbs": l2_gbs, "hbm_gbs": hbm_gbs,
                       "frac_l2": gbs / l2_gbs if l2_gbs else None, "frac_hbm": gbs / hbm_gbs if hbm_gbs else None,
-                      "basis": "(nodes loaded x 32 B + triangles tested x 52 B) of the marches' and shading's "
+                      "basis": "(nodes loaded x 32 B + triangles tested x 48 B) of the marches' and shading's "
                                "BVH queries, counted on the device, / march kernel time"}
         out["mean_evals_per_sample"] = st["mean_evals"] / samples
     return out

@@ -360,7 +360,8 @@ typedef struct {
   uint64_t surr_accepted; /* of which outside the band (used as the lazy mean's bound) */
   /* BVH work of the marches' mesh-mean queries and the shading's mesh
    * intersections, counted only with profiling mode 2: nodes loaded (32 bytes
-   * each) and triangles tested (52 bytes: index, face, three vertices) */
+   * each) and triangles tested (48 bytes each: the leaf-ordered record of the
+   * three vertices and the triangle id) */
   uint64_t bvh_nodes;
   uint64_t bvh_tris;
 } mupsi_render_stats;

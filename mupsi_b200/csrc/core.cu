@@ -379,10 +379,21 @@ int make_device_mesh(const mupsi_mesh_desc& md, DMesh& d, std::vector<void*>& al
   }
   if (total > 0.0f)
     for (auto& c : cdf) c /= total;
+  // the triangles in leaf order (DMesh::soup)
+  std::vector<float> soup(12 * idx.size(), 0.0f);
+  for (size_t i = 0; i < idx.size(); ++i) {
+    const int32_t* f = md.faces + 3 * (int64_t)idx[i];
+    float* q = &soup[12 * i];
+    for (int k = 0; k < 3; ++k)
+      for (int c = 0; c < 3; ++c) q[3 * k + c] = md.vertices[3 * (int64_t)f[k] + c];
+    std::memcpy(&q[9], &idx[i], 4);
+  }
   std::memset(&d, 0, sizeof d);
   const BNode* dn = nullptr;
+  const float* dsoup = nullptr;
   cudaError_t e;
   if ((e = upload(allocs, reinterpret_cast<const BNode*>(nodes.data()), nodes.size(), dn)) != cudaSuccess ||
+      (e = upload(allocs, soup.data(), soup.size(), dsoup)) != cudaSuccess ||
       (e = upload(allocs, idx.data(), idx.size(), d.tri_idx)) != cudaSuccess ||
       (e = upload(allocs, md.faces, 3 * md.num_faces, d.faces)) != cudaSuccess ||
       (e = upload(allocs, md.vertices, 3 * md.num_vertices, d.verts)) != cudaSuccess ||
@@ -395,6 +406,7 @@ int make_device_mesh(const mupsi_mesh_desc& md, DMesh& d, std::vector<void*>& al
       return fail(MUPSI_ERR_CUDA, std::string("mesh upload: ") + cudaGetErrorString(e));
   }
   d.nodes = dn;
+  d.soup = reinterpret_cast<const float4*>(dsoup);
   d.num_nodes = (int64_t)nodes.size();
   d.num_faces = md.num_faces;
   d.root = root;

@@ -33,6 +33,11 @@ MD Ray make_ray(v3 o, v3 d) {
 struct DMesh {
   const BNode* nodes;
   const uint32_t* tri_idx;
+  // the triangles in leaf order (entry i is triangle tri_idx[i]): 3 float4 per
+  // entry holding its three vertices and, in the last word but two, its id, so a
+  // leaf reads its triangles with independent 16-byte loads instead of
+  // index -> face -> vertex chains
+  const float4* soup;
   const int32_t* faces;   // [F*3]
   const float* verts;     // [V*3]
   const float* face_n;    // [F*3]
@@ -51,7 +56,7 @@ struct DMesh {
 };
 
 // BVH work tallies of one traversal: every node load (32 bytes) and every
-// triangle tested (index 4 + face 12 + vertices 36 = 52 bytes). CNT = false
+// triangle tested (its 48-byte leaf-order record). CNT = false
 // compiles to nothing; the counted copies of the traversals run only while a
 // scene's profiling asks for BVH counts (the uncounted code is unchanged).
 constexpr int kBvhCountSlots = 64;
@@ -77,6 +82,16 @@ struct BvhTally<true> {
 };
 
 MD v3 vert(const DMesh& m, int32_t i) { return ld3(m.verts + 3 * (int64_t)i); }
+// Leaf-order entry i: the triangle's id and vertices (the same floats as
+// verts[faces[3 id + k]]).
+MD uint32_t leaf_tri(const DMesh& m, uint32_t i, v3& a, v3& b, v3& c) {
+  const float4* q = m.soup + 3 * (int64_t)i;
+  const float4 x = __ldg(q), y = __ldg(q + 1), z = __ldg(q + 2);
+  a = mk3(x.x, x.y, x.z);
+  b = mk3(x.w, y.x, y.y);
+  c = mk3(y.z, y.w, z.x);
+  return __float_as_uint(z.y);
+}
 
 // AABB::intersect slab test (bvh/boudingbox.cpp:6-38)
 MD bool aabb_hit(const BNode& b, const Ray& r) {
@@ -152,10 +167,10 @@ MD bool bvh_intersect_inl(const DMesh& m, Ray& r, uint32_t& tri, float& uu, floa
       uint32_t start = nd.left, cnt = nd.right & ~LEAF_FLAG;
       for (uint32_t i = start; i < start + cnt; ++i) {
         tl.tri();
-        uint32_t ti = __ldg(m.tri_idx + i);
-        const int32_t* f = m.faces + 3 * (int64_t)ti;
+        v3 a, b, c;
+        const uint32_t ti = leaf_tri(m, i, a, b, c);
         float t, u, v;
-        if (ray_tri(r, vert(m, __ldg(f)), vert(m, __ldg(f + 1)), vert(m, __ldg(f + 2)), t, u, v)) {
+        if (ray_tri(r, a, b, c, t, u, v)) {
           r.ft = t;
           tri = ti;
           uu = u;
@@ -197,9 +212,10 @@ MD bool bvh_occluded(const DMesh& m, const Ray& r, bool& overflow) {
     if (nd.right & LEAF_FLAG) {
       uint32_t start = nd.left, cnt = nd.right & ~LEAF_FLAG;
       for (uint32_t i = start; i < start + cnt; ++i) {
-        const int32_t* f = m.faces + 3 * (int64_t)__ldg(m.tri_idx + i);
+        v3 a, b, c;
+        leaf_tri(m, i, a, b, c);
         float t, u, v;
-        if (ray_tri(r, vert(m, __ldg(f)), vert(m, __ldg(f + 1)), vert(m, __ldg(f + 2)), t, u, v)) return true;
+        if (ray_tri(r, a, b, c, t, u, v)) return true;
       }
     } else {
       BNode ln = load_node(m.nodes, nd.left), rn = load_node(m.nodes, nd.right);
@@ -307,10 +323,9 @@ MD float bvh_closest_inl(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overf
       uint32_t start = nd.left, cnt = nd.right & ~LEAF_FLAG;
       for (uint32_t i = start; i < start + cnt; ++i) {
         tl.tri();
-        uint32_t ti = __ldg(m.tri_idx + i);
-        const int32_t* f = m.faces + 3 * (int64_t)ti;
-        v3 tmp;
-        float d = dist2_tri(p, vert(m, __ldg(f)), vert(m, __ldg(f + 1)), vert(m, __ldg(f + 2)), tmp);
+        v3 a, b, c, tmp;
+        const uint32_t ti = leaf_tri(m, i, a, b, c);
+        float d = dist2_tri(p, a, b, c, tmp);
         if (d < best || (LOWTIE && d == best && d < best_init && ti < btri)) {
           best = d;
           tri = ti;

@@ -2462,27 +2462,15 @@ int mupsi_gpu_batch_render(mupsi_batch* b, const mupsi_batch_args* a) {
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return work(x) < work(y); });
   const int64_t W = wave_paths();
   // interleaved: every wave takes a share of every instance's passes, so all
-  // instances progress together and complete in the last wave; K waves of at
-  // most W paths each, instance i contributing about spp_i / K passes to each
+  // instances progress together and complete in the last wave; K = total / W
+  // waves, instance i contributing about spp_i / K passes to each (a wave can
+  // exceed W by the passes rounding up; the path buffers are sized to the
+  // largest wave)
   int K = 1;
   if (a->schedule == MUPSI_SCHEDULE_INTERLEAVED) {
     int64_t total = 0;
     for (int i = 0; i < n; ++i) total += work(i);
-    K = (int)std::max<int64_t>(1, (total + W - 1) / W);
-    for (;; ++K) {  // the smallest K whose largest wave fits W (one pass may exceed W alone)
-      int64_t worst = 0;
-      for (int k = 0; k < K; ++k) {
-        int64_t load = 0;
-        for (int i = 0; i < n; ++i) {
-          const int64_t p0 = (int64_t)a->spp[i] * k / K, p1 = (int64_t)a->spp[i] * (k + 1) / K;
-          load += (p1 - p0) * b->inst[i]->width * b->inst[i]->height;
-        }
-        worst = std::max(worst, load);
-      }
-      bool single = false;  // a wave holding one pass of one instance cannot shrink further
-      for (int i = 0; i < n; ++i) single |= work(i) / std::max(1, a->spp[i]) > W;
-      if (worst <= W || single || K >= (1 << 16)) break;
-    }
+    K = (int)std::min<int64_t>(1 << 16, std::max<int64_t>(1, (total + W - 1) / W));
   }
   std::vector<WaveChunk> chunks;
   std::vector<WaveDesc> waves;

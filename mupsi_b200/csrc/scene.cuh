@@ -480,10 +480,9 @@ MD float bvh_closest_group_impl(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool
           const uint32_t start = nd.left, cnt = nd.right & ~LEAF_FLAG;
           for (uint32_t i = start; i < start + cnt; ++i) {
             tl.tri();
-            const uint32_t ti = __ldg(m.tri_idx + i);
-            const int32_t* f = m.faces + 3 * (int64_t)ti;
-            v3 tmp;
-            const float d = dist2_tri(p, vert(m, __ldg(f)), vert(m, __ldg(f + 1)), vert(m, __ldg(f + 2)), tmp);
+            v3 a, b, c, tmp;
+            const uint32_t ti = leaf_tri(m, i, a, b, c);
+            const float d = dist2_tri(p, a, b, c, tmp);
             if (d < best_init && (d < lbest || (d == lbest && ti < btri))) {
               lbest = d;
               btri = ti;
