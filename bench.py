@@ -51,6 +51,7 @@ def _args():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=3.0, help="CPU work per reference step")
     ap.add_argument("--extras", type=int, default=1, help="also time configurations 1-4 (single GPU)")
+    ap.add_argument("--parity", type=int, default=1, help="also compare the configuration-0 image in expectation")
     ap.add_argument("--only", choices=EXTRAS, default=None,
                     help="time only this configuration (its JSON object, no bench line)")
     return ap.parse_args()
@@ -430,7 +431,7 @@ def run_gpu(args):
     cpu = parity = None
     if rank == 0 and world == 1:
         cpu, kept = cpu_baseline_config0(sc, seconds=15.0)
-        parity = image_parity_config0(gs, kept)
+        parity = image_parity_config0(gs, kept) if args.parity else None
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",

@@ -553,6 +553,7 @@ __device__ void march_lanes(const DScene* const* __restrict__ scenes, Paths& P, 
               m.mu_hi = b.y;
               m.t_j = b.z;
               if (march_apply_prediction(S->media[med], m, P.pred[(round - 1) & 1][j])) accs++;
+              if (fl & 4) march_resume_decide<MK>(S, m, b.w, &solo, ovf);  // suspended in march_decide
             } else {
               marches++;
             }
@@ -564,11 +565,12 @@ __device__ void march_lanes(const DScene* const* __restrict__ scenes, Paths& P, 
     if (!__any_sync(full, active || drew)) break;
     // this lane's ray up to its next psi step (at most `budget` visited steps)
     v3 p = mk3(0.0f, 0.0f, 0.0f);
-    const bool want = active && march_cheap<MK>(S, m, p, ovf, &solo, budget);
-    if (MK != MEAN_SPHERE_ONLY && active && m.status == 3) {  // suspended: save the march, request a prediction at p
-      const int fl = (m.fprev_pos ? 1 : 0) | (m.fprev_big ? 2 : 0) | (m.n_req << 8);
+    // suspended (status 3 at a step march_cheap reached, 4 in march_decide with
+    // the step's psi): save the march, request a prediction at p
+    auto suspend = [&]() {
+      const int fl = (m.fprev_pos ? 1 : 0) | (m.fprev_big ? 2 : 0) | (m.status == 4 ? 4 : 0) | (m.n_req << 8);
       P.ms0[idx] = make_float4(m.t, __int_as_float(m.k), m.fprev, __int_as_float(fl));
-      P.ms1[idx] = make_float4(m.mu_j, m.mu_hi, m.t_j, 0.0f);
+      P.ms1[idx] = make_float4(m.mu_j, m.mu_hi, m.t_j, m.status == 4 ? m.spec_q : 0.0f);
       const uint32_t slot = atomicAdd(&P.rcounts[it * R + round], 1u);
       P.req[round & 1][slot] = make_float4(p.x, p.y, p.z, __uint_as_float(idx));
       reqs++;
@@ -578,7 +580,10 @@ __device__ void march_lanes(const DScene* const* __restrict__ scenes, Paths& P, 
       mus += m.n_mu;
       pars += m.n_par;
       active = false;
-    }
+    };
+    // (a resumed march may have finished in march_resume_decide)
+    const bool want = active && m.status == 0 && march_cheap<MK>(S, m, p, ovf, &solo, budget);
+    if (MK != MEAN_SPHERE_ONLY && active && m.status == 3) suspend();
     // the warp's psi values, two points per round; the kernel parameters are
     // read once when every ray of the warp has the same scene and medium
     float qv = 0.0f;
@@ -613,6 +618,7 @@ __device__ void march_lanes(const DScene* const* __restrict__ scenes, Paths& P, 
     if (want) {
       m.n_psi++;
       march_decide<MK>(S, m, p, qv, &solo, ovf);
+      if (MK != MEAN_SPHERE_ONLY && m.status == 4) suspend();
     }
     // hits: the gradient at the hit point (GPMedium::evalWithGradient), two per round
     const bool hit = active && m.status == 1;
@@ -791,6 +797,7 @@ __global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? MUPSI_SPHERE_MAR
               m.t_j = b.z;
               const bool used = march_apply_prediction(S->media[med], m, P.pred[(round - 1) & 1][j]);
               if (grp.sub == 0 && used) accs++;
+              if (fl & 4) march_resume_decide<MK>(S, m, b.w, &grp, ovf);  // suspended in march_decide
             } else if (grp.sub == 0) {
               marches++;
             }
@@ -801,13 +808,16 @@ __global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? MUPSI_SPHERE_MAR
     }
     if (!__any_sync(0xffffffffu, active || skipped)) break;
     if (active) {
-      v3 p;
-      if (march_cheap<MK>(S, m, p, ovf, &grp)) march_psi<MK, true>(S, m, p, grp, ovf);
-      if (MK != MEAN_SPHERE_ONLY && m.status == 3) {  // suspended: save the march, request a prediction at p
+      v3 p = mk3(0.0f, 0.0f, 0.0f);
+      // (a resumed march may have finished in march_resume_decide)
+      if (m.status == 0 && march_cheap<MK>(S, m, p, ovf, &grp)) march_psi<MK, true>(S, m, p, grp, ovf);
+      if (MK != MEAN_SPHERE_ONLY && m.status >= 3) {
+        // suspended (status 3 at a step march_cheap reached, 4 in march_decide
+        // with the step's psi): save the march, request a prediction at p
         if (grp.sub == 0) {
-          const int fl = (m.fprev_pos ? 1 : 0) | (m.fprev_big ? 2 : 0) | (m.n_req << 8);
+          const int fl = (m.fprev_pos ? 1 : 0) | (m.fprev_big ? 2 : 0) | (m.status == 4 ? 4 : 0) | (m.n_req << 8);
           P.ms0[idx] = make_float4(m.t, __int_as_float(m.k), m.fprev, __int_as_float(fl));
-          P.ms1[idx] = make_float4(m.mu_j, m.mu_hi, m.t_j, 0.0f);
+          P.ms1[idx] = make_float4(m.mu_j, m.mu_hi, m.t_j, m.status == 4 ? m.spec_q : 0.0f);
           const uint32_t slot = atomicAdd(&P.rcounts[it * R + round], 1u);
           P.req[round & 1][slot] = make_float4(p.x, p.y, p.z, __uint_as_float(idx));
           reqs++;

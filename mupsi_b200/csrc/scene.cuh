@@ -350,7 +350,8 @@ struct March {
   bool fprev_pos;
   bool fprev_big; // |f_origin| > B: its value never decides the 1e-6 test
   float fprev;
-  int status;     // 0 running, 1 hit, 2 exited, 3 suspended for a surrogate prediction
+  int status;     // 0 running, 1 hit, 2 exited, 3 suspended for a surrogate prediction at a
+                  // step march_cheap reached, 4 ... in march_decide (psi of the step in spec_q)
   int medium;
   uint32_t n_steps, n_psi;  // work counters: steps visited, psi evaluations
   uint32_t n_mu, n_par;     // mesh means: exact evaluations, parity casts among them
@@ -758,6 +759,19 @@ MD bool march_apply_prediction(const DMedium& md, March& m, float pred) {
 template <int MK>
 MD void march_decide(const DScene* S, March& m, v3 p, float q, const Group* g, bool& ovf);
 
+// A march suspended in march_decide (status 4) resumes there: the step's psi q
+// (saved with the march) and the prediction's anchor, or, without a usable
+// prediction, the exact mean (t_resumed blocks a second request).
+// Out of line: inlined into the refill path it doubled the mesh kernel's spills.
+template <int MK>
+static __device__ __noinline__ void march_resume_decide(const DScene* S, March& m, float q, const Group* g,
+                                                        bool& ovf) {
+  m.pend_exact = false;
+  m.pend_lb = 0.0f;  // the |mu| bound of the step did not settle it before the suspension
+  m.pend_sgn = 0.0f;
+  march_decide<MK>(S, m, m.o + m.d * m.t, q, g, ovf);
+}
+
 // Phase B: f at the pending point (value only); decides hit or next step. The
 // psi sum is shared by the lanes of group g (all of which hold the same march).
 // WIDE: the group has G >= 4 lanes.
@@ -837,6 +851,14 @@ MD void march_decide(const DScene* S, March& m, v3 p, float q, const Group* g, b
         march_advance(S, m, -INFINITY);
         return;
       }
+    }
+    if (MK != MEAN_SPHERE_ONLY && m.may_request && m.t != m.t_resumed && m.n_req < md.surr_max) {
+      // ask the surrogate before a BVH query here too: a prediction outside the
+      // band bounds |mu| at this step, which may settle the sign with this psi
+      // (march_resume_decide); the exact mean stays the fallback
+      m.spec_q = q;
+      m.status = 4;
+      return;
     }
     float mu = mean_exact<MK>(S, m, p, m.t, ovf, g);
     m.mu_j = mu;
