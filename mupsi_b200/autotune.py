@@ -28,9 +28,12 @@ CANDIDATES = {
     "min_group": [4, 8, 16, 32],
     "shade_block": [64, 128],
     "wave_paths": [1 << 21, 1 << 22, 1 << 23, 1 << 24],
-    "block_rays": [0, 4, 8, 16],
-    "lane_rays": [0, 1, 2, 4, 8, 16],
-    "lane_max_tris": [0, 1 << 17, 1 << 18, 1 << 20, 1 << 22],
+    "block_rays": [0, 4, 8, 12, 16, 24],
+    "lane_rays": [0, 1, 2, 4],
+    # mesh means only, which the tuning workload does not hold: the measured
+    # choice (a level-6 mesh is faster one ray per lane, a level-8 mesh with
+    # lane groups)
+    "lane_max_tris": [1 << 18],
 }
 DEFAULT = {"march_block": 128, "min_group": 4, "shade_block": 128, "wave_paths": 1 << 23, "block_rays": 8,
            "lane_rays": 1, "lane_max_tris": 1 << 18}
