@@ -398,7 +398,8 @@ def run_gpu(args):
                  "traffic_note": "not measurable inside the run (no device counters without a profiler); "
                                  "ncu's DRAM bytes for this kernel are in profiles/",
                  "launches": st["march_launches"], "ms_per_launch": st["march_ms"] / max(1, st["march_launches"]),
-                 "impulse_evals_per_launch": st["impulse_evals"] / max(1, st["march_launches"])})
+                 "impulse_evals_per_launch": st["impulse_evals"] / max(1, st["march_launches"]),
+                 "iter_rays": st["iter_medium"][:10], "iter_march_ms": [round(x, 4) for x in st["iter_march_ms"][:10]]})
 
     # end to end through the public API with pinned host buffers: scene upload,
     # render, framebuffer read back, release, every step

@@ -379,6 +379,33 @@ int make_device_mesh(const mupsi_mesh_desc& md, DMesh& d, std::vector<void*>& al
   }
   if (total > 0.0f)
     for (auto& c : cdf) c /= total;
+  // device node order: breadth first from the root (node 0), a pad at 1, and
+  // every inner node's children side by side at (left, left + 1), left even, so
+  // a traversal reads both with one 64-byte load. Boxes, leaf ranges and the
+  // tree are the reference's; only node positions change (traversal order
+  // follows boxes and centroids, not positions).
+  std::vector<HostNode> dev_nodes;
+  uint32_t occl_ref = 0;  // where the reference's node 0 (BVH::occluded's start) lands
+  if (!nodes.empty()) {
+    dev_nodes.reserve(nodes.size() + 1);
+    dev_nodes.push_back(nodes[root]);
+    dev_nodes.push_back(HostNode{});
+    std::vector<std::pair<uint32_t, uint32_t>> order{{root, 0u}};  // (reference index, device index)
+    for (size_t h = 0; h < order.size(); ++h) {
+      const uint32_t o = order[h].first, di = order[h].second;
+      if (o == 0) occl_ref = di;
+      const HostNode n = nodes[o];
+      if (n.right & 0x80000000u) continue;  // a leaf keeps (start, count | LEAF)
+      const uint32_t l = (uint32_t)dev_nodes.size();
+      dev_nodes.push_back(nodes[n.left]);
+      dev_nodes.push_back(nodes[n.right]);
+      dev_nodes[di].left = l;
+      dev_nodes[di].right = l + 1;
+      order.push_back({n.left, l});
+      order.push_back({n.right, l + 1});
+    }
+    root = 0;
+  }
   // the triangles in leaf order (DMesh::soup)
   std::vector<float> soup(12 * idx.size(), 0.0f);
   for (size_t i = 0; i < idx.size(); ++i) {
@@ -392,7 +419,7 @@ int make_device_mesh(const mupsi_mesh_desc& md, DMesh& d, std::vector<void*>& al
   const BNode* dn = nullptr;
   const float* dsoup = nullptr;
   cudaError_t e;
-  if ((e = upload(allocs, reinterpret_cast<const BNode*>(nodes.data()), nodes.size(), dn)) != cudaSuccess ||
+  if ((e = upload(allocs, reinterpret_cast<const BNode*>(dev_nodes.data()), dev_nodes.size(), dn)) != cudaSuccess ||
       (e = upload(allocs, soup.data(), soup.size(), dsoup)) != cudaSuccess ||
       (e = upload(allocs, idx.data(), idx.size(), d.tri_idx)) != cudaSuccess ||
       (e = upload(allocs, md.faces, 3 * md.num_faces, d.faces)) != cudaSuccess ||
@@ -407,10 +434,11 @@ int make_device_mesh(const mupsi_mesh_desc& md, DMesh& d, std::vector<void*>& al
   }
   d.nodes = dn;
   d.soup = reinterpret_cast<const float4*>(dsoup);
-  d.num_nodes = (int64_t)nodes.size();
+  d.num_nodes = (int64_t)dev_nodes.size();
   d.num_faces = md.num_faces;
   d.root = root;
-  d.occl_start = 0;
+  d.occl_ref = occl_ref;
+  d.occl_start = occl_ref;
   d.total_area = total;
   HostM4 T = translate_scale(md.position, md.scale), Ti = inverse4(T);
   std::memcpy(d.T.m, T.m, sizeof T.m);
@@ -665,7 +693,7 @@ int mupsi_gpu_mesh_set_occlusion(mupsi_mesh* mesh, int32_t mode) {
   if (!mesh) return fail(MUPSI_ERR_INVALID, "null mesh");
   if (mode != MUPSI_OCCLUSION_REFERENCE && mode != MUPSI_OCCLUSION_ROOT)
     return fail(MUPSI_ERR_INVALID, "unknown occlusion mode");
-  mesh->store.d.occl_start = mode == MUPSI_OCCLUSION_ROOT ? mesh->store.d.root : 0u;
+  mesh->store.d.occl_start = mode == MUPSI_OCCLUSION_ROOT ? mesh->store.d.root : mesh->store.d.occl_ref;
   return MUPSI_OK;
 }
 

@@ -45,7 +45,8 @@ struct DMesh {
   const float* cdf;       // area CDF [F]
   int64_t num_nodes, num_faces;
   uint32_t root;
-  uint32_t occl_start;    // first node of BVH::occluded: 0 as the reference, or root
+  uint32_t occl_start;    // first node of BVH::occluded: occl_ref as the reference, or root
+  uint32_t occl_ref;      // device position of the reference's node 0 (its post-order first leaf)
   float total_area;
   m4 T, Tinv;
   int identity;           // Tinv.isIdentity()
@@ -142,6 +143,27 @@ MD BNode load_node(const BNode* nodes, uint32_t i) {
   n.right = __float_as_uint(b.w);
   return n;
 }
+// The device node array keeps every inner node's two children side by side
+// at (left, left + 1) with left even (mesh upload re-lays the reference's
+// post-order array out breadth first): one 64-byte read loads both.
+MD BNode unpack_node(float4 a, float4 b) {
+  BNode n;
+  n.mn[0] = a.x;
+  n.mn[1] = a.y;
+  n.mn[2] = a.z;
+  n.mx[0] = a.w;
+  n.mx[1] = b.x;
+  n.mx[2] = b.y;
+  n.left = __float_as_uint(b.z);
+  n.right = __float_as_uint(b.w);
+  return n;
+}
+MD void load_pair(const BNode* nodes, uint32_t left, BNode& l, BNode& r) {
+  const float4* p = reinterpret_cast<const float4*>(nodes + left);
+  const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
+  l = unpack_node(a, b);
+  r = unpack_node(c, d);
+}
 MD int node_axis(const BNode& b) {
   float d0 = b.mx[0] - b.mn[0], d1 = b.mx[1] - b.mn[1], d2 = b.mx[2] - b.mn[2];
   return (d0 > d1 && d0 > d2) ? 0 : (d1 > d2 ? 1 : 2);
@@ -179,7 +201,8 @@ MD bool bvh_intersect_inl(const DMesh& m, Ray& r, uint32_t& tri, float& uu, floa
         }
       }
     } else {
-      BNode ln = load_node(m.nodes, nd.left), rn = load_node(m.nodes, nd.right);
+      BNode ln, rn;
+      load_pair(m.nodes, nd.left, ln, rn);
       tl.node(2);
       int axis = node_axis(nd);
       float lc = node_centroid(ln, axis), rc = node_centroid(rn, axis);
@@ -218,7 +241,8 @@ MD bool bvh_occluded(const DMesh& m, const Ray& r, bool& overflow) {
         if (ray_tri(r, a, b, c, t, u, v)) return true;
       }
     } else {
-      BNode ln = load_node(m.nodes, nd.left), rn = load_node(m.nodes, nd.right);
+      BNode ln, rn;
+      load_pair(m.nodes, nd.left, ln, rn);
       int axis = node_axis(nd);
       float lc = node_centroid(ln, axis), rc = node_centroid(rn, axis);
       bool near_first = (get(r.d, axis) > 0) ? (lc < rc) : (lc > rc);
@@ -335,7 +359,8 @@ MD float bvh_closest_inl(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overf
         }
       }
     } else {
-      BNode ln = load_node(m.nodes, nd.left), rn = load_node(m.nodes, nd.right);
+      BNode ln, rn;
+      load_pair(m.nodes, nd.left, ln, rn);
       tl.node(2);
       float dl = dist2_aabb(p, ln), dr = dist2_aabb(p, rn);
       if (sp + 2 > BVH_STACK) {

@@ -2684,7 +2684,7 @@ int mupsi_gpu_scene_set_occlusion(mupsi_scene* scene, int32_t mode) {
   if (mode != MUPSI_OCCLUSION_REFERENCE && mode != MUPSI_OCCLUSION_ROOT)
     return fail(MUPSI_ERR_INVALID, "unknown occlusion mode");
   for (int i = 0; i < scene->h.nmesh; ++i)
-    scene->h.meshes[i].occl_start = mode == MUPSI_OCCLUSION_ROOT ? scene->h.meshes[i].root : 0u;
+    scene->h.meshes[i].occl_start = mode == MUPSI_OCCLUSION_ROOT ? scene->h.meshes[i].root : scene->h.meshes[i].occl_ref;
   MUPSI_CUDA(cudaDeviceSynchronize());
   MUPSI_CUDA(cudaMemcpy(scene->d, &scene->h, sizeof(DScene), cudaMemcpyHostToDevice));
   return MUPSI_OK;

@@ -494,7 +494,8 @@ MD float bvh_closest_group_impl(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool
         } else if (sp + 2 > BVH_STACK) {
           ovf = true;
         } else {
-          const BNode ln = load_node(m.nodes, nd.left), rn = load_node(m.nodes, nd.right);
+          BNode ln, rn;
+          load_pair(m.nodes, nd.left, ln, rn);
           tl.node(2);
           const float dl = dist2_aabb(p, ln), dr = dist2_aabb(p, rn);
           if (dl < dr) {
