@@ -67,6 +67,22 @@ def test_noalloc_mesh_mean(gpu):
     assert (ref[:, 0] < 1).sum() > 20
 
 
+def test_noalloc_allocates_nothing(gpu):
+    """After the first call (which looks up the static array), calls leave the
+    device's free memory unchanged: no allocation, no pool growth."""
+    import torch
+    gs = GpuScene(S.config_mesh_scene(level=3, width=32, height=32, spp=4, seed=5))
+    xs, ys, ks = (torch.from_numpy(a).cuda() for a in _samples(32, 32, 4))
+    out = torch.empty((len(xs), 3), dtype=torch.float32, device="cuda")
+    gs.trace_noalloc(xs, ys, ks, out)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(5):
+        gs.trace_noalloc(xs, ys, ks, out)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+
+
 def test_noalloc_limits(gpu):
     import torch
     gs = GpuScene(S.config0_scene(16, 16, 1))
