@@ -32,8 +32,8 @@ extern "C" {
 #endif
 
 /* 2: mupsi_tuning gained block_rays; 3: mupsi_render_stats gained bvh_nodes/bvh_tris,
- * mupsi_tuning gained lane_rays */
-#define MUPSI_GPU_ABI_VERSION 3
+ * mupsi_tuning gained lane_rays; 4: mupsi_tuning gained mu_batch */
+#define MUPSI_GPU_ABI_VERSION 4
 
 typedef enum { MUPSI_MEM_HOST = 0, MUPSI_MEM_DEVICE = 1 } mupsi_mem;
 
@@ -515,6 +515,9 @@ typedef struct mupsi_tuning {
   int32_t lane_max_tris; /* mesh means: one ray per lane only while every mesh mean of the scene
                             has at most this many triangles (larger meshes keep lane groups,
                             which share each closest-point query); >= 0 */
+  int32_t mu_batch;    /* mesh means marched one ray per lane: a march that needs the exact mean
+                          (a BVH query) waits until this many of its warp's marches do, or all of
+                          them, and those queries run together; 0 = each at once. 0..32 */
 } mupsi_tuning;
 int mupsi_gpu_set_tuning(const mupsi_tuning* t);
 int mupsi_gpu_get_tuning(mupsi_tuning* out);

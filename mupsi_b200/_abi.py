@@ -170,6 +170,7 @@ class Tuning(C.Structure):
         ("block_rays", C.c_int32),
         ("lane_rays", C.c_int32),
         ("lane_max_tris", C.c_int32),
+        ("mu_batch", C.c_int32),
     ]
 
 

@@ -236,7 +236,8 @@ class DeviceMesh:
 
 
 TUNING_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning.json")
-_TUNING_KEYS = ("march_block", "min_group", "shade_block", "wave_paths", "block_rays", "lane_rays", "lane_max_tris")
+_TUNING_KEYS = ("march_block", "min_group", "shade_block", "wave_paths", "block_rays", "lane_rays", "lane_max_tris",
+                "mu_batch")
 _tuning_applied = False
 
 
@@ -255,7 +256,7 @@ def get_tuning():
 
 def set_tuning(**kw):
     """Change some launch shapes (march_block, min_group, shade_block, wave_paths, block_rays, lane_rays,
-    lane_max_tris). The committed tuning file is applied first, so a value set
+    lane_max_tris, mu_batch). The committed tuning file is applied first, so a value set
     here is not replaced when the first scene is created."""
     if kw:
         _ensure_tuning()

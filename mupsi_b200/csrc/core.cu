@@ -5,6 +5,8 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -14,6 +16,7 @@
 
 namespace mupsi {
 
+constexpr int kWideRowsHost = 8;  // float4 rows of a four-wide node (DMesh::wide)
 static thread_local std::string g_last_error;
 static std::atomic<int64_t> g_launches{0};
 
@@ -352,6 +355,69 @@ static cudaError_t upload(std::vector<void*>& allocs, const T* src, size_t count
   return e;
 }
 
+// The binary tree four wide (DMesh::wide, WNode rows): each node takes the two
+// children of a binary node and keeps replacing its inner child of largest box
+// surface by that child's two children while it has fewer than four. Boxes and
+// leaf ranges are the binary tree's own; node 0 is the root. Empty for a tree
+// that is a single leaf or whose leaf slots exceed the child encoding.
+static std::vector<float> build_wide(const std::vector<HostNode>& nodes, uint32_t root, int64_t num_faces) {
+  std::vector<float> w;
+  constexpr uint32_t kLeaf = 0x80000000u;
+  if (nodes.empty() || (nodes[root].right & kLeaf) || num_faces >= (1ll << 28)) return w;
+  auto area = [&](uint32_t i) {
+    const HostNode& n = nodes[i];
+    const float dx = n.mx[0] - n.mn[0], dy = n.mx[1] - n.mn[1], dz = n.mx[2] - n.mn[2];
+    return dx * dy + dy * dz + dz * dx;
+  };
+  // nodes breadth first: (binary inner node, wide index)
+  std::vector<std::pair<uint32_t, uint32_t>> order{{root, 0u}};
+  w.assign(kWideRowsHost * 4, 0.0f);
+  for (size_t h = 0; h < order.size(); ++h) {
+    const uint32_t b = order[h].first, wi = order[h].second;
+    uint32_t kids[4] = {nodes[b].left, nodes[b].right, 0, 0};
+    int nk = 2;
+    while (nk < 4) {
+      int pick = -1;
+      float pa = -1.0f;
+      for (int i = 0; i < nk; ++i)
+        if (!(nodes[kids[i]].right & kLeaf) && area(kids[i]) > pa) {
+          pa = area(kids[i]);
+          pick = i;
+        }
+      if (pick < 0) break;
+      const uint32_t k = kids[pick];
+      kids[pick] = nodes[k].left;
+      kids[nk++] = nodes[k].right;
+    }
+    for (int i = 0; i < 4; ++i) {
+      float* row = &w[(size_t)kWideRowsHost * 4 * wi];
+      uint32_t ref = kLeaf;  // unused slot: count 0, empty box
+      float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+      if (i < nk) {
+        const HostNode& c = nodes[kids[i]];
+        for (int a = 0; a < 3; ++a) {
+          lo[a] = c.mn[a];
+          hi[a] = c.mx[a];
+        }
+        if (c.right & kLeaf) {
+          ref = kLeaf | ((c.right & ~kLeaf) << 28) | c.left;
+        } else {
+          ref = (uint32_t)(w.size() / (kWideRowsHost * 4));
+          order.push_back({kids[i], ref});
+          w.resize(w.size() + kWideRowsHost * 4, 0.0f);
+          row = &w[(size_t)kWideRowsHost * 4 * wi];
+        }
+      }
+      for (int a = 0; a < 3; ++a) {
+        row[4 * a + i] = lo[a];
+        row[4 * (3 + a) + i] = hi[a];
+      }
+      std::memcpy(&row[4 * 6 + i], &ref, 4);
+    }
+  }
+  return w;
+}
+
 int make_device_mesh(const mupsi_mesh_desc& md, DMesh& d, std::vector<void*>& allocs) {
   if (md.num_vertices < 0 || md.num_faces < 0) return fail(MUPSI_ERR_INVALID, "negative mesh size");
   if ((md.num_vertices > 0 && !md.vertices) || (md.num_faces > 0 && !md.faces))
@@ -384,6 +450,7 @@ int make_device_mesh(const mupsi_mesh_desc& md, DMesh& d, std::vector<void*>& al
   // a traversal reads both with one 64-byte load. Boxes, leaf ranges and the
   // tree are the reference's; only node positions change (traversal order
   // follows boxes and centroids, not positions).
+  const std::vector<float> wide = build_wide(nodes, root, md.num_faces);
   std::vector<HostNode> dev_nodes;
   uint32_t occl_ref = 0;  // where the reference's node 0 (BVH::occluded's start) lands
   if (!nodes.empty()) {
@@ -431,6 +498,14 @@ int make_device_mesh(const mupsi_mesh_desc& md, DMesh& d, std::vector<void*>& al
   if (md.vertex_normals) {
     if ((e = upload(allocs, md.vertex_normals, 3 * md.num_vertices, d.vert_n)) != cudaSuccess)
       return fail(MUPSI_ERR_CUDA, std::string("mesh upload: ") + cudaGetErrorString(e));
+  }
+  if (!wide.empty()) {
+    const float* dw = nullptr;
+    if ((e = upload(allocs, wide.data(), wide.size(), dw)) != cudaSuccess)
+      return fail(e == cudaErrorMemoryAllocation ? MUPSI_ERR_OOM : MUPSI_ERR_CUDA,
+                  std::string("mesh upload: ") + cudaGetErrorString(e));
+    d.wide = reinterpret_cast<const float4*>(dw);
+    d.wide_root = 0;
   }
   d.nodes = dn;
   d.soup = reinterpret_cast<const float4*>(dsoup);

@@ -54,7 +54,19 @@ struct DMesh {
   // nullable: BVH work counters (instrumentation), kBvhCountSlots pairs of
   // (nodes loaded, triangles tested); set only while a scene counts its work
   unsigned long long* count;
+  // nullable: the same tree four wide (WNode), for the closest-point queries
+  // whose answer does not depend on the tree's shape (bvh_closest_lowtie)
+  const float4* wide;
+  uint32_t wide_root;
 };
+
+// A node of the four-wide tree: the boxes of up to four children of the
+// binary tree (two or three of its levels collapsed), as 16-byte rows
+// lo.x[4], lo.y[4], lo.z[4], hi.x[4], hi.y[4], hi.z[4], child[4], unused[4]:
+// one 128-byte read per visit. child: a node index, or W_LEAF | count << 28 |
+// first leaf-order slot; an unused slot has an empty box (lo = +inf, hi = -inf).
+constexpr uint32_t W_LEAF = 0x80000000u;
+constexpr int kWideRows = 8;  // float4 rows per node
 
 // BVH work tallies of one traversal: every node load (32 bytes) and every
 // triangle tested (its 48-byte leaf-order record). CNT = false
@@ -380,6 +392,97 @@ MD float bvh_closest_inl(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overf
   return sqrtf(best);
 }
 
+// BVH::closest over the four-wide tree with the lane-group rule (LOWTIE of
+// bvh_closest_inl): boxes farther than the best are pruned, equal ones kept,
+// and among triangles at the best distance the lowest index wins, so the
+// triangle and point found do not depend on the tree's shape: they are the
+// binary tree's. Its boxes are the binary tree's boxes, with the same
+// distance arithmetic. Stack entries carry their box distance, so a popped
+// entry is pruned without reloading its node.
+template <bool CNT = false>
+MD float bvh4_closest_inl(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overflow, float best_init, bool* found) {
+  BvhTally<CNT> tl;
+  uint32_t sr[BVH_STACK];
+  float sd[BVH_STACK];
+  int sp = 0;
+  sr[0] = m.wide_root;
+  sd[0] = 0.0f;
+  sp = 1;
+  float best = best_init;
+  if (found) *found = false;
+  uint32_t btri = 0xffffffffu;
+  while (sp > 0) {
+    --sp;
+    const uint32_t ref = sr[sp];
+    if (sd[sp] > best) continue;
+    if (ref & W_LEAF) {
+      const uint32_t start = ref & 0x0fffffffu, cnt = (ref >> 28) & 7u;
+      for (uint32_t i = start; i < start + cnt; ++i) {
+        tl.tri();
+        v3 a, b, c, tmp;
+        const uint32_t ti = leaf_tri(m, i, a, b, c);
+        const float d = dist2_tri(p, a, b, c, tmp);
+        if (d < best || (d == best && d < best_init && ti < btri)) {
+          best = d;
+          tri = ti;
+          btri = ti;
+          q = tmp;
+          if (found) *found = true;
+        }
+      }
+      continue;
+    }
+    const float4* np = m.wide + (size_t)kWideRows * ref;
+    const float4 lx = __ldg(np), ly = __ldg(np + 1), lz = __ldg(np + 2);
+    const float4 hx = __ldg(np + 3), hy = __ldg(np + 4), hz = __ldg(np + 5);
+    const uint4 ch = __ldg(reinterpret_cast<const uint4*>(np + 6));
+    tl.node(4);
+    // the four children's distances, as dist2_aabb forms them
+    auto d2 = [&](float ax, float ay, float az, float bx, float by, float bz) {
+      const float dx = max3_il(ax - p.x, 0.0f, p.x - bx);
+      const float dy = max3_il(ay - p.y, 0.0f, p.y - by);
+      const float dz = max3_il(az - p.z, 0.0f, p.z - bz);
+      return dx * dx + dy * dy + dz * dz;
+    };
+    float dd[4] = {d2(lx.x, ly.x, lz.x, hx.x, hy.x, hz.x), d2(lx.y, ly.y, lz.y, hx.y, hy.y, hz.y),
+                   d2(lx.z, ly.z, lz.z, hx.z, hy.z, hz.z), d2(lx.w, ly.w, lz.w, hx.w, hy.w, hz.w)};
+    uint32_t cr[4] = {ch.x, ch.y, ch.z, ch.w};
+    // kept children pushed farthest first, so the nearest is popped next
+    // (a sorting network on the four; pruned ones sort to the end as +inf)
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (dd[k] > best) dd[k] = INFINITY;
+    auto cs = [&](int a, int b) {
+      if (dd[b] > dd[a]) {
+        const float t = dd[a];
+        dd[a] = dd[b];
+        dd[b] = t;
+        const uint32_t u = cr[a];
+        cr[a] = cr[b];
+        cr[b] = u;
+      }
+    };
+    cs(0, 1);
+    cs(2, 3);
+    cs(0, 2);
+    cs(1, 3);
+    cs(1, 2);
+    if (sp + 4 > BVH_STACK) {
+      overflow = true;
+      break;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (dd[k] != INFINITY) {
+        sr[sp] = cr[k];
+        sd[sp] = dd[k];
+        ++sp;
+      }
+  }
+  tl.flush(m);
+  return sqrtf(best);
+}
+
 // The traversals out of line: every kernel carries one copy of each instead of
 // one per query site. The mesh-mean march, whose warps otherwise stall on
 // instruction fetch, renders a level-6 mesh at 512x512x4 in 227 ms instead of
@@ -405,8 +508,13 @@ static __device__ __noinline__ float bvh_closest(const DMesh& m, v3 p, uint32_t&
   return bvh_closest_inl(m, p, tri, q, overflow, best_init, found);
 }
 // One lane's closest-point query with the lane-group rule (LOWTIE).
+// (The four-wide tree when the mesh has one: the same triangle and point.)
 static __device__ __noinline__ float bvh_closest_lowtie(const DMesh& m, v3 p, uint32_t& tri, v3& q, bool& overflow,
                                                         float best_init, bool* found) {
+  if (m.wide) {
+    if (m.count) return bvh4_closest_inl<true>(m, p, tri, q, overflow, best_init, found);
+    return bvh4_closest_inl<false>(m, p, tri, q, overflow, best_init, found);
+  }
   if (m.count) return bvh_closest_inl<true, true>(m, p, tri, q, overflow, best_init, found);
   return bvh_closest_inl<false, true>(m, p, tri, q, overflow, best_init, found);
 }

@@ -242,6 +242,8 @@ struct WaveCfg {
   int block_rays;                // block-per-ray marches while n <= block_rays * blocks (sphere means)
   int lane_rays;                 // > 0: one ray per lane for long sphere-mean queues (march_lanes), this
                                  // many visited steps per ray between the warp's psi rounds
+  int mu_batch = 0;              // > 0: one-ray-per-lane mesh marches leave their BVH queries until this
+                                 // many of a warp's marches wait for one (or all of them do)
   int* err;                      // device error word (ERR_* bits)
   unsigned long long* counters;  // nullable work counters
 };
@@ -539,6 +541,7 @@ __device__ void march_lanes(const DScene* const* __restrict__ scenes, Paths& P, 
             march_begin(S, m, mk3(o.x, o.y, o.z), mk3(d.x, d.y, d.z), o.w, 3.402823466e+38f, med,
                         medium_seed(S, meta.x, meta.y, meta.z, meta_bounce(meta.w)), load_cond(P, idx));
             m.may_request = MK != MEAN_SPHERE_ONLY && can_suspend && m.lazy && S->media[med].surr;
+            m.defer_mu = MK != MEAN_SPHERE_ONLY && m.lazy && !m.may_request && cfg.mu_batch > 0;
             if (MK != MEAN_SPHERE_ONLY && resume) {
               const float4 a = P.ms0[idx], b = P.ms1[idx];
               const int fl = __float_as_int(a.w);
@@ -646,7 +649,7 @@ __device__ void march_lanes(const DScene* const* __restrict__ scenes, Paths& P, 
       if (lane == a) nz = ga;
       if (lane == b && b != a) nz = gb;
     }
-    if (active && m.status != 0) {
+    if (active && (m.status == 1 || m.status == 2)) {
       if (hit) {  // march_result: normalize(grad f) at the hit step
         const DMedium& md = S->media[m.medium];
         const float4 mu = mean_value_grad<MK>(S, md, ph, ovf);
@@ -665,6 +668,22 @@ __device__ void march_lanes(const DScene* const* __restrict__ scenes, Paths& P, 
       mus += m.n_mu;
       pars += m.n_par;
       active = false;
+    }
+    if constexpr (MK != MEAN_SPHERE_ONLY) {
+      // marches waiting for an exact mean (statuses 5, 6) query the BVH together
+      // once mu_batch of them wait, or every active one does: one lane's
+      // traversal no longer holds the warp's other marches at each query
+      // (deferring the origins' and the hits' queries the same way measured slower)
+      const bool wait = active && (m.status == 5 || m.status == 6);
+      const unsigned wm = __ballot_sync(full, wait);
+      if (wm && (__popc(wm) >= cfg.mu_batch || wm == __ballot_sync(full, active))) {
+        if (wait) {
+          if (m.status == 5)
+            march_exact_step<MK>(S, m, &solo, ovf);
+          else
+            march_exact_decide<MK>(S, m, &solo, ovf);
+        }
+      }
     }
   }
   if (ovf) atomicOr(cfg.err, ERR_BVH_STACK);
@@ -1625,7 +1644,7 @@ int ensure_paths(mupsi_scene* s, int64_t cap) {
 
 // Launch shapes of the wave kernels (mupsi_gpu_set_tuning; chosen by the
 // project's autotuner, mupsi_b200/autotune.py).
-mupsi_tuning g_tuning = {128, 4, 128, 0, 8, 1, 262144};
+mupsi_tuning g_tuning = {128, 4, 128, 0, 8, 1, 262144, 16};
 
 // Persistent march grid: resident blocks per SM x SMs.
 struct MarchLaunch {
@@ -1764,6 +1783,7 @@ WaveExec scene_exec(mupsi_scene* s) {
   w.cfg.min_group = g_tuning.min_group;
   w.cfg.block_rays = g_tuning.block_rays;
   w.cfg.lane_rays = lane_rays_for(s->h);
+  w.cfg.mu_batch = g_tuning.mu_batch;
   w.cfg.err = s->err;
   w.cfg.counters = s->profile ? s->counters : nullptr;
   w.mlp = s->surr_mlp;
@@ -2001,6 +2021,7 @@ void batch_wave_launches(mupsi_batch* b, int iters) {
   w.cfg.min_group = g_tuning.min_group;
   w.cfg.block_rays = g_tuning.block_rays;
   w.cfg.lane_rays = batch_lane_rays(b);
+  w.cfg.mu_batch = g_tuning.mu_batch;
   w.cfg.err = b->err;
   w.cfg.counters = nullptr;
   WaveSrc src;
@@ -2013,7 +2034,8 @@ void batch_wave_launches(mupsi_batch* b, int iters) {
 
 bool same_tuning(const mupsi_tuning& a, const mupsi_tuning& c) {
   return a.march_block == c.march_block && a.min_group == c.min_group && a.shade_block == c.shade_block &&
-         a.block_rays == c.block_rays && a.lane_rays == c.lane_rays && a.lane_max_tris == c.lane_max_tris;
+         a.block_rays == c.block_rays && a.lane_rays == c.lane_rays && a.lane_max_tris == c.lane_max_tris &&
+         a.mu_batch == c.mu_batch;
 }
 
 // The graph of a wave with `iters` bounce iterations, captured on first use.
@@ -2398,6 +2420,7 @@ int mupsi_gpu_set_tuning(const mupsi_tuning* t) {
   if (t->block_rays < 0 || t->block_rays > 256) return fail(MUPSI_ERR_INVALID, "block_rays must be in [0, 256]");
   if (t->lane_rays < 0 || t->lane_rays > 64) return fail(MUPSI_ERR_INVALID, "lane_rays must be in [0, 64]");
   if (t->lane_max_tris < 0) return fail(MUPSI_ERR_INVALID, "lane_max_tris must be >= 0");
+  if (t->mu_batch < 0 || t->mu_batch > 32) return fail(MUPSI_ERR_INVALID, "mu_batch must be in [0, 32]");
   g_tuning = *t;
   return MUPSI_OK;
 }

@@ -351,7 +351,9 @@ struct March {
   bool fprev_big; // |f_origin| > B: its value never decides the 1e-6 test
   float fprev;
   int status;     // 0 running, 1 hit, 2 exited, 3 suspended for a surrogate prediction at a
-                  // step march_cheap reached, 4 ... in march_decide (psi of the step in spec_q)
+                  // step march_cheap reached, 4 ... in march_decide (psi of the step in spec_q),
+                  // 5 waiting for the exact mean at a step march_cheap reached (defer_mu),
+                  // 6 ... in march_decide (psi of the step in spec_q)
   int medium;
   uint32_t n_steps, n_psi;  // work counters: steps visited, psi evaluations
   uint32_t n_mu, n_par;     // mesh means: exact evaluations, parity casts among them
@@ -366,6 +368,10 @@ struct March {
   bool may_request;
   int n_req;
   float t_resumed;
+  // BVH queries of the lazy mean left to the caller (statuses 5 and 6), which
+  // runs them for many marches at once (march_exact_step / march_exact_decide);
+  // exact_here: mu_j is the exact mean at the current step
+  bool defer_mu, exact_here;
   // pending step between the two phases
   bool pend_exact;  // pend_mu holds the exact mean at the pending point
   float pend_mu, pend_lb, pend_sgn;
@@ -405,6 +411,8 @@ MD void march_begin(const DScene* S, March& m, v3 o, v3 d, float near_t, float f
   m.t_j = 0.0f;
   m.mu_hi = 0.0f;
   m.may_request = false;
+  m.defer_mu = false;
+  m.exact_here = false;
   m.n_req = 0;
   m.t_resumed = -1.0f;
   m.pend_exact = false;
@@ -680,6 +688,12 @@ MD bool march_cheap(const DScene* S, March& m, v3& p, bool& ovf, const Group* g 
       m.t_j = m.t;
       lb = fabsf(mu);
       sgn = mu;
+    } else if (m.exact_here) {  // resumed with the exact mean of this step (status 5)
+      m.exact_here = false;
+      mu = m.mu_j;
+      lb = fabsf(mu);
+      sgn = mu;
+      exact = true;
     } else {
       lb = mu_lower(m, m.t);
       sgn = m.mu_j;
@@ -697,6 +711,11 @@ MD bool march_cheap(const DScene* S, March& m, v3& p, bool& ovf, const Group* g 
           // ask the surrogate first: the march is suspended here and resumes
           // at this step with the prediction (march_apply_prediction)
           m.status = 3;
+          return false;
+        }
+        if (m.defer_mu) {  // the caller queries the BVH (march_exact_step), then this step goes on
+          m.n_steps--;
+          m.status = 5;
           return false;
         }
         mu = mean_exact<MK>(S, m, p, m.t, ovf, g);
@@ -760,6 +779,21 @@ MD bool march_apply_prediction(const DMedium& md, March& m, float pred) {
 template <int MK>
 MD void march_decide(const DScene* S, March& m, v3 p, float q, const Group* g, bool& ovf);
 
+// f at the current step decided: the origin's value, a hit, or the next step.
+MD void march_settle(const DScene* S, March& m, float f) {
+  if (m.init) {
+    m.fprev = f;
+    m.fprev_pos = f > 0.0f;
+    m.init = false;
+    return;
+  }
+  if ((f > 0.0f) != m.fprev_pos && (m.fprev_big || (double)fabsf(m.fprev - f) > 1e-6)) {
+    m.status = 1;
+    return;
+  }
+  march_advance(S, m, -INFINITY);
+}
+
 // A march suspended in march_decide (status 4) resumes there: the step's psi q
 // (saved with the march) and the prediction's anchor, or, without a usable
 // prediction, the exact mean (t_resumed blocks a second request).
@@ -771,6 +805,36 @@ static __device__ __noinline__ void march_resume_decide(const DScene* S, March& 
   m.pend_lb = 0.0f;  // the |mu| bound of the step did not settle it before the suspension
   m.pend_sgn = 0.0f;
   march_decide<MK>(S, m, m.o + m.d * m.t, q, g, ovf);
+}
+
+// A march waiting for the exact mean at the step march_cheap reached (status
+// 5): the BVH query, then the step goes on as march_cheap takes it with the
+// exact value. Out of line, as march_resume_decide.
+template <int MK>
+static __device__ __noinline__ void march_exact_step(const DScene* S, March& m, const Group* g, bool& ovf) {
+  const float mu = mean_exact<MK>(S, m, m.o + m.d * m.t, m.t, ovf, g);
+  m.mu_j = mu;
+  m.mu_hi = fabsf(mu);
+  m.t_j = m.t;
+  m.exact_here = true;
+  m.status = 0;
+}
+// A march waiting for the exact mean in march_decide (status 6, the step's psi
+// in spec_q): the BVH query and the rest of march_decide.
+template <int MK>
+static __device__ __noinline__ void march_exact_decide(const DScene* S, March& m, const Group* g, bool& ovf) {
+  m.status = 0;
+  const v3 p = m.o + m.d * m.t;
+  const DMedium& md = S->media[m.medium];
+  const float q = m.spec_q;
+  float c = m.c.active ? cond_value(md.k, m.c, p) : 0.0f;
+  float mu = mean_exact<MK>(S, m, p, m.t, ovf, g);
+  m.mu_j = mu;
+  m.mu_hi = fabsf(mu);
+  m.t_j = m.t;
+  float f = mu + q;
+  if (m.c.active) f += c;
+  march_settle(S, m, f);
 }
 
 // Phase B: f at the pending point (value only); decides hit or next step. The
@@ -861,6 +925,11 @@ MD void march_decide(const DScene* S, March& m, v3 p, float q, const Group* g, b
       m.status = 4;
       return;
     }
+    if (m.defer_mu) {  // the caller queries the BVH (march_exact_decide)
+      m.spec_q = q;
+      m.status = 6;
+      return;
+    }
     float mu = mean_exact<MK>(S, m, p, m.t, ovf, g);
     m.mu_j = mu;
     m.mu_hi = fabsf(mu);
@@ -868,17 +937,7 @@ MD void march_decide(const DScene* S, March& m, v3 p, float q, const Group* g, b
     f = mu + q;
     if (m.c.active) f += c;
   }
-  if (m.init) {
-    m.fprev = f;
-    m.fprev_pos = f > 0.0f;
-    m.init = false;
-    return;
-  }
-  if ((f > 0.0f) != m.fprev_pos && (m.fprev_big || (double)fabsf(m.fprev - f) > 1e-6)) {
-    m.status = 1;
-    return;
-  }
-  march_advance(S, m, -INFINITY);
+  march_settle(S, m, f);
 }
 
 // GPMedium::evalWithGradient with the psi sum shared by group g (WIDE: g.G >= 4)

@@ -103,7 +103,7 @@ def load():
         if not os.path.exists(LIB_PATH):
             raise FileNotFoundError(f"{LIB_PATH} is missing: build it with `python -m mupsi_b200.build`")
         _lib = _setup(C.CDLL(LIB_PATH))
-        if _lib.mupsi_gpu_abi_version() != 3:
+        if _lib.mupsi_gpu_abi_version() != 4:
             raise RuntimeError("libmupsi_gpu.so ABI version mismatch")
     return _lib
 

@@ -108,12 +108,15 @@ def test_lane_rays_render_matches(gpu, tuning_restored):
 
 def test_lane_rays_mesh_render_matches(gpu, tuning_restored):
     """Mesh means marched one ray per lane (the lazy mean's closest-point
-    queries on one lane with the lane-group tie rule) or by lane groups, and a
-    mesh above lane_max_tris kept on lane groups: identical images."""
+    queries on one lane with the lane-group tie rule, over the four-wide tree;
+    with mu_batch > 0 a warp's marches that need the exact mean wait and query
+    the BVH together) or by lane groups (binary tree), and a mesh above
+    lane_max_tris kept on lane groups: identical images."""
     sc = S.config_mesh_scene(level=5, width=128, height=128, spp=4, seed=2)
     imgs = []
-    for lr, lmt in ((0, 1 << 18), (1, 1 << 18), (4, 1 << 18), (1, 0)):
-        set_tuning(lane_rays=lr, lane_max_tris=lmt)
+    for lr, lmt, mb in ((0, 1 << 18, 16), (1, 1 << 18, 0), (1, 1 << 18, 16), (4, 1 << 18, 8), (1, 1 << 18, 32),
+                        (1, 0, 16)):
+        set_tuning(lane_rays=lr, lane_max_tris=lmt, mu_batch=mb)
         r = GpuRenderer()
         g = GpuScene(sc)
         r.prepare_render(g)
@@ -180,3 +183,5 @@ def test_batch_zero_spp_and_errors(gpu):
         set_tuning(march_block=256)
     with pytest.raises(MupsiError):
         set_tuning(block_rays=257)
+    with pytest.raises(MupsiError):
+        set_tuning(mu_batch=33)
