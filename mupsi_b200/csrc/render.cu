@@ -740,7 +740,8 @@ __global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? MUPSI_SPHERE_MAR
     }
   }
   if (LANES && !SH && cfg.lane_rays) {
-    // long queues: one ray per lane, at least 2 rays per warp on average
+    // long queues: one ray per lane, at least 2 rays per warp on average (4, 8 or
+    // 16 measured the same: the late bounces' time is their longest marches)
     const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
     if ((uint64_t)n >= 2 * warps) {
       int r = 2;
