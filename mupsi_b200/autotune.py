@@ -34,12 +34,13 @@ CANDIDATES = {
     # choice (a level-6 mesh is faster one ray per lane, a level-8 mesh with
     # lane groups)
     "lane_max_tris": [1 << 18],
-    # the same (measured on the level-6 mesh render: 0 / 8 / 16 / 24 / 32 ->
-    # 318 / 274 / 265 / 259 / 267 ms at 512^2 x 8)
-    "mu_batch": [16],
+    # the same (measured on the level-6 mesh render at 512^2 x 8 with the
+    # one-ray-per-lane mesh march at 16 blocks per SM: 8 / 16 / 24 / 32 ->
+    # 248 / 232 / 227 / 227 ms)
+    "mu_batch": [24],
 }
 DEFAULT = {"march_block": 128, "min_group": 4, "shade_block": 128, "wave_paths": 1 << 23, "block_rays": 8,
-           "lane_rays": 1, "lane_max_tris": 1 << 18, "mu_batch": 16}
+           "lane_rays": 1, "lane_max_tris": 1 << 18, "mu_batch": 24}
 
 
 def coordinate_descent(measure, candidates=CANDIDATES, start=DEFAULT, passes=2):

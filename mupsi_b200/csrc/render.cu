@@ -711,7 +711,7 @@ __device__ void march_lanes(const DScene* const* __restrict__ scenes, Paths& P, 
 #define MUPSI_MESH_MARCH_BLOCKS 16  // ... of the general (mesh-mean) march with lane groups
 #endif
 #ifndef MUPSI_MESH_LANE_MARCH_BLOCKS
-#define MUPSI_MESH_LANE_MARCH_BLOCKS 8  // ... and of the mesh-mean march with one ray per lane
+#define MUPSI_MESH_LANE_MARCH_BLOCKS 16  // ... and of the mesh-mean march with one ray per lane
 #endif
 // LANES: the instantiation carries march_lanes (one ray per lane); the mesh
 // kernel without it keeps its registers for the lane-group march alone
@@ -1645,7 +1645,7 @@ int ensure_paths(mupsi_scene* s, int64_t cap) {
 
 // Launch shapes of the wave kernels (mupsi_gpu_set_tuning; chosen by the
 // project's autotuner, mupsi_b200/autotune.py).
-mupsi_tuning g_tuning = {128, 4, 128, 0, 8, 1, 262144, 16};
+mupsi_tuning g_tuning = {128, 4, 128, 0, 8, 1, 262144, 24};
 
 // Persistent march grid: resident blocks per SM x SMs.
 struct MarchLaunch {

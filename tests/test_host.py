@@ -134,7 +134,7 @@ def test_batch_scenes_parameters():
 def test_autotune_coordinate_descent():
     from mupsi_b200.autotune import CANDIDATES, DEFAULT, coordinate_descent
     target = {"march_block": 96, "min_group": 16, "shade_block": 64, "wave_paths": 1 << 22, "block_rays": 4,
-              "lane_rays": 0, "lane_max_tris": 1 << 18, "mu_batch": 16}
+              "lane_rays": 0, "lane_max_tris": 1 << 18, "mu_batch": 24}
 
     def cost(cfg):
         return sum(abs(np.log2(cfg[k] + 1) - np.log2(target[k] + 1)) for k in target) + 1.0
