@@ -902,7 +902,10 @@ __global__ void __launch_bounds__(128, MK == MEAN_SPHERE_ONLY ? MUPSI_SPHERE_MAR
 // SDFMedium / ExternalGPMedium::sampleDistance for the paths of iteration `it`
 // whose medium is a field medium (k_march leaves them): one thread per path,
 // sphere tracing bounded by the reference's iteration limits (512 / 1024).
-__global__ void __launch_bounds__(128) k_march_field(const DScene* const* __restrict__ scenes, Paths P, int it,
+#ifndef MUPSI_FIELD_MARCH_BLOCKS
+#define MUPSI_FIELD_MARCH_BLOCKS 6  // resident 128-thread blocks per SM the field march is compiled for
+#endif
+__global__ void __launch_bounds__(128, MUPSI_FIELD_MARCH_BLOCKS) k_march_field(const DScene* const* __restrict__ scenes, Paths P, int it,
                                                      WaveCfg cfg) {
   bool ovf = false;
   if (cfg.shadow_pass) {  // the shadow jobs of field media (SDFMedium / ExternalGPMedium::transmittance)
