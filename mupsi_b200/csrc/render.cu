@@ -963,7 +963,10 @@ MD void push(uint32_t* q, uint32_t* count, uint32_t v) {
 }
 
 // One bounce of PathTracer::trace for every live path of iteration `it`.
-__global__ void __launch_bounds__(128) k_shade(const DScene* const* __restrict__ scenes, Paths P, int it, WaveCfg cfg) {
+#ifndef MUPSI_SHADE_BLOCKS
+#define MUPSI_SHADE_BLOCKS 4  // resident 128-thread blocks per SM the shading kernel is compiled for
+#endif
+__global__ void __launch_bounds__(128, MUPSI_SHADE_BLOCKS) k_shade(const DScene* const* __restrict__ scenes, Paths P, int it, WaveCfg cfg) {
   const uint32_t n = P.counts[2 * it + 1];
   const uint32_t* q = P.q[2 + (it & 1)];
   uint32_t* qm_next = P.q[(it + 1) & 1];
