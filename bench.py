@@ -312,6 +312,38 @@ def march_roofline(st, samples, ops=OPS_PER_IMPULSE, bvh=None, l2_gbs=None, hbm_
     return out
 
 
+def march_per_iteration(sc, st, pass0, pass1, fb, flush):
+    """The march roofline per bounce iteration of a render: each iteration's
+    impulse evaluations are the difference of two renders whose max_bounce
+    differs by one (iteration i runs the same marches in every render that
+    reaches it), set against that iteration's march time in the profiled
+    full render `st`."""
+    from mupsi_b200 import scene as S
+    from mupsi_b200.api import GpuRenderer, GpuScene
+    peak, _ = issue_bound(OPS_PER_IMPULSE)
+    imps = [0]
+    for b in range(1, sc.max_bounce + 1):
+        sb = S.config0_scene(sc.width, sc.height, sc.spp)
+        sb.max_bounce = b
+        g = GpuScene(sb)
+        r = GpuRenderer()
+        r.prepare_render(g)
+        g.profile(True)
+        flush.fill_(4)
+        r.start_render_progressive(pass1, spp_begin=pass0, out=fb)
+        imps.append(g.stats(reset=True)["impulse_evals"])
+        g.close()
+    rows = []
+    for i in range(sc.max_bounce):
+        ms = float(st["iter_march_ms"][i])
+        n = imps[i + 1] - imps[i]
+        rate = n / (ms / 1e3) if ms > 0 else 0.0
+        rows.append({"iteration": i, "rays": int(st["iter_medium"][i]), "impulse_evals": int(n),
+                     "march_ms": round(ms, 4), "Gimpulse_evals_s": round(rate / 1e9, 2),
+                     "frac": round(rate / peak, 4)})
+    return rows
+
+
 def bvh_bytes_per_sample(gs, render, samples):
     """Algorithmic BVH bytes per path sample of `render()` (counted traversals)."""
     gs.profile(True, bvh=True)
@@ -400,6 +432,8 @@ def run_gpu(args):
                  "launches": st["march_launches"], "ms_per_launch": st["march_ms"] / max(1, st["march_launches"]),
                  "impulse_evals_per_launch": st["impulse_evals"] / max(1, st["march_launches"]),
                  "iter_rays": st["iter_medium"][:10], "iter_march_ms": [round(x, 4) for x in st["iter_march_ms"][:10]]})
+    if world == 1:
+        roof["per_iteration"] = march_per_iteration(sc, st, pass0, pass1, fb, flush)
 
     # end to end through the public API with pinned host buffers: scene upload,
     # render, framebuffer read back, release, every step
