@@ -495,6 +495,9 @@ __device__ void march_block_rays(const DScene* const* __restrict__ scenes, Paths
 // Round r >= 1 of a march with a surrogate resumes the marches suspended in
 // round r - 1 with their predictions (req/pred lists); a march that asks for a
 // prediction is saved and suspended as in the lane-group march.
+#ifndef MUPSI_LANE_SPEC
+#define MUPSI_LANE_SPEC 1  // sphere means: a round's idle half-warp computes psi at the next step ahead
+#endif
 template <int MK>
 __device__ void march_lanes(const DScene* const* __restrict__ scenes, Paths& P, uint32_t n,
                             const uint32_t* __restrict__ q, uint32_t* cursor, const WaveCfg& cfg, int rays_per_warp,
@@ -590,11 +593,19 @@ __device__ void march_lanes(const DScene* const* __restrict__ scenes, Paths& P, 
     // the warp's psi values, two points per round; the kernel parameters are
     // read once when every ray of the warp has the same scene and medium
     float qv = 0.0f;
-    const unsigned vmask = __ballot_sync(full, want);
+    bool fresh = want;  // false: the step's psi was computed ahead (below)
+    if constexpr (MUPSI_LANE_SPEC && MK == MEAN_SPHERE_ONLY) {
+      if (want && m.spec_valid && m.spec_t == m.t) {
+        qv = m.spec_q;  // the same point and order: the same bits
+        fresh = false;
+      }
+      if (want) m.spec_valid = false;
+    }
+    const unsigned vmask = __ballot_sync(full, fresh);
     const int ref = vmask ? __ffs(vmask) - 1 : 0;
     const DScene* S0 = reinterpret_cast<const DScene*>(__shfl_sync(full, reinterpret_cast<unsigned long long>(S), ref));
     const int m0 = __shfl_sync(full, m.medium, ref);
-    const bool uni = __all_sync(full, !want || (S == S0 && m.medium == m0));
+    const bool uni = __all_sync(full, !fresh || (S == S0 && m.medium == m0));
     for (unsigned vm = vmask; vm;) {
       const int a = __ffs(vm) - 1;
       vm &= vm - 1u;
@@ -604,8 +615,31 @@ __device__ void march_lanes(const DScene* const* __restrict__ scenes, Paths& P, 
         vm &= vm - 1u;
       }
       const int src = lane < 16 ? a : b;
-      const v3 ps = mk3(__shfl_sync(full, p.x, src), __shfl_sync(full, p.y, src), __shfl_sync(full, p.z, src));
+      v3 ps = mk3(__shfl_sync(full, p.x, src), __shfl_sync(full, p.y, src), __shfl_sync(full, p.z, src));
       const uint32_t sd = __shfl_sync(full, m.seed, src);
+      // one point left (a round with an idle half-warp; in the late part of a
+      // launch most rounds): the upper half computes psi at the step after
+      // a's, the step march_advance moves to when this one is no hit, so a
+      // march that needs psi there too finds it ready (the 32-lane group's
+      // speculation, march_psi)
+      float tn = 0.0f;
+      bool spec = false;
+      if constexpr (MUPSI_LANE_SPEC && MK == MEAN_SPHERE_ONLY) {
+        if (b == a) {
+          bool ok;
+          if (m.use_tab) {
+            ok = active && m.k + 1 <= S->tab_steps;
+            tn = ok ? __ldg(S->tab + m.k + 1) : m.t;
+          } else {
+            tn = m.t + m.dt;
+            ok = active && tn < m.ft && tn != m.t;
+          }
+          const v3 pe = m.o + m.d * tn;
+          spec = __shfl_sync(full, ok ? 1 : 0, a) != 0;
+          const v3 pa = mk3(__shfl_sync(full, pe.x, a), __shfl_sync(full, pe.y, a), __shfl_sync(full, pe.z, a));
+          if (spec && lane >= 16) ps = pa;
+        }
+      }
       const DScene* Ss = S0;
       int ms = m0;
       if (!uni) {
@@ -617,6 +651,11 @@ __device__ void march_lanes(const DScene* const* __restrict__ scenes, Paths& P, 
       const float va = __shfl_sync(full, v, 0), vb = __shfl_sync(full, v, 16);
       if (lane == a) qv = va;
       if (lane == b && b != a) qv = vb;
+      if (MUPSI_LANE_SPEC && MK == MEAN_SPHERE_ONLY && spec && lane == a) {
+        m.spec_q = vb;
+        m.spec_t = tn;
+        m.spec_valid = true;
+      }
     }
     if (want) {
       m.n_psi++;
