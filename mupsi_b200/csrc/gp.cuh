@@ -135,6 +135,9 @@ MD void for_each_impulse(const KParams& k, int nx, int ny, int nz, uint32_t seed
   }
 }
 
+#ifndef MUPSI_SLOT_PAIRS
+#define MUPSI_SLOT_PAIRS 1  // value sums of a 3-impulse slot: both cells drawn at once
+#endif
 // One impulse's term w h (and w grad h when GRAD) added to the running sums.
 template <bool GRAD>
 struct PsiAcc {
@@ -158,12 +161,57 @@ struct PsiAcc {
   }
 };
 
+// The signed terms w h of one cell's impulses in draw order, each formed as
+// PsiAcc forms it (value only).
+template <int N>
+struct PsiTerms {
+  const KParams& k;
+  v3 p;
+  float h[N];
+  int n = 0;
+  MD void operator()(v3 s, uint32_t wsign) {
+    v3 d = p - s;
+    float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
+    h[n++] = __uint_as_float(__float_as_uint(ex2_approx(r2 * k.k2)) | wsign);
+  }
+};
+// The terms of cell c (0..27; 27 is outside the 27 neighbours and only ever
+// drawn, never added) with 3 impulses per cell, from jumped-ahead states.
+MD void cell_terms3(const KParams& k, int cx, int cy, int cz, uint32_t seed, int c, PsiTerms<3>& t) {
+  const int nx = cx + c / 9 - 1, ny = cy + (c / 3) % 3 - 1, nz = cz + c % 3 - 1;
+  const uint32_t cs = make_seed4((uint32_t)nx, (uint32_t)ny, (uint32_t)nz, seed);
+  const uint64_t st = (uint64_t)(uint32_t)(cs + 1u);
+  cell_impulses_ahead<3>(k, st, (float)nx * k.kr, (float)ny * k.kr, (float)nz * k.kr, t);
+}
 // Unnormalised InternalNoise sums over neighbour cells [c0, c1) of the 27, in
 // the reference's (dx, dy, dz) order (cell c = 9(dx+1) + 3(dy+1) + (dz+1)).
 // GRAD = false computes the value only.
 template <bool GRAD, int PPC = 0>
 MD void psi_sums_cells(const KParams& k, v3 p, int cx, int cy, int cz, uint32_t seed, int c0, int c1, float& sv,
                        float& sx, float& sy, float& sz) {
+  if constexpr (!GRAD && PPC < 0 && MUPSI_SLOT_PAIRS) {
+    if (k.ppc == 3 && c1 - c0 <= 2) {
+      // a slot of one or two cells: both cells' impulses drawn at once (six
+      // independent chains for the scheduler instead of two runs of three; a
+      // one-cell slot's lanes wait for the two-cell ones anyway), then added
+      // in the reference's order, so the same bits as the loop below
+      PsiTerms<3> ta{k, p}, tb{k, p};
+      cell_terms3(k, cx, cy, cz, seed, c0, ta);
+      cell_terms3(k, cx, cy, cz, seed, c0 + 1, tb);
+      float v = 0.0f;
+      v = v + ta.h[0];
+      v = v + ta.h[1];
+      v = v + ta.h[2];
+      if (c1 - c0 == 2) {
+        v = v + tb.h[0];
+        v = v + tb.h[1];
+        v = v + tb.h[2];
+      }
+      sv = v;
+      sx = sy = sz = 0.0f;
+      return;
+    }
+  }
   PsiAcc<GRAD> acc{k, p};
 #pragma unroll 1
   for (int c = c0; c < c1; ++c) {
